@@ -1,0 +1,252 @@
+// extern "C" entry points of include/fiim_b200.h and the C++ overloads with the
+// reference's exact signatures (include/fiim_b200_compat.hpp), so that the reference's
+// example drivers relink against this library unchanged.
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "fiim_b200.h"
+#include "fiim_internal.h"
+#include "fiim_solver.h"
+
+namespace {
+
+// Reference-facing calls reuse one solver per host thread while the problem shape is
+// unchanged, so repeated solves skip allocation, tuning and graph capture; the data
+// is uploaded again on every call, as the reference reads its arrays on every call.
+struct OneShot {
+    fiim::Solver *s = nullptr;
+    std::vector<long> key;
+    ~OneShot() {
+        if (s) {
+            s->destroy();
+            delete s;
+        }
+    }
+};
+thread_local OneShot g_one;
+
+int oneshot(int variant, int issym, char mode, int nr, int n, const double *Av, const int *Aj,
+            const int *Ai, const double *b, double tol, int NMAX, const double *Gv, const int *Gj,
+            const int *Gi, const double *IDv, const double *Hv, const int *Hj, const int *Hi,
+            const double *Lv, const int *Lj, const int *Li, const double *Uv, const int *Uj,
+            const int *Ui, double *x, double *resval, int *iter, int verbose, int *info) {
+    if (n <= 0 || !Ai || !Aj || !Av || !b || !x || !Gi || !Gj || !Gv || !IDv || !resval || !iter || !info)
+        return fiim::set_error(FIIM_EARG, "null argument or n <= 0");
+    fiim_options o;
+    fiim_options_default(&o);
+    o.variant = variant;
+    o.issym = issym;
+    o.mode = mode;
+    o.nr = nr;
+    o.verbose = verbose;
+    o.memory = FIIM_MEM_HOST;
+    const bool combined = (variant == FIIM_ACIFIM && mode == 'C' && nr > 1);
+    std::vector<long> key = {variant, issym, (long)mode, combined ? nr : 1, n, Ai[n], Gi[n],
+                             (!issym && Hi) ? Hi[n] : -1, (combined && Li) ? Li[n] : -1,
+                             (combined && Ui) ? Ui[n] : -1};
+    int rc;
+    if (g_one.s && g_one.key == key && !issym) {
+        g_one.s->opt.verbose = verbose;
+        rc = g_one.s->reload(Ai, Aj, Av, Gi, Gj, Gv, IDv, Hi, Hj, Hv, Li, Lj, Lv, Ui, Uj, Uv);
+    } else {
+        if (g_one.s) {
+            g_one.s->destroy();
+            delete g_one.s;
+            g_one.s = nullptr;
+        }
+        auto *s = new fiim::Solver;
+        rc = s->create(n, Ai, Aj, Av, Gi, Gj, Gv, IDv, Hi, Hj, Hv, Li, Lj, Lv, Ui, Uj, Uv, o);
+        if (rc != FIIM_OK) {
+            s->destroy();
+            delete s;
+            return rc;
+        }
+        g_one.s = s;
+        g_one.key = key;
+    }
+    if (rc != FIIM_OK) return rc;
+    fiim_result r{};
+    rc = g_one.s->solve(b, x, tol, NMAX, &r);
+    if (rc != FIIM_OK) return rc;
+    *resval = r.resval;
+    *iter = r.iter;
+    if (r.info >= 0) *info = r.info;   // NMAX < 0: the reference leaves info untouched
+    return FIIM_OK;
+}
+
+void throw_on(int rc) {
+    if (rc != FIIM_OK) throw std::runtime_error(std::string("fiim_b200: ") + fiim::last_error());
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *fiim_last_error(void) { return fiim::last_error(); }
+
+void fiim_options_default(fiim_options *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof *o);
+    o->variant = FIIM_AFIIM;
+    o->precision = FIIM_FP64;
+    o->memory = FIIM_MEM_HOST;
+    o->mode = 'E';
+    o->nr = 1;
+    o->autotune = 1;
+    o->inner_tol = 1e-5;
+    o->inner_nmax = 1000;
+    o->max_refine = 50;
+}
+
+int fiim_EPBiCGSTAB_afiim(int n, double *Av, int *Aj, int *Ai, double *b, double tol, int NMAX,
+                          double *Gv, int *Gj, int *Gi, double *IDv, double *Hv, int *Hj, int *Hi,
+                          double *x, double *resval, int *iter, int verbose, int *info) {
+    if (!Hv || !Hj || !Hi) return fiim::set_error(FIIM_EARG, "H is required");
+    return oneshot(FIIM_AFIIM, 0, 'E', 1, n, Av, Aj, Ai, b, tol, NMAX, Gv, Gj, Gi, IDv, Hv, Hj, Hi,
+                   nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, x, resval, iter, verbose,
+                   info);
+}
+
+int fiim_EPBiCGSTAB_pdfiim(int n, int issym, double *Av, int *Aj, int *Ai, double *b, double tol,
+                           int NMAX, double *Gv, int *Gj, int *Gi, double *ID, double *Hv, int *Hj,
+                           int *Hi, double *x, double *resval, int *iter, int verbose, int *info) {
+    if (!issym && (!Hv || !Hj || !Hi)) return fiim::set_error(FIIM_EARG, "H is required unless issym");
+    return oneshot(FIIM_PDFIIM, issym ? 1 : 0, 'E', 1, n, Av, Aj, Ai, b, tol, NMAX, Gv, Gj, Gi, ID,
+                   Hv, Hj, Hi, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, x, resval, iter,
+                   verbose, info);
+}
+
+int fiim_PBiCGSTAB_acifim(int n, double *Av, int *Aj, int *Ai, double *b, double tol, int NMAX,
+                          double *Gv, int *Gj, int *Gi, double *IDv, double *Hv, int *Hj, int *Hi,
+                          double *Lv, int *Lj, int *Li, double *Uv, int *Uj, int *Ui, int nr,
+                          char mode, double *x, double *resval, int *iter, int verbose, int *info) {
+    if (mode != 'E' && mode != 'C')
+        return fiim::set_error(FIIM_EARG, "ACIFIM mode '%c' applies triangular solves, not the factored inverse", mode);
+    if (!Hv || !Hj || !Hi) return fiim::set_error(FIIM_EARG, "H is required");
+    return oneshot(FIIM_ACIFIM, 0, mode, nr, n, Av, Aj, Ai, b, tol, NMAX, Gv, Gj, Gi, IDv, Hv, Hj,
+                   Hi, Lv, Lj, Li, Uv, Uj, Ui, x, resval, iter, verbose, info);
+}
+
+int fiim_solver_create(fiim_solver_t *out, int n, const int *Ai, const int *Aj, const double *Av,
+                       const int *Gi, const int *Gj, const double *Gv, const double *IDv,
+                       const int *Hi, const int *Hj, const double *Hv, const int *Li,
+                       const int *Lj, const double *Lv, const int *Ui, const int *Uj,
+                       const double *Uv, const fiim_options *opt) {
+    if (!out) return fiim::set_error(FIIM_EARG, "out is NULL");
+    *out = nullptr;
+    fiim_options o;
+    if (opt) o = *opt;
+    else fiim_options_default(&o);
+    if (o.precision != FIIM_FP64) {
+        return fiim_mixed_create(out, n, Ai, Aj, Av, Gi, Gj, Gv, IDv, Hi, Hj, Hv, &o);
+    }
+    auto *s = new fiim::Solver;
+    const int rc = s->create(n, Ai, Aj, Av, Gi, Gj, Gv, IDv, Hi, Hj, Hv, Li, Lj, Lv, Ui, Uj, Uv, o);
+    if (rc != FIIM_OK) {
+        s->destroy();
+        delete s;
+        return rc;
+    }
+    *out = reinterpret_cast<fiim_solver_t>(s);
+    return FIIM_OK;
+}
+
+int fiim_solver_solve(fiim_solver_t h, const double *b, double *x, double tol, int NMAX,
+                      fiim_result *res) {
+    if (!h || !b || !x) return fiim::set_error(FIIM_EARG, "null argument");
+    if (fiim_is_mixed(h)) return fiim_mixed_solve(h, b, x, tol, NMAX, res);
+    return reinterpret_cast<fiim::Solver *>(h)->solve(b, x, tol, NMAX, res);
+}
+
+int64_t fiim_solver_device_bytes(fiim_solver_t h) {
+    if (!h) return -1;
+    if (fiim_is_mixed(h)) return fiim_mixed_device_bytes(h);
+    return (int64_t) reinterpret_cast<fiim::Solver *>(h)->device_bytes();
+}
+
+int fiim_solver_spmv_shape(fiim_solver_t h, int which, int *vec) {
+    if (!h || !vec || fiim_is_mixed(h)) return fiim::set_error(FIIM_EARG, "bad handle");
+    auto *s = reinterpret_cast<fiim::Solver *>(h);
+    const fiim::DevCsr *m[] = {&s->A, &s->G, &s->H, &s->L, &s->U};
+    if (which < 0 || which > 4) return fiim::set_error(FIIM_EARG, "which in 0..4 (A, G, H, L, U)");
+    *vec = m[which]->vec;
+    return FIIM_OK;
+}
+
+int fiim_solver_destroy(fiim_solver_t h) {
+    if (!h) return FIIM_OK;
+    if (fiim_is_mixed(h)) return fiim_mixed_destroy(h);
+    auto *s = reinterpret_cast<fiim::Solver *>(h);
+    s->destroy();
+    delete s;
+    return FIIM_OK;
+}
+
+int fiim_spmv(int n, const int *Ai, const int *Aj, const double *Av, const double *x, double *y,
+              int vec, void *stream) {
+    return fiim::spmv_api(n, Ai, Aj, Av, x, y, vec, static_cast<cudaStream_t>(stream));
+}
+
+int fiim_prec_apply(int n, const int *Gi, const int *Gj, const double *Gv, const double *IDv,
+                    const int *Hi, const int *Hj, const double *Hv, const double *r, double *z,
+                    double *tm, void *stream) {
+    return fiim::prec_api(n, Gi, Gj, Gv, IDv, Hi, Hj, Hv, r, z, tm, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------
+// C++ overloads with the reference's signatures (mangled names match the reference's
+// libafiim.so exports). They throw std::runtime_error on a GPU-side failure, which the
+// reference's CPU code could not report.
+
+// AFIIM/src/bicgstab.hpp:82-100
+void EPBiCGSTAB(int n, double *Av, int *Aj, int *Ai, double *b, double tol, int NMAX, double *Gv,
+                int *Gj, int *Gi, double *IDv, double *Hv, int *Hj, int *Hi, double *x,
+                double *resval, int *iter, int verbose, int *info) {
+    throw_on(fiim_EPBiCGSTAB_afiim(n, Av, Aj, Ai, b, tol, NMAX, Gv, Gj, Gi, IDv, Hv, Hj, Hi, x,
+                                   resval, iter, verbose, info));
+}
+
+// ACIFIM/src/bicgstab.hpp:94-120
+void PBiCGSTAB(int n, double *Av, int *Aj, int *Ai, double *b, double tol, int NMAX, double *Gv,
+               int *Gj, int *Gi, double *IDv, double *Hv, int *Hj, int *Hi, double *Lv, int *Lj,
+               int *Li, double *Uv, int *Uj, int *Ui, int nr, char mode, double *x, double *resval,
+               int *iter, int verbose, int *info) {
+    throw_on(fiim_PBiCGSTAB_acifim(n, Av, Aj, Ai, b, tol, NMAX, Gv, Gj, Gi, IDv, Hv, Hj, Hi, Lv, Lj,
+                                   Li, Uv, Uj, Ui, nr, mode, x, resval, iter, verbose, info));
+}
+
+// PDFIIM/src/bicgstab.hpp:75-86 takes sparseMatrix<int,int,double>. This class has the
+// member layout of PDFIIM/src/sparseMatrix.hpp:68-75 (an ABI that must match for the
+// reference's callers to link), and the SYMMETRIC tag value of PDFIIM/src/constants.hpp.
+template <typename P, typename R, typename S>
+class sparseMatrix {
+public:
+    int stype;
+    int mtype;
+    std::vector<S> v;
+    std::vector<R> i, j;
+    P r, c, nnz;
+};
+
+void EPBiCGSTAB(sparseMatrix<int, int, double> &A, std::vector<double> &b, double tol, int NMAX,
+                sparseMatrix<int, int, double> &G, std::vector<double> &ID,
+                sparseMatrix<int, int, double> &H, std::vector<double> &x, double *resval,
+                int *iter, int verbose, int *info) {
+    constexpr int kSymmetricTag = 1;
+    const int issym = (A.mtype == kSymmetricTag);
+    const int n = A.r;
+    if ((int)x.size() < n || (int)b.size() < n || (int)ID.size() < n)
+        throw std::runtime_error("fiim_b200: vector sizes smaller than A.r");
+    throw_on(fiim_EPBiCGSTAB_pdfiim(n, issym, A.v.data(), A.j.data(), A.i.data(), b.data(), tol,
+                                    NMAX, G.v.data(), G.j.data(), G.i.data(), ID.data(),
+                                    issym ? nullptr : H.v.data(), issym ? nullptr : H.j.data(),
+                                    issym ? nullptr : H.i.data(), x.data(), resval, iter, verbose,
+                                    info));
+}

@@ -1,0 +1,67 @@
+// Internal declarations shared by the host-side translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+#include <cstdarg>
+#include <cstddef>
+#include <vector>
+
+#include "fiim_b200.h"
+
+namespace fiim {
+
+int set_error(int code, const char *fmt, ...);
+const char *last_error();
+int check_device(int *dev_out);
+int num_sms();
+
+#define FIIM_CUDA(call)                                                                   \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            cudaGetLastError();                                                           \
+            return ::fiim::set_error(FIIM_ECUDA, "%s: %s (%s:%d)", #call,                 \
+                                     cudaGetErrorString(e_), __FILE__, __LINE__);         \
+        }                                                                                 \
+    } while (0)
+
+#define FIIM_TRY(call)                      \
+    do {                                    \
+        int rc_ = (call);                   \
+        if (rc_ != FIIM_OK) return rc_;     \
+    } while (0)
+
+// One device allocation carved into 256-byte aligned pieces.
+struct Arena {
+    void *base = nullptr;
+    size_t cap = 0, used = 0;
+    int reserve(size_t bytes);   // ensure capacity (reallocates only to grow); resets use
+    void *take(size_t bytes);    // nullptr when exhausted
+    void release();
+    static size_t need(size_t bytes);
+};
+
+// A CSR matrix resident on the device. v holds FP64 values; v32 / v16 are optional
+// FP32 / BF16 copies for the mixed-precision inner solve.
+struct DevCsr {
+    long n = 0, nnz = 0;
+    int *rp = nullptr, *ci = nullptr;
+    double *v = nullptr;
+    float *v32 = nullptr;
+    __nv_bfloat16 *v16 = nullptr;
+    int vec = 8;                 // lanes per row of the SpMV
+    std::vector<long> sig;       // tuning-cache key: n, nnz, sampled row offsets
+};
+
+// Host CSR (owning), used for symmetric expansion and transposes.
+struct HostCsr {
+    int n = 0;
+    std::vector<int> rp, ci;
+    std::vector<double> v;
+};
+
+int heuristic_vec(long n, long nnz);
+
+}  // namespace fiim

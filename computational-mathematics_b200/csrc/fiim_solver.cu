@@ -1,0 +1,738 @@
+// Host side of the B200 solve phase: device layout, SpMV shape selection, the
+// device-driven iteration graph and the handle API of include/fiim_b200.h.
+//
+// Data layout in HBM (one solver, one arena allocation, 256-byte aligned pieces):
+//   A, G, H (L, U for ACIFIM mode 'C'): CSR with int32 row offsets and columns and
+//   FP64 values; for a symmetric PDFIIM input, A is expanded to full CSR and
+//   H = G^T is formed once at set-up (a gather-form CSR, no atomics in the solve).
+//   Vectors x, b, r, r0, p, v, s, t, pc, sc, tm (+ t1, t2, t3 for mode 'C'): FP64[n].
+//   DState (device scalars) and per-block reduction partials: a few KB.
+//   Mixed precision adds FP32 copies of A, G, H, D^{-1} and FP32 inner vectors.
+//
+// The solve is three launches: the fused start kernel (r = b - A x, r0, p, ||r0||),
+// one CUDA graph whose WHILE node runs the nine-kernel iteration body until the
+// device sets its condition to 0, and the FP64 true-residual kernel.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <iostream>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "fiim_b200.h"
+#include "fiim_internal.h"
+#include "fiim_kernels.cuh"
+#include "fiim_solver.h"
+
+namespace fiim {
+
+// ------------------------------------------------------------------ errors / device
+static thread_local std::string g_err;
+
+int set_error(int code, const char *fmt, ...) {
+    char buf[768];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+const char *last_error() { return g_err.c_str(); }
+
+int check_device(int *dev_out) {
+    int dev = 0, count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return set_error(FIIM_ENODEV, "no CUDA device visible");
+    }
+    FIIM_CUDA(cudaGetDevice(&dev));
+    int major = 0;
+    FIIM_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    if (major != 10)
+        return set_error(FIIM_ENODEV, "device %d has compute capability %d.x; this library is built for sm_100a",
+                         dev, major);
+    if (dev_out) *dev_out = dev;
+    return FIIM_OK;
+}
+
+int num_sms() {
+    static int sms[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!sms[dev]) cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+    return sms[dev] > 0 ? sms[dev] : 148;
+}
+
+// ------------------------------------------------------------------ arena
+int Arena::reserve(size_t bytes) {
+    used = 0;
+    if (bytes <= cap) return FIIM_OK;
+    release();
+    if (cudaMalloc(&base, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        base = nullptr;
+        return set_error(FIIM_ENOMEM, "cudaMalloc of %zu bytes failed", bytes);
+    }
+    cap = bytes;
+    return FIIM_OK;
+}
+
+void *Arena::take(size_t bytes) {
+    const size_t a = (used + 255) & ~size_t(255);
+    if (a + bytes > cap) return nullptr;
+    used = a + bytes;
+    return static_cast<char *>(base) + a;
+}
+
+void Arena::release() {
+    if (base) cudaFree(base);
+    base = nullptr;
+    cap = used = 0;
+}
+
+size_t Arena::need(size_t bytes) { return (bytes + 255) & ~size_t(255); }
+
+// ------------------------------------------------------------------ launch shapes
+// Resident blocks per SM of a kernel, cached by kernel address.
+template <typename K>
+int occupancy(K kernel) {
+    static std::mutex mu;
+    static std::map<const void *, int> occ;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = occ.find((const void *)kernel);
+    if (it != occ.end()) return it->second;
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kThreads, 0) != cudaSuccess || b < 1) {
+        cudaGetLastError();
+        b = 4;
+    }
+    occ[(const void *)kernel] = b;
+    return b;
+}
+
+// Grid: enough blocks for the work, capped at one full wave of resident blocks.
+template <typename K>
+int grid_for(K kernel, long units_per_block, long units) {
+    const long need = std::max<long>(1, (units + units_per_block - 1) / units_per_block);
+    return (int)std::min<long>(need, (long)occupancy(kernel) * num_sms());
+}
+
+template <int VEC, int FILL, typename V, typename Epi>
+static cudaError_t spmv_vec(cudaStream_t s, const CsrView<V> &M, const double *x, const Epi &epi,
+                            DState *st, double *partials) {
+    auto kern = k_spmv<VEC, V, Epi, FILL>;
+    const int g = grid_for(kern, (32 / VEC) * kWarps, M.n);
+    kern<<<g, kThreads, 0, s>>>(M, x, epi, st, partials);
+    return cudaGetLastError();
+}
+
+template <int FILL = 0, typename V, typename Epi>
+cudaError_t launch_spmv(int vec, cudaStream_t s, const CsrView<V> &M, const double *x,
+                        const Epi &epi, DState *st, double *partials) {
+    switch (vec) {
+        case 2: return spmv_vec<2, FILL>(s, M, x, epi, st, partials);
+        case 4: return spmv_vec<4, FILL>(s, M, x, epi, st, partials);
+        case 8: return spmv_vec<8, FILL>(s, M, x, epi, st, partials);
+        case 16: return spmv_vec<16, FILL>(s, M, x, epi, st, partials);
+        default: return spmv_vec<32, FILL>(s, M, x, epi, st, partials);
+    }
+}
+
+template <typename K>
+static int stream_grid(K kernel, long n) { return grid_for(kernel, kThreads, n); }
+
+int heuristic_vec(long n, long nnz) {
+    const double mean = n > 0 ? (double)nnz / (double)n : 1.0;
+    int v = 2;
+    while (v < 32 && v < mean) v <<= 1;
+    return v;
+}
+
+static CsrView<double> view(const DevCsr &M) { return CsrView<double>{M.rp, M.ci, M.v, (int)M.n}; }
+
+// Time each lane count on this matrix and keep the fastest; cached by signature.
+static int autotune_vec(const DevCsr &M, const double *x, double *y, cudaStream_t s) {
+    static std::mutex mu;
+    static std::map<std::vector<long>, int> cache;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = cache.find(M.sig);
+        if (it != cache.end()) return it->second;
+    }
+    const int cands[5] = {2, 4, 8, 16, 32};
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int best = heuristic_vec(M.n, M.nnz);
+    float best_ms = 1e30f;
+    const int reps = M.nnz > 4000000 ? 3 : 8;
+    for (int c : cands) {
+        launch_spmv(c, s, view(M), x, EpiStore{y}, nullptr, nullptr);
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < reps; ++r) launch_spmv(c, s, view(M), x, EpiStore{y}, nullptr, nullptr);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms * 0.97f) {
+            best_ms = ms;
+            best = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaGetLastError();
+    std::lock_guard<std::mutex> lk(mu);
+    cache[M.sig] = best;
+    return best;
+}
+
+// ------------------------------------------------------------------ host CSR helpers
+// Full CSR of a symmetric matrix given by its stored upper triangle (entries with
+// col < row are ignored, as MKL's SYMMETRIC + UPPER descriptor does).
+static void expand_sym_upper(int n, const int *rp, const int *ci, const double *v, HostCsr &out) {
+    out.n = n;
+    out.rp.assign(n + 1, 0);
+    for (int i = 0; i < n; ++i)
+        for (int k = rp[i]; k < rp[i + 1]; ++k) {
+            const int j = ci[k];
+            if (j < i) continue;
+            out.rp[i + 1]++;
+            if (j != i) out.rp[j + 1]++;
+        }
+    for (int i = 0; i < n; ++i) out.rp[i + 1] += out.rp[i];
+    out.ci.resize(out.rp[n]);
+    out.v.resize(out.rp[n]);
+    std::vector<int> pos(out.rp.begin(), out.rp.end() - 1);
+    // Mirrored (lower) entries first: row j receives (j, i) for i < j in increasing i,
+    // then its own upper entries in stored order, so columns stay ascending.
+    std::vector<int> lower_count(n, 0);
+    for (int i = 0; i < n; ++i)
+        for (int k = rp[i]; k < rp[i + 1]; ++k)
+            if (ci[k] > i) lower_count[ci[k]]++;
+    std::vector<int> upos(n);
+    for (int i = 0; i < n; ++i) upos[i] = out.rp[i] + lower_count[i];
+    for (int i = 0; i < n; ++i)
+        for (int k = rp[i]; k < rp[i + 1]; ++k) {
+            const int j = ci[k];
+            if (j < i) continue;
+            out.ci[upos[i]] = j;
+            out.v[upos[i]++] = v[k];
+            if (j != i) {
+                out.ci[pos[j]] = i;
+                out.v[pos[j]++] = v[k];
+            }
+        }
+}
+
+// CSR of T^T where T is the upper triangle (col >= row) of (rp, ci, v).
+static void transpose_upper(int n, const int *rp, const int *ci, const double *v, HostCsr &out) {
+    out.n = n;
+    out.rp.assign(n + 1, 0);
+    for (int i = 0; i < n; ++i)
+        for (int k = rp[i]; k < rp[i + 1]; ++k)
+            if (ci[k] >= i) out.rp[ci[k] + 1]++;
+    for (int i = 0; i < n; ++i) out.rp[i + 1] += out.rp[i];
+    out.ci.resize(out.rp[n]);
+    out.v.resize(out.rp[n]);
+    std::vector<int> pos(out.rp.begin(), out.rp.end() - 1);
+    for (int i = 0; i < n; ++i)
+        for (int k = rp[i]; k < rp[i + 1]; ++k)
+            if (ci[k] >= i) {
+                out.ci[pos[ci[k]]] = i;
+                out.v[pos[ci[k]]++] = v[k];
+            }
+}
+
+static void signature(DevCsr &M, const int *host_rp) {
+    M.sig.clear();
+    M.sig.push_back(M.n);
+    M.sig.push_back(M.nnz);
+    const long step = std::max<long>(1, M.n / 64);
+    for (long i = 0; i <= M.n; i += step) M.sig.push_back(host_rp[i]);
+    M.sig.push_back(host_rp[M.n]);
+}
+
+// Upload one CSR matrix into pre-carved buffers (capacity nnz_cap) and apply MKL's
+// TRIANGULAR fill semantics: fill 1 keeps col >= row, fill 2 keeps col <= row
+// (AFIIM/src/bicgstab.cpp:140-147). The check runs on the device; the rare matrix
+// with entries outside its triangle is compacted on the host.
+static int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, const double *v,
+                      int fill, bool device_src, cudaStream_t s, unsigned long long *d_count,
+                      unsigned long long *h_count) {
+    M.n = n;
+    long nnz;
+    std::vector<int> hrp;
+    if (device_src) {
+        hrp.resize(n + 1);
+        FIIM_CUDA(cudaMemcpyAsync(hrp.data(), rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
+        FIIM_CUDA(cudaStreamSynchronize(s));
+        nnz = hrp[n];
+    } else {
+        nnz = rp[n];
+    }
+    if (nnz > nnz_cap) return set_error(FIIM_EARG, "matrix has %ld entries, capacity %ld", nnz, nnz_cap);
+    if (nnz < 0) return set_error(FIIM_EARG, "negative row offset at n");
+    M.nnz = nnz;
+    const cudaMemcpyKind kind = device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    FIIM_CUDA(cudaMemcpyAsync(M.rp, rp, sizeof(int) * (n + 1), kind, s));
+    if (nnz > 0) {
+        FIIM_CUDA(cudaMemcpyAsync(M.ci, ci, sizeof(int) * nnz, kind, s));
+        FIIM_CUDA(cudaMemcpyAsync(M.v, v, sizeof(double) * nnz, kind, s));
+    }
+    signature(M, device_src ? hrp.data() : rp);
+    if (fill == 0 || nnz == 0) return FIIM_OK;
+    FIIM_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s));
+    const int g = std::min(num_sms() * 8, std::max(1, (n + kThreads - 1) / kThreads));
+    k_count_outside<<<g, kThreads, 0, s>>>(n, M.rp, M.ci, fill == 1, d_count);
+    FIIM_CUDA(cudaGetLastError());
+    FIIM_CUDA(cudaMemcpyAsync(h_count, d_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    FIIM_CUDA(cudaStreamSynchronize(s));
+    if (*h_count == 0) return FIIM_OK;
+    std::vector<int> crp(n + 1), cci(nnz);
+    std::vector<double> cv(nnz);
+    FIIM_CUDA(cudaMemcpy(crp.data(), M.rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+    FIIM_CUDA(cudaMemcpy(cci.data(), M.ci, sizeof(int) * nnz, cudaMemcpyDeviceToHost));
+    FIIM_CUDA(cudaMemcpy(cv.data(), M.v, sizeof(double) * nnz, cudaMemcpyDeviceToHost));
+    long c = 0;
+    std::vector<int> nrp(n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+        for (int k = crp[i]; k < crp[i + 1]; ++k) {
+            const int j = cci[k];
+            if ((fill == 1) ? (j >= i) : (j <= i)) {
+                cci[c] = j;
+                cv[c] = cv[k];
+                ++c;
+            }
+        }
+        nrp[i + 1] = (int)c;
+    }
+    M.nnz = c;
+    FIIM_CUDA(cudaMemcpy(M.rp, nrp.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice));
+    if (c > 0) {
+        FIIM_CUDA(cudaMemcpy(M.ci, cci.data(), sizeof(int) * c, cudaMemcpyHostToDevice));
+        FIIM_CUDA(cudaMemcpy(M.v, cv.data(), sizeof(double) * c, cudaMemcpyHostToDevice));
+    }
+    signature(M, nrp.data());
+    return FIIM_OK;
+}
+
+static int carve_csr(Arena &ar, DevCsr &M, long n, long nnz) {
+    M.rp = static_cast<int *>(ar.take(sizeof(int) * (n + 1)));
+    M.ci = static_cast<int *>(ar.take(sizeof(int) * std::max<long>(nnz, 1)));
+    M.v = static_cast<double *>(ar.take(sizeof(double) * std::max<long>(nnz, 1)));
+    if (!M.rp || !M.ci || !M.v) return set_error(FIIM_ENOMEM, "arena exhausted");
+    return FIIM_OK;
+}
+
+static size_t csr_bytes(long n, long nnz) {
+    return Arena::need(sizeof(int) * (n + 1)) + Arena::need(sizeof(int) * std::max<long>(nnz, 1)) +
+           Arena::need(sizeof(double) * std::max<long>(nnz, 1));
+}
+
+// ------------------------------------------------------------------ preconditioner
+// out = M in for the chosen preconditioner; the last product's epilogue stores the
+// result and, when `norm`, also accumulates ||out||^2 into st->pc2.
+int Solver::enqueue_prec(const double *in, double *out, bool norm) {
+    cudaStream_t s = stream;
+    const bool combined = (opt.variant == FIIM_ACIFIM && opt.mode == 'C' && opt.nr > 1);
+    if (!combined) {
+        // tm = IDv o (H in); out = G tm   (AFIIM/src/bicgstab.cpp:172-175)
+        FIIM_CUDA(launch_spmv(H.vec, s, view(H), in, EpiScale{tm, IDv}, st, partials));
+        if (norm) FIIM_CUDA(launch_spmv(G.vec, s, view(G), tm, EpiNorm{out}, st, partials));
+        else FIIM_CUDA(launch_spmv(G.vec, s, view(G), tm, EpiStore{out}, st, partials));
+        return FIIM_OK;
+    }
+    // ACIFIM apply() mode 'C' (ACIFIM/src/bicgstab.cpp:395-404,408,411-420).
+    FIIM_CUDA(launch_spmv(H.vec, s, view(H), in, EpiStore{t1}, st, partials));
+    for (int it = 1; it < opt.nr; ++it) {
+        FIIM_CUDA(launch_spmv(L.vec, s, view(L), t1, EpiSubFrom{t3, in}, st, partials));
+        if (it == opt.nr - 1)
+            FIIM_CUDA(launch_spmv(H.vec, s, view(H), t3, EpiAccumScale{t1, t2, IDv}, st, partials));
+        else
+            FIIM_CUDA(launch_spmv(H.vec, s, view(H), t3, EpiAccum{t1}, st, partials));
+    }
+    FIIM_CUDA(launch_spmv(G.vec, s, view(G), t2, EpiStore{out}, st, partials));
+    for (int it = 1; it < opt.nr; ++it) {
+        FIIM_CUDA(launch_spmv(U.vec, s, view(U), out, EpiSubFrom{t3, t2}, st, partials));
+        if (it == opt.nr - 1 && norm)
+            FIIM_CUDA(launch_spmv(G.vec, s, view(G), t3, EpiAccumNorm{out}, st, partials));
+        else
+            FIIM_CUDA(launch_spmv(G.vec, s, view(G), t3, EpiAccum{out}, st, partials));
+    }
+    return FIIM_OK;
+}
+
+int Solver::kernels_per_iteration() const {
+    const bool combined = (opt.variant == FIIM_ACIFIM && opt.mode == 'C' && opt.nr > 1);
+    const int prec = combined ? 2 + 4 * (opt.nr - 1) : 2;
+    return 2 * prec + 5;
+}
+
+// One BiCGSTAB iteration (AFIIM/src/bicgstab.cpp:170-274) as launches on `stream`.
+int Solver::enqueue_iteration(bool cond, cudaGraphConditionalHandle h) {
+    cudaStream_t s = stream;
+    const long nn = n;
+    FIIM_TRY(enqueue_prec(p, pc, true));                                             // K1-K2
+    FIIM_CUDA(launch_spmv(A.vec, s, view(A), pc, EpiAlpha{v, r0}, st, partials));     // K3
+    k_update_s<<<stream_grid(k_update_s, nn), kThreads, 0, s>>>(nn, r, v, x, sv, st, partials);  // K4
+    FIIM_CUDA(cudaGetLastError());
+    FIIM_TRY(enqueue_prec(sv, sc, false));                                           // K5-K6
+    FIIM_CUDA(launch_spmv(A.vec, s, view(A), sc, EpiOmega{t, sv}, st, partials));    // K7
+    k_update_xr<<<stream_grid(k_update_xr, nn), kThreads, 0, s>>>(nn, pc, sc, sv, t, r0, x, r, st,
+                                                                  partials);          // K8
+    FIIM_CUDA(cudaGetLastError());
+    k_update_p<<<stream_grid(k_update_p, nn), kThreads, 0, s>>>(nn, r, v, p, st, h, cond ? 1 : 0);  // K9
+    FIIM_CUDA(cudaGetLastError());
+    return FIIM_OK;
+}
+
+int Solver::build_graph() {
+    if (exec) {
+        cudaGraphExecDestroy(exec);
+        exec = nullptr;
+    }
+    if (graph) {
+        cudaGraphDestroy(graph);
+        graph = nullptr;
+    }
+    use_cond = false;
+    // Preferred: one graph whose WHILE node repeats the iteration body on the device.
+    do {
+        cudaGraph_t g = nullptr;
+        if (cudaGraphCreate(&g, 0) != cudaSuccess) break;
+        cudaGraphConditionalHandle h;
+        if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+            cudaGraphDestroy(g);
+            break;
+        }
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (cudaGraphAddNode(&node, g, nullptr, 0, &cp) != cudaSuccess) {
+            cudaGraphDestroy(g);
+            break;
+        }
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        if (cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGraphDestroy(g);
+            break;
+        }
+        const int rc = enqueue_iteration(true, h);
+        cudaGraph_t captured = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(stream, &captured);
+        if (rc != FIIM_OK || ec != cudaSuccess) {
+            cudaGraphDestroy(g);
+            break;
+        }
+        cudaGraphExec_t e = nullptr;
+        if (cudaGraphInstantiate(&e, g, 0) != cudaSuccess) {
+            cudaGraphDestroy(g);
+            break;
+        }
+        graph = g;
+        exec = e;
+        use_cond = true;
+    } while (0);
+    cudaGetLastError();
+    if (use_cond) return FIIM_OK;
+    // Fallback: a graph of one iteration, relaunched by the host until done.
+    FIIM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue_iteration(false, cudaGraphConditionalHandle{});
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(stream, &g);
+    if (rc != FIIM_OK) return rc;
+    FIIM_CUDA(ec);
+    FIIM_CUDA(cudaGraphInstantiate(&exec, g, 0));
+    graph = g;
+    return FIIM_OK;
+}
+
+// ------------------------------------------------------------------ set-up
+int Solver::create(int n_, const int *Ai, const int *Aj, const double *Av, const int *Gi,
+                   const int *Gj, const double *Gv, const double *IDv_, const int *Hi,
+                   const int *Hj, const double *Hv, const int *Li, const int *Lj, const double *Lv,
+                   const int *Ui, const int *Uj, const double *Uv, const fiim_options &o) {
+    opt = o;
+    n = n_;
+    if (n <= 0 || !Ai || !Aj || !Av || !Gi || !Gj || !Gv || !IDv_)
+        return set_error(FIIM_EARG, "null array or n <= 0");
+    if (opt.variant < FIIM_AFIIM || opt.variant > FIIM_ACIFIM) return set_error(FIIM_EARG, "bad variant");
+    if (opt.issym && opt.variant != FIIM_PDFIIM) return set_error(FIIM_EARG, "issym is a PDFIIM input form");
+    if (opt.variant == FIIM_ACIFIM && opt.mode != 'E' && opt.mode != 'C')
+        return set_error(FIIM_EARG, "ACIFIM mode '%c' is not the factored-inverse product (only 'E' and 'C')", opt.mode);
+    const bool combined = (opt.variant == FIIM_ACIFIM && opt.mode == 'C' && opt.nr > 1);
+    if (!opt.issym && (!Hi || !Hj || !Hv)) return set_error(FIIM_EARG, "H is required");
+    if (combined && (!Li || !Lj || !Lv || !Ui || !Uj || !Uv)) return set_error(FIIM_EARG, "mode 'C' needs L and U");
+    if (opt.precision != FIIM_FP64) return set_error(FIIM_EARG, "mixed precision is served by fiim_mixed_*");
+    FIIM_TRY(check_device(&device));
+    if (!stream) FIIM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    const bool dev_src = (opt.memory == FIIM_MEM_DEVICE);
+
+    // Host-side forms needed for symmetric input: full A and G^T.
+    HostCsr Afull, Gt;
+    std::vector<int> hA_rp, hA_ci, hG_rp, hG_ci;
+    std::vector<double> hA_v, hG_v;
+    const int *aRp = Ai, *aCi = Aj, *hRp = Hi, *hCi = Hj;
+    const double *aV = Av, *hV = Hv;
+    bool a_dev = dev_src, h_dev = dev_src;
+    if (opt.issym) {
+        auto fetch = [&](const int *rp, const int *ci, const double *v, std::vector<int> &orp,
+                         std::vector<int> &oci, std::vector<double> &ov) -> int {
+            orp.resize(n + 1);
+            if (dev_src) FIIM_CUDA(cudaMemcpy(orp.data(), rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+            else std::memcpy(orp.data(), rp, sizeof(int) * (n + 1));
+            const long z = orp[n];
+            oci.resize(z);
+            ov.resize(z);
+            if (dev_src) {
+                FIIM_CUDA(cudaMemcpy(oci.data(), ci, sizeof(int) * z, cudaMemcpyDeviceToHost));
+                FIIM_CUDA(cudaMemcpy(ov.data(), v, sizeof(double) * z, cudaMemcpyDeviceToHost));
+            } else {
+                std::memcpy(oci.data(), ci, sizeof(int) * z);
+                std::memcpy(ov.data(), v, sizeof(double) * z);
+            }
+            return FIIM_OK;
+        };
+        FIIM_TRY(fetch(Ai, Aj, Av, hA_rp, hA_ci, hA_v));
+        FIIM_TRY(fetch(Gi, Gj, Gv, hG_rp, hG_ci, hG_v));
+        expand_sym_upper(n, hA_rp.data(), hA_ci.data(), hA_v.data(), Afull);
+        transpose_upper(n, hG_rp.data(), hG_ci.data(), hG_v.data(), Gt);
+        aRp = Afull.rp.data(); aCi = Afull.ci.data(); aV = Afull.v.data(); a_dev = false;
+        hRp = Gt.rp.data(); hCi = Gt.ci.data(); hV = Gt.v.data(); h_dev = false;
+    }
+    auto nnz_of = [&](const int *rp, bool dev) -> long {
+        if (!dev) return rp[n];
+        int z = 0;
+        if (cudaMemcpy(&z, rp + n, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+        return z;
+    };
+    const long nA = nnz_of(aRp, a_dev), nG = nnz_of(Gi, dev_src), nH = nnz_of(hRp, h_dev);
+    const long nL = combined ? nnz_of(Li, dev_src) : 0, nU = combined ? nnz_of(Ui, dev_src) : 0;
+    if (nA < 0 || nG < 0 || nH < 0 || nL < 0 || nU < 0) return set_error(FIIM_ECUDA, "reading row offsets failed");
+
+    const int nvec = combined ? 14 : 11;
+    size_t bytes = csr_bytes(n, nA) + csr_bytes(n, nG) + csr_bytes(n, nH);
+    if (combined) bytes += csr_bytes(n, nL) + csr_bytes(n, nU);
+    bytes += (size_t)(nvec + 1) * Arena::need(sizeof(double) * n);
+    const int max_blocks = num_sms() * 32;
+    bytes += Arena::need(sizeof(DState)) + Arena::need(sizeof(double) * 4 * max_blocks) + 1024;
+    FIIM_TRY(arena.reserve(bytes));
+    FIIM_TRY(carve_csr(arena, A, n, nA));
+    FIIM_TRY(carve_csr(arena, G, n, nG));
+    FIIM_TRY(carve_csr(arena, H, n, nH));
+    if (combined) {
+        FIIM_TRY(carve_csr(arena, L, n, nL));
+        FIIM_TRY(carve_csr(arena, U, n, nU));
+    }
+    capA = nA; capG = nG; capH = nH; capL = nL; capU = nU;
+    double **vecs[] = {&IDv, &x, &b, &r, &r0, &p, &v, &sv, &t, &pc, &sc, &tm, &t1, &t2, &t3};
+    for (int k = 0; k < nvec + 1; ++k) {
+        *vecs[k] = static_cast<double *>(arena.take(sizeof(double) * n));
+        if (!*vecs[k]) return set_error(FIIM_ENOMEM, "arena exhausted");
+    }
+    st = static_cast<DState *>(arena.take(sizeof(DState)));
+    partials = static_cast<double *>(arena.take(sizeof(double) * 4 * max_blocks));
+    d_count = static_cast<unsigned long long *>(arena.take(sizeof(unsigned long long)));
+    if (!st || !partials || !d_count) return set_error(FIIM_ENOMEM, "arena exhausted");
+    if (!hst) FIIM_CUDA(cudaHostAlloc(&hst, sizeof(DState) + 64, cudaHostAllocDefault));
+    h_count = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(hst) + sizeof(DState) + 32);
+    FIIM_CUDA(cudaMemsetAsync(st, 0, sizeof(DState), stream));
+
+    FIIM_TRY(upload_csr(A, capA, n, aRp, aCi, aV, 0, a_dev, stream, d_count, h_count));
+    FIIM_TRY(upload_csr(G, capG, n, Gi, Gj, Gv, 1, dev_src, stream, d_count, h_count));
+    FIIM_TRY(upload_csr(H, capH, n, hRp, hCi, hV, 2, h_dev, stream, d_count, h_count));
+    if (combined) {
+        FIIM_TRY(upload_csr(L, capL, n, Li, Lj, Lv, 2, dev_src, stream, d_count, h_count));
+        FIIM_TRY(upload_csr(U, capU, n, Ui, Uj, Uv, 1, dev_src, stream, d_count, h_count));
+    }
+    FIIM_CUDA(cudaMemcpyAsync(IDv, IDv_, sizeof(double) * n,
+                              dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
+    FIIM_CUDA(cudaStreamSynchronize(stream));
+
+    DevCsr *mats[] = {&A, &G, &H, &L, &U};
+    for (int k = 0; k < (combined ? 5 : 3); ++k) {
+        DevCsr &M = *mats[k];
+        M.vec = heuristic_vec(M.n, M.nnz);
+        if (opt.autotune) {
+            FIIM_CUDA(cudaMemsetAsync(tm, 0, sizeof(double) * n, stream));
+            M.vec = autotune_vec(M, tm, t, stream);
+        }
+    }
+    FIIM_CUDA(cudaStreamSynchronize(stream));
+    FIIM_TRY(build_graph());
+    if (!ev0) {
+        FIIM_CUDA(cudaEventCreate(&ev0));
+        FIIM_CUDA(cudaEventCreate(&ev1));
+    }
+    return FIIM_OK;
+}
+
+// Refill the values of an existing solver (same sizes); the graph stays valid because
+// every buffer keeps its address.
+int Solver::reload(const int *Ai, const int *Aj, const double *Av, const int *Gi, const int *Gj,
+                   const double *Gv, const double *IDv_, const int *Hi, const int *Hj,
+                   const double *Hv, const int *Li, const int *Lj, const double *Lv, const int *Ui,
+                   const int *Uj, const double *Uv) {
+    FIIM_CUDA(cudaSetDevice(device));
+    const bool dev_src = (opt.memory == FIIM_MEM_DEVICE);
+    const bool combined = (opt.variant == FIIM_ACIFIM && opt.mode == 'C' && opt.nr > 1);
+    if (opt.issym) return set_error(FIIM_EARG, "reload does not serve symmetric input");
+    FIIM_TRY(upload_csr(A, capA, n, Ai, Aj, Av, 0, dev_src, stream, d_count, h_count));
+    FIIM_TRY(upload_csr(G, capG, n, Gi, Gj, Gv, 1, dev_src, stream, d_count, h_count));
+    FIIM_TRY(upload_csr(H, capH, n, Hi, Hj, Hv, 2, dev_src, stream, d_count, h_count));
+    if (combined) {
+        FIIM_TRY(upload_csr(L, capL, n, Li, Lj, Lv, 2, dev_src, stream, d_count, h_count));
+        FIIM_TRY(upload_csr(U, capU, n, Ui, Uj, Uv, 1, dev_src, stream, d_count, h_count));
+    }
+    FIIM_CUDA(cudaMemcpyAsync(IDv, IDv_, sizeof(double) * n,
+                              dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
+    return FIIM_OK;
+}
+
+// ------------------------------------------------------------------ solve
+int Solver::solve(const double *b_in, double *x_io, double tol, int nmax, fiim_result *res) {
+    FIIM_CUDA(cudaSetDevice(device));
+    const bool dev_src = (opt.memory == FIIM_MEM_DEVICE);
+    const cudaMemcpyKind in_kind = dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind out_kind = dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    FIIM_CUDA(cudaMemcpyAsync(b, b_in, sizeof(double) * n, in_kind, stream));
+    FIIM_CUDA(cudaMemcpyAsync(x, x_io, sizeof(double) * n, in_kind, stream));
+
+    DState h = {};
+    h.tol = tol;
+    h.eps = 1.11022302462516e-16;                                    // AFIIM/src/bicgstab.cpp:108
+    h.nmax = nmax;
+    h.info = -1;
+    if (opt.variant == FIIM_ACIFIM) h.maxmsteps = std::min(std::max(n, 2000) / 50, 40);  // ACIFIM :132
+    else h.maxmsteps = std::min(std::max(n, 500) / 50, 20);                               // AFIIM :114
+    h.alpha_guard = (opt.variant == FIIM_ACIFIM);
+    *hst = h;
+    FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
+    FIIM_CUDA(cudaEventRecord(ev0, stream));
+    // Start: r = b - A x, r0 = r, p = r, ro = ||r0|| (AFIIM/src/bicgstab.cpp:151-165).
+    FIIM_CUDA(launch_spmv(A.vec, stream, view(A), x, EpiInit{b, p, r0, r}, st, partials));
+    int launches = 1;
+    if (use_cond) {
+        FIIM_CUDA(cudaGraphLaunch(exec, stream));
+    } else {
+        // Host-driven fallback: launch ahead in growing chunks; kernels of iterations
+        // past termination return at once.
+        int launched = 0, chunk = 1;
+        for (;;) {
+            for (int k = 0; k < chunk; ++k) FIIM_CUDA(cudaGraphLaunch(exec, stream));
+            launched += chunk;
+            FIIM_CUDA(cudaMemcpyAsync(&hst->done, &st->done, sizeof(int), cudaMemcpyDeviceToHost, stream));
+            FIIM_CUDA(cudaStreamSynchronize(stream));
+            if (hst->done) break;
+            if (launched > std::max(nmax, 0) + 2)
+                return set_error(FIIM_ETIMEOUT, "solve not finished after %d iterations", launched);
+            chunk = std::min(chunk * 2, 16);
+        }
+        hst->loops = launched;
+    }
+    // FP64 true residual ||b - A x|| / ||b||.
+    FIIM_CUDA(launch_spmv(A.vec, stream, view(A), x, EpiResid{b, nullptr}, st, partials));
+    launches += 1;
+    FIIM_CUDA(cudaEventRecord(ev1, stream));
+    const int fallback_loops = hst->loops;
+    FIIM_CUDA(cudaMemcpyAsync(hst, st, sizeof(DState), cudaMemcpyDeviceToHost, stream));
+    FIIM_CUDA(cudaMemcpyAsync(x_io, x, sizeof(double) * n, out_kind, stream));
+    FIIM_CUDA(cudaStreamSynchronize(stream));
+    if (!use_cond) hst->loops = fallback_loops;
+    float ms = 0.f;
+    FIIM_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+    if (hst->info == -5) return set_error(FIIM_ETIMEOUT, "device loop guard tripped");
+    launches += hst->loops * kernels_per_iteration();
+    last_launches = launches;
+    if (res) {
+        res->resval = hst->rc / hst->ro;
+        res->true_relres = std::sqrt(hst->ts) / std::sqrt(hst->tt);
+        res->iter = hst->iter;
+        res->info = hst->info;
+        res->refine_steps = 0;
+        res->device_ms = ms;
+        res->launches = launches;
+    }
+    if (opt.verbose) print_status(hst->info, hst->iter, hst->rc / hst->ro);
+    return FIIM_OK;
+}
+
+// The reference's termination messages (AFIIM/src/bicgstab.cpp:227-252,279-280;
+// PDFIIM prints its divergence text on stagnation too, PDFIIM/src/bicgstab.cpp:257-261).
+void Solver::print_status(int info, int iter, double rel) const {
+    if (info == 1 || (info == 2 && opt.variant == FIIM_PDFIIM)) {
+        std::cout << "BiCGSTAB diverged and iterations stopped with relative residual " << rel
+                  << " in iteration " << iter << "\n";
+        std::cout << "Try to increase the quality of preconditioning\n";
+    } else if (info == 2) {
+        std::cout << "BiCGSTAB stagnated with relative residual " << rel << " in iteration " << iter << "\n";
+        std::cout << "Try increasing prescribed tolerance\n";
+    } else if (info == 0) {
+        std::cout << "Convergence in " << iter << " iterations with relative residual " << rel << "\n";
+    }
+    if (info == 3)
+        std::cout << "Convergence failed after " << iter << " iterations with relative residual " << rel << "\n";
+}
+
+void Solver::destroy() {
+    if (device >= 0) cudaSetDevice(device);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    ev0 = ev1 = nullptr;
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+    if (hst) cudaFreeHost(hst);
+    hst = nullptr;
+    arena.release();
+}
+
+// ------------------------------------------------------------------ kernel-level API
+int spmv_api(int n, const int *Ai, const int *Aj, const double *Av, const double *x, double *y,
+             int vec, cudaStream_t s) {
+    if (n <= 0 || !Ai || !Aj || !Av || !x || !y) return set_error(FIIM_EARG, "null array or n <= 0");
+    FIIM_TRY(check_device(nullptr));
+    if (vec != 2 && vec != 4 && vec != 8 && vec != 16 && vec != 32) {
+        int z = 0;
+        FIIM_CUDA(cudaMemcpyAsync(&z, Ai + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+        FIIM_CUDA(cudaStreamSynchronize(s));
+        vec = heuristic_vec(n, z);
+    }
+    FIIM_CUDA(launch_spmv(vec, s, CsrView<double>{Ai, Aj, Av, n}, x, EpiStore{y}, nullptr, nullptr));
+    return FIIM_OK;
+}
+
+int prec_api(int n, const int *Gi, const int *Gj, const double *Gv, const double *IDv_, const int *Hi,
+             const int *Hj, const double *Hv, const double *rr, double *z, double *tmv, cudaStream_t s) {
+    if (n <= 0 || !Gi || !Gj || !Gv || !IDv_ || !Hi || !Hj || !Hv || !rr || !z || !tmv)
+        return set_error(FIIM_EARG, "null array or n <= 0");
+    FIIM_TRY(check_device(nullptr));
+    int zz[2] = {0, 0};
+    FIIM_CUDA(cudaMemcpyAsync(&zz[0], Gi + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FIIM_CUDA(cudaMemcpyAsync(&zz[1], Hi + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FIIM_CUDA(cudaStreamSynchronize(s));
+    FIIM_CUDA(launch_spmv<2>(heuristic_vec(n, zz[1]), s, CsrView<double>{Hi, Hj, Hv, n}, rr,
+                             EpiScale{tmv, IDv_}, nullptr, nullptr));
+    FIIM_CUDA(launch_spmv<1>(heuristic_vec(n, zz[0]), s, CsrView<double>{Gi, Gj, Gv, n}, tmv,
+                             EpiStore{z}, nullptr, nullptr));
+    return FIIM_OK;
+}
+
+}  // namespace fiim

@@ -1,0 +1,341 @@
+"""Python mirror of the reference's solve-phase interface over libfiim_b200.so.
+
+The functions keep the reference's names, argument meaning and in/out convention:
+
+* ``EPBiCGSTAB``        — AFIIM/src/bicgstab.hpp:82-100 (pointer form)
+* ``EPBiCGSTAB_pdfiim`` — PDFIIM/src/bicgstab.hpp:75-86 (sparseMatrix form, as CSR arrays)
+* ``PBiCGSTAB``         — ACIFIM/src/bicgstab.hpp:94-120 (modes 'E' and 'C')
+
+``x`` is the initial guess in and the solution out (updated in place); the scalars come
+back as ``(resval, iter, info)`` with the reference's ``info`` codes (0 converged,
+1 diverged, 2 stagnated, 3 NMAX). A GPU-side failure raises ``FiimError``; there is no
+CPU fallback.
+
+``Solver`` wraps the handle API (set up once, solve many times) for host (numpy) or
+device (torch CUDA tensor) arrays. Generators and the host PDFIIM construction are
+exposed for tests and benchmarks.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfiim_b200.so")
+
+FIIM_OK, FIIM_EARG, FIIM_ECUDA, FIIM_ENOMEM, FIIM_ENODEV, FIIM_ETIMEOUT = 0, -1, -2, -3, -4, -5
+AFIIM, PDFIIM, ACIFIM = 0, 1, 2
+FP64, MIXED_FP32, MIXED_BF16 = 0, 1, 2
+MEM_HOST, MEM_DEVICE = 0, 1
+_VARIANTS = {"afiim": AFIIM, "pdfiim": PDFIIM, "acifim": ACIFIM}
+_PRECISIONS = {"fp64": FP64, "fp32": MIXED_FP32, "bf16": MIXED_BF16}
+
+# Every extern "C" symbol include/fiim_b200.h declares.
+EXPORTS = (
+    "fiim_last_error", "fiim_options_default", "fiim_EPBiCGSTAB_afiim", "fiim_EPBiCGSTAB_pdfiim",
+    "fiim_PBiCGSTAB_acifim", "fiim_solver_create", "fiim_solver_solve", "fiim_solver_device_bytes",
+    "fiim_solver_spmv_shape", "fiim_solver_destroy", "fiim_spmv", "fiim_prec_apply",
+    "fiim_gen_poisson2d", "fiim_gen_convdiff3d", "fiim_gen_convdiff2d", "fiim_gen_batch_params",
+    "fiim_gen_zipf", "fiim_gen_zipf_mean", "fiim_rand_normal", "fiim_model_rhs", "fiim_pdfiim_build",
+)
+
+
+class FiimError(RuntimeError):
+    def __init__(self, rc: int, msg: str):
+        super().__init__(f"fiim_b200 error {rc}: {msg}")
+        self.rc = rc
+
+
+class Options(C.Structure):
+    _fields_ = [("variant", C.c_int), ("issym", C.c_int), ("precision", C.c_int), ("memory", C.c_int),
+                ("mode", C.c_char), ("nr", C.c_int), ("autotune", C.c_int), ("verbose", C.c_int),
+                ("inner_tol", C.c_double), ("inner_nmax", C.c_int), ("max_refine", C.c_int)]
+
+
+class Result(C.Structure):
+    _fields_ = [("resval", C.c_double), ("true_relres", C.c_double), ("iter", C.c_int), ("info", C.c_int),
+                ("refine_steps", C.c_int), ("device_ms", C.c_double), ("launches", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libfiim_b200.so (raises if it was not built: there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} not built; run `make -C {HERE}`")
+        L = C.CDLL(LIB_PATH, mode=os.RTLD_LOCAL)
+        L.fiim_last_error.restype = C.c_char_p
+        L.fiim_solver_device_bytes.restype = C.c_int64
+        for name in ("fiim_gen_poisson2d", "fiim_gen_convdiff3d", "fiim_gen_convdiff2d", "fiim_gen_zipf"):
+            getattr(L, name).restype = C.c_long
+        L.fiim_gen_zipf_mean.restype = C.c_double
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != FIIM_OK:
+        raise FiimError(rc, lib().fiim_last_error().decode())
+
+
+def _i(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _ptr(a):
+    """ctypes pointer of a numpy array or a torch tensor (host or device), or None."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(C.c_void_p)
+
+
+# ----------------------------------------------------------------------------- drop-ins
+def EPBiCGSTAB(n, Av, Aj, Ai, b, tol, NMAX, Gv, Gj, Gi, IDv, Hv, Hj, Hi, x, verbose=0):
+    """AFIIM EPBiCGSTAB on the GPU. x (float64, C-contiguous) is updated in place."""
+    assert x.dtype == np.float64 and x.flags.c_contiguous
+    resval, it, info = C.c_double(0), C.c_int(0), C.c_int(-1)
+    arrs = [_d(Av), _i(Aj), _i(Ai), _d(b), _d(Gv), _i(Gj), _i(Gi), _d(IDv), _d(Hv), _i(Hj), _i(Hi)]
+    _check(lib().fiim_EPBiCGSTAB_afiim(
+        C.c_int(n), *[_ptr(a) for a in arrs[:4]], C.c_double(tol), C.c_int(NMAX),
+        *[_ptr(a) for a in arrs[4:]], _ptr(x), C.byref(resval), C.byref(it), C.c_int(verbose), C.byref(info)))
+    return resval.value, it.value, info.value
+
+
+def EPBiCGSTAB_pdfiim(A, b, tol, NMAX, G, ID, H, x, issym=False, verbose=0):
+    """PDFIIM EPBiCGSTAB. A, G, H are (Ai, Aj, Av) CSR triples; H may be None when issym."""
+    assert x.dtype == np.float64 and x.flags.c_contiguous
+    Ai, Aj, Av = _i(A[0]), _i(A[1]), _d(A[2])
+    Gi, Gj, Gv = _i(G[0]), _i(G[1]), _d(G[2])
+    if H is None:
+        Hi = Hj = Hv = None
+    else:
+        Hi, Hj, Hv = _i(H[0]), _i(H[1]), _d(H[2])
+    resval, it, info = C.c_double(0), C.c_int(0), C.c_int(-1)
+    _check(lib().fiim_EPBiCGSTAB_pdfiim(
+        C.c_int(len(Ai) - 1), C.c_int(int(issym)), _ptr(Av), _ptr(Aj), _ptr(Ai), _ptr(_d(b)),
+        C.c_double(tol), C.c_int(NMAX), _ptr(Gv), _ptr(Gj), _ptr(Gi), _ptr(_d(ID)), _ptr(Hv), _ptr(Hj),
+        _ptr(Hi), _ptr(x), C.byref(resval), C.byref(it), C.c_int(verbose), C.byref(info)))
+    return resval.value, it.value, info.value
+
+
+def PBiCGSTAB(n, Av, Aj, Ai, b, tol, NMAX, Gv, Gj, Gi, IDv, Hv, Hj, Hi, Lv, Lj, Li, Uv, Uj, Ui, nr, mode, x,
+              verbose=0):
+    """ACIFIM PBiCGSTAB (modes 'E' and 'C')."""
+    assert x.dtype == np.float64 and x.flags.c_contiguous
+    resval, it, info = C.c_double(0), C.c_int(0), C.c_int(-1)
+    lu = [None if a is None else (_i(a) if k % 3 else _d(a)) for k, a in enumerate((Lv, Lj, Li, Uv, Uj, Ui))]
+    _check(lib().fiim_PBiCGSTAB_acifim(
+        C.c_int(n), _ptr(_d(Av)), _ptr(_i(Aj)), _ptr(_i(Ai)), _ptr(_d(b)), C.c_double(tol), C.c_int(NMAX),
+        _ptr(_d(Gv)), _ptr(_i(Gj)), _ptr(_i(Gi)), _ptr(_d(IDv)), _ptr(_d(Hv)), _ptr(_i(Hj)), _ptr(_i(Hi)),
+        *[_ptr(a) for a in lu], C.c_int(nr), C.c_char(mode.encode()), _ptr(x), C.byref(resval),
+        C.byref(it), C.c_int(verbose), C.byref(info)))
+    return resval.value, it.value, info.value
+
+
+# ----------------------------------------------------------------------------- handle API
+class Solver:
+    """Set up once (upload, SpMV shape tuning, graph capture); solve many times.
+
+    A: (Ai, Aj, Av); F: dict with Gi, Gj, Gv, IDv, Hi, Hj, Hv (and Li.., Ui.. for mode 'C').
+    Arrays are numpy (memory='host') or torch CUDA tensors (memory='device')."""
+
+    def __init__(self, A, F, variant="afiim", issym=False, precision="fp64", mode="E", nr=1,
+                 autotune=True, memory="host", verbose=0, inner_tol=1e-5, inner_nmax=1000, max_refine=50):
+        self._h = C.c_void_p(0)
+        o = Options()
+        lib().fiim_options_default(C.byref(o))
+        o.variant = _VARIANTS[variant]
+        o.issym = int(issym)
+        o.precision = _PRECISIONS[precision]
+        o.memory = MEM_DEVICE if memory == "device" else MEM_HOST
+        o.mode = mode.encode()
+        o.nr = nr
+        o.autotune = int(autotune)
+        o.verbose = verbose
+        o.inner_tol = inner_tol
+        o.inner_nmax = inner_nmax
+        o.max_refine = max_refine
+        self.memory = memory
+        conv = (lambda a, ints: a) if memory == "device" else (lambda a, ints: None if a is None else (_i(a) if ints else _d(a)))
+        self._keep = []
+
+        def P(a, ints):
+            a = conv(a, ints)
+            self._keep.append(a)
+            return _ptr(a)
+
+        g = lambda k: F.get(k)
+        n = len(A[0]) - 1
+        self.n = n
+        _check(lib().fiim_solver_create(
+            C.byref(self._h), C.c_int(n), P(A[0], True), P(A[1], True), P(A[2], False),
+            P(g("Gi"), True), P(g("Gj"), True), P(g("Gv"), False), P(g("IDv"), False),
+            P(g("Hi"), True), P(g("Hj"), True), P(g("Hv"), False),
+            P(g("Li"), True), P(g("Lj"), True), P(g("Lv"), False),
+            P(g("Ui"), True), P(g("Uj"), True), P(g("Uv"), False), C.byref(o)))
+        self._keep = []
+
+    def solve(self, b, x, tol=1e-8, nmax=500) -> dict:
+        """x is updated in place; returns the result fields as a dict."""
+        r = Result()
+        if self.memory != "device":
+            b = _d(b)
+            assert x.dtype == np.float64 and x.flags.c_contiguous
+        _check(lib().fiim_solver_solve(self._h, _ptr(b), _ptr(x), C.c_double(tol), C.c_int(nmax), C.byref(r)))
+        return r.as_dict()
+
+    def device_bytes(self) -> int:
+        return int(lib().fiim_solver_device_bytes(self._h))
+
+    def spmv_shape(self, which: int) -> int:
+        v = C.c_int(0)
+        _check(lib().fiim_solver_spmv_shape(self._h, C.c_int(which), C.byref(v)))
+        return v.value
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().fiim_solver_destroy(self._h)
+            self._h = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ----------------------------------------------------------------------------- kernel API
+def spmv(Ai, Aj, Av, x, y, vec=0, stream=0):
+    """y = A x on device tensors (torch CUDA), FP64."""
+    _check(lib().fiim_spmv(C.c_int(Ai.numel() - 1), _ptr(Ai), _ptr(Aj), _ptr(Av), _ptr(x), _ptr(y),
+                           C.c_int(vec), C.c_void_p(stream)))
+
+
+def prec_apply(Gi, Gj, Gv, IDv, Hi, Hj, Hv, r, z, tm, stream=0):
+    """z = G (IDv o (H r)) on device tensors."""
+    _check(lib().fiim_prec_apply(C.c_int(Gi.numel() - 1), _ptr(Gi), _ptr(Gj), _ptr(Gv), _ptr(IDv), _ptr(Hi),
+                                 _ptr(Hj), _ptr(Hv), _ptr(r), _ptr(z), _ptr(tm), C.c_void_p(stream)))
+
+
+# ----------------------------------------------------------------------------- generators
+def _gen(fn, *args):
+    nnz = fn(*args, None, None, None)
+    if nnz < 0:
+        raise FiimError(FIIM_EARG, "bad generator arguments")
+    return nnz
+
+
+def gen_poisson2d(nx, ny=None):
+    ny = nx if ny is None else ny
+    L = lib()
+    nnz = _gen(L.fiim_gen_poisson2d, C.c_int(nx), C.c_int(ny))
+    n = nx * ny
+    Ai, Aj, Av = np.zeros(n + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
+    L.fiim_gen_poisson2d(C.c_int(nx), C.c_int(ny), _ptr(Ai), _ptr(Aj), _ptr(Av))
+    return Ai, Aj, Av
+
+
+def gen_convdiff3d(N, peclet=0.5):
+    L = lib()
+    nnz = _gen(L.fiim_gen_convdiff3d, C.c_int(N), C.c_double(peclet))
+    n = N ** 3
+    Ai, Aj, Av = np.zeros(n + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
+    L.fiim_gen_convdiff3d(C.c_int(N), C.c_double(peclet), _ptr(Ai), _ptr(Aj), _ptr(Av))
+    return Ai, Aj, Av
+
+
+def gen_convdiff2d(N, diff, theta, peclet):
+    L = lib()
+    args = (C.c_int(N), C.c_double(diff), C.c_double(theta), C.c_double(peclet))
+    nnz = _gen(L.fiim_gen_convdiff2d, *args)
+    Ai, Aj, Av = np.zeros(N * N + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
+    L.fiim_gen_convdiff2d(*args, _ptr(Ai), _ptr(Aj), _ptr(Av))
+    return Ai, Aj, Av
+
+
+def batch_params(seed, k, side_lo=32, side_hi=256, d_lo=0.1, d_hi=10.0, pe_max=1.0):
+    side, diff, theta, pe = C.c_int(0), C.c_double(0), C.c_double(0), C.c_double(0)
+    lib().fiim_gen_batch_params(C.c_uint64(seed), C.c_int(k), C.c_int(side_lo), C.c_int(side_hi),
+                                C.c_double(d_lo), C.c_double(d_hi), C.c_double(pe_max), C.byref(side),
+                                C.byref(diff), C.byref(theta), C.byref(pe))
+    return side.value, diff.value, theta.value, pe.value
+
+
+def zipf_scale(n, alpha=2.0, cap=512, mean=16.0, seed=20261203, sample=200000):
+    """Scale of the Zipf draws that gives the target mean row length (bisection)."""
+    L = lib()
+    lo, hi = 0.5, 64.0
+    for _ in range(40):
+        mid = 0.5 * (lo + hi)
+        m = L.fiim_gen_zipf_mean(C.c_int(n), C.c_double(alpha), C.c_int(cap), C.c_double(mid),
+                                 C.c_uint64(seed), C.c_int(sample))
+        if m < mean:
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
+
+
+def gen_zipf(n, scale, alpha=2.0, cap=512, seed=20261203):
+    L = lib()
+    args = (C.c_int(n), C.c_double(alpha), C.c_int(cap), C.c_double(scale), C.c_uint64(seed))
+    nnz = _gen(L.fiim_gen_zipf, *args)
+    Ai, Aj, Av = np.zeros(n + 1, np.int32), np.zeros(nnz, np.int32), np.zeros(nnz)
+    L.fiim_gen_zipf(*args, _ptr(Ai), _ptr(Aj), _ptr(Av))
+    return Ai, Aj, Av
+
+
+def rand_normal(n, seed):
+    out = np.zeros(n)
+    lib().fiim_rand_normal(C.c_long(n), C.c_uint64(seed), _ptr(out))
+    return out
+
+
+def model_rhs(A):
+    Ai, Aj, Av = _i(A[0]), _i(A[1]), _d(A[2])
+    b = np.zeros(len(Ai) - 1)
+    lib().fiim_model_rhs(C.c_int(len(Ai) - 1), _ptr(Ai), _ptr(Aj), _ptr(Av), _ptr(b))
+    return b
+
+
+def pdfiim_build(A, ftol, prefill=1, lfill=1, postfill=1, warpsize=-1, filttype="I", patt="B"):
+    """Host PDFIIM construction (same factors as PDFIIM/src/parPrec.cpp:95-588). Returns a factor dict."""
+    Ai, Aj, Av = _i(A[0]), _i(A[1]), _d(A[2])
+    n = len(Ai) - 1
+    ng, nh = C.c_int(0), C.c_int(0)
+    L = lib()
+    args = (C.c_int(n), _ptr(Ai), _ptr(Aj), _ptr(Av), C.c_int(prefill), C.c_int(lfill), C.c_int(postfill),
+            C.c_double(ftol), C.c_int(warpsize), C.c_char(filttype.encode()), C.c_char(patt.encode()))
+    rc = L.fiim_pdfiim_build(*args, C.byref(ng), C.byref(nh), None, None, None, None, None, None, None)
+    if rc != FIIM_OK:
+        raise FiimError(rc, "pdfiim_build rejected its arguments")
+    F = {"Gv": np.zeros(ng.value), "Gj": np.zeros(ng.value, np.int32), "Gi": np.zeros(n + 1, np.int32),
+         "IDv": np.zeros(n), "Hv": np.zeros(nh.value), "Hj": np.zeros(nh.value, np.int32),
+         "Hi": np.zeros(n + 1, np.int32)}
+    _check(L.fiim_pdfiim_build(*args, C.byref(ng), C.byref(nh), _ptr(F["Gv"]), _ptr(F["Gj"]), _ptr(F["Gi"]),
+                               _ptr(F["IDv"]), _ptr(F["Hv"]), _ptr(F["Hj"]), _ptr(F["Hi"])))
+    return F
+
+
+@dataclass
+class Problem:
+    """A generated system with its factors, as the benches and tests use it."""
+    A: tuple
+    b: np.ndarray
+    F: dict
+    name: str

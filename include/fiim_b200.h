@@ -1,0 +1,185 @@
+/* fiim_b200.h — C-ABI of the B200 (sm_100a) solve phase for factored approximate
+ * inverse preconditioned BiCGSTAB, z = G * D^{-1} * (H * r).
+ *
+ * The reference (cfilelispapadopoulos/Computational-Mathematics) exports the solve phase
+ * as C++ free functions linked from lib*.so with MKL underneath; it has no C or
+ * foreign-function binding. Each entry point below replaces one of those functions,
+ * with the same argument meaning, the same in/out convention (caller owns every
+ * array; x is the initial guess in and the solution out; status through *info) and
+ * the same termination logic, but computes on the GPU. All entry points return an
+ * int status (FIIM_OK or a negative FIIM_E* code) in addition to the reference's
+ * *info, since a GPU call can fail in ways the CPU one could not.
+ *
+ * Pointer spaces: the fiim_EPBiCGSTAB_* / fiim_PBiCGSTAB_* drop-ins take HOST arrays
+ * and do the host->device upload, solve and download inside the call, as the
+ * reference's blocking call does. The handle API (fiim_solver_*) takes host or
+ * device arrays according to fiim_options.memory. The kernel-level entry points
+ * (fiim_spmv, fiim_prec_apply) take DEVICE arrays and a cudaStream_t (as void*).
+ */
+#ifndef FIIM_B200_H
+#define FIIM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define FIIM_OK 0
+#define FIIM_EARG (-1)      /* invalid argument (sizes, null pointers, unsupported mode) */
+#define FIIM_ECUDA (-2)     /* a CUDA runtime call failed; see fiim_last_error() */
+#define FIIM_ENOMEM (-3)    /* device allocation failed */
+#define FIIM_ENODEV (-4)    /* no CUDA device, or the device is not sm_100 */
+#define FIIM_ETIMEOUT (-5)  /* the solve did not finish within the host-side iteration guard */
+
+/* ---- solver variants: whose control flow is reproduced --------------------- */
+#define FIIM_AFIIM 0  /* AFIIM/src/bicgstab.cpp:87-297: maxmsteps = min(max(n,500)/50, 20)      */
+#define FIIM_PDFIIM 1 /* PDFIIM/src/bicgstab.cpp:80-310: as AFIIM; symmetric A uses G^T for H  */
+#define FIIM_ACIFIM 2 /* ACIFIM/src/bicgstab.cpp:97-327: min(max(n,2000)/50, 40), alpha guard  */
+
+/* ---- precision of the preconditioner / inner solve -------------------------- */
+#define FIIM_FP64 0        /* everything in FP64, as the reference                          */
+#define FIIM_MIXED_FP32 1  /* FP64 iterative refinement around an FP32 inner BiCGSTAB       */
+#define FIIM_MIXED_BF16 2  /* as FP32, with G, H stored in BF16 (FP32 accumulation)          */
+
+#define FIIM_MEM_HOST 0
+#define FIIM_MEM_DEVICE 1
+
+/* Last error message of the calling thread (static storage, never NULL). */
+const char *fiim_last_error(void);
+
+/* ===========================================================================
+ * Reference-facing drop-ins (host arrays).
+ * ======================================================================== */
+
+/* Replaces EPBiCGSTAB of AFIIM (AFIIM/src/bicgstab.hpp:82-100, body bicgstab.cpp:87-297).
+ * A: CSR (Av, Aj, Ai) 0-based; G: upper CSR incl. unit diagonal; IDv: D^{-1};
+ * H: lower CSR incl. unit diagonal (layout of afiim, AFIIM/src/prec.cpp:682-740).
+ * verbose != 0 prints the reference's termination messages. */
+int fiim_EPBiCGSTAB_afiim(int n, double *Av, int *Aj, int *Ai, double *b, double tol, int NMAX,
+                          double *Gv, int *Gj, int *Gi, double *IDv, double *Hv, int *Hj, int *Hi,
+                          double *x, double *resval, int *iter, int verbose, int *info);
+
+/* Replaces EPBiCGSTAB of PDFIIM (PDFIIM/src/bicgstab.hpp:75-86, body bicgstab.cpp:80-310),
+ * with the sparseMatrix<int,int,double> members passed as raw CSR arrays
+ * (sparseMatrix.hpp:68-75: v, j, i). issym != 0 is A.mtype == SYMMETRIC: A holds its
+ * upper triangle only and the solver applies G^T where H would be (bicgstab.cpp:189-192);
+ * H may then be NULL. */
+int fiim_EPBiCGSTAB_pdfiim(int n, int issym, double *Av, int *Aj, int *Ai, double *b, double tol,
+                           int NMAX, double *Gv, int *Gj, int *Gi, double *ID, double *Hv, int *Hj,
+                           int *Hi, double *x, double *resval, int *iter, int verbose, int *info);
+
+/* Replaces PBiCGSTAB of ACIFIM (ACIFIM/src/bicgstab.hpp:94-120, body bicgstab.cpp:97-327)
+ * for mode 'E' (explicit G*D^{-1}*H, apply() at bicgstab.cpp:393-394,408-410) and mode
+ * 'C' (Richardson-coupled with nr steps through L and U, bicgstab.cpp:395-404,411-420).
+ * Modes 'I' and 'J' (triangular solves with L, U) return FIIM_EARG. */
+int fiim_PBiCGSTAB_acifim(int n, double *Av, int *Aj, int *Ai, double *b, double tol, int NMAX,
+                          double *Gv, int *Gj, int *Gi, double *IDv, double *Hv, int *Hj, int *Hi,
+                          double *Lv, int *Lj, int *Li, double *Uv, int *Uj, int *Ui, int nr,
+                          char mode, double *x, double *resval, int *iter, int verbose, int *info);
+
+/* ===========================================================================
+ * Handle API: set up once (upload, layout, tuning), solve many times.
+ * ======================================================================== */
+typedef struct fiim_solver_s *fiim_solver_t;
+
+typedef struct {
+    int variant;       /* FIIM_AFIIM / FIIM_PDFIIM / FIIM_ACIFIM                          */
+    int issym;         /* PDFIIM symmetric input (see fiim_EPBiCGSTAB_pdfiim)              */
+    int precision;     /* FIIM_FP64 / FIIM_MIXED_FP32 / FIIM_MIXED_BF16                    */
+    int memory;        /* FIIM_MEM_HOST or FIIM_MEM_DEVICE for every array argument        */
+    char mode;         /* ACIFIM preconditioner mode: 'E' (default) or 'C'                 */
+    int nr;            /* ACIFIM mode 'C' relaxation steps                                 */
+    int autotune;      /* 1: time candidate SpMV shapes at set-up and keep the fastest     */
+    int verbose;       /* print the reference's termination messages                       */
+    double inner_tol;  /* mixed: inner FP32 BiCGSTAB relative tolerance (default 1e-5)     */
+    int inner_nmax;    /* mixed: inner iteration cap per refinement step (default 1000)    */
+    int max_refine;    /* mixed: outer refinement steps cap (default 50)                   */
+} fiim_options;
+
+/* Defaults: FIIM_AFIIM, FP64, host memory, mode 'E', nr 1, autotune 1. */
+void fiim_options_default(fiim_options *opt);
+
+typedef struct {
+    double resval;        /* reference-style ||r_k|| / ||r_0|| at termination (lagged, see docs) */
+    double true_relres;   /* ||b - A x|| / ||b|| recomputed in FP64 after the solve              */
+    int iter;             /* iterations (outer+inner total for mixed precision)                  */
+    int info;             /* 0 converged, 1 diverged, 2 stagnated, 3 NMAX / non-finite alpha     */
+    int refine_steps;     /* mixed precision: outer refinement steps taken                       */
+    double device_ms;     /* device time of the solve, CUDA events on the solve stream           */
+    int launches;         /* kernels this solve launched (graph nodes included)                  */
+} fiim_result;
+
+/* Factors may be given as (G, IDv, H) for every variant; L and U only for ACIFIM 'C'.
+ * For issym, H may be NULL. Arrays are read during the call only. */
+int fiim_solver_create(fiim_solver_t *out, int n, const int *Ai, const int *Aj, const double *Av,
+                       const int *Gi, const int *Gj, const double *Gv, const double *IDv,
+                       const int *Hi, const int *Hj, const double *Hv, const int *Li,
+                       const int *Lj, const double *Lv, const int *Ui, const int *Uj,
+                       const double *Uv, const fiim_options *opt);
+
+/* Solve A x = b. b and x live in opt->memory space; x is the initial guess in and the
+ * solution out. NMAX and tol mean what they mean in the reference; for mixed precision
+ * tol is the outer FP64 relative-residual target. */
+int fiim_solver_solve(fiim_solver_t s, const double *b, double *x, double tol, int NMAX,
+                      fiim_result *res);
+
+/* Bytes of device memory the solver holds. */
+int64_t fiim_solver_device_bytes(fiim_solver_t s);
+
+/* Kernel timing of the last solve: per kernel family, launches and summed device ms. */
+int fiim_solver_spmv_shape(fiim_solver_t s, int which, int *vec);
+
+int fiim_solver_destroy(fiim_solver_t s);
+
+/* ===========================================================================
+ * Kernel-level entry points (device arrays, caller's stream; asynchronous).
+ * ======================================================================== */
+
+/* y = A x, FP64 CSR. vec = lanes per row (2,4,8,16,32) or 0 to choose from nnz/n.
+ * Replaces mkl_sparse_d_mv(NON_TRANSPOSE, 1.0, A, GENERAL, x, 0.0, y)
+ * (AFIIM/src/bicgstab.cpp:151,178,195). */
+int fiim_spmv(int n, const int *Ai, const int *Aj, const double *Av, const double *x, double *y,
+              int vec, void *stream);
+
+/* z = G (IDv o (H r)), FP64; tm is caller scratch of n doubles. Replaces the explicit
+ * preconditioner application (AFIIM/src/bicgstab.cpp:172-175; ACIFIM apply mode 'E').
+ * G entries below the diagonal and H entries above it are ignored, as MKL's
+ * TRIANGULAR descriptors do (AFIIM/src/bicgstab.cpp:140-147). */
+int fiim_prec_apply(int n, const int *Gi, const int *Gj, const double *Gv, const double *IDv,
+                    const int *Hi, const int *Hj, const double *Hv, const double *r, double *z,
+                    double *tm, void *stream);
+
+/* ===========================================================================
+ * Problem generators (host; sizing pass with null arrays returns nnz).
+ * ======================================================================== */
+long fiim_gen_poisson2d(int nx, int ny, int *Ai, int *Aj, double *Av);
+long fiim_gen_convdiff3d(int N, double peclet, int *Ai, int *Aj, double *Av);
+long fiim_gen_convdiff2d(int N, double diff, double theta, double peclet, int *Ai, int *Aj,
+                         double *Av);
+void fiim_gen_batch_params(uint64_t seed, int k, int side_lo, int side_hi, double d_lo,
+                           double d_hi, double pe_max, int *side, double *diff, double *theta,
+                           double *peclet);
+long fiim_gen_zipf(int n, double alpha, int cap, double scale, uint64_t seed, int *Ai, int *Aj,
+                   double *Av);
+double fiim_gen_zipf_mean(int n, double alpha, int cap, double scale, uint64_t seed, int sample);
+void fiim_rand_normal(long n, uint64_t seed, double *out);
+void fiim_model_rhs(int n, const int *Ai, const int *Aj, const double *Av, double *b);
+
+/* ===========================================================================
+ * Factor construction on the host (PDFIIM dynamic patterns), for callers and
+ * benchmarks that need factors without the reference library. Produces the same
+ * G, D^{-1}, H as pdfiim (PDFIIM/src/parPrec.cpp:95-588) for filttype/patt given.
+ * Two calls: first with Gv == NULL returns sizes through nnzG/nnzH and keeps the
+ * result in an internal buffer bound to the calling thread; the second copies it out.
+ * ======================================================================== */
+int fiim_pdfiim_build(int n, const int *Ai, const int *Aj, const double *Av, int prefill,
+                      int lfill, int postfill, double ftol, int warpsize, char filttype,
+                      char patt, int *nnzG, int *nnzH, double *Gv, int *Gj, int *Gi,
+                      double *D, double *Hv, int *Hj, int *Hi);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FIIM_B200_H */
