@@ -1,0 +1,363 @@
+"""Benchmark of the preconditioned BiCGSTAB solve phase on B200.
+
+Workload (one GPU): 3D 7-point upwind convection-diffusion on a 128^3 grid (n = 2,097,152,
+nnz = 14,581,760), unit diffusion, cell Peclet 0.5, b ~ N(0,1) (seed 20261203), x0 = 0,
+PDFIIM factors eps 0.05 (prefill 2, lfill 2, postfill 1, no warpsize limit, inf-norm filter,
+both-triangle pattern) built by the library's host construction, FP64 BiCGSTAB to 1e-8,
+NMAX 1200. A step is one full solve. Synthetic data (the reference names no dataset).
+
+  value  solves/s with A, G, D^-1, H, b resident in HBM (handle API, device arrays),
+         device time of each solve call (CUDA events on the solver's stream)
+  e2e    solves/s through the reference-facing C-ABI call fiim_EPBiCGSTAB_pdfiim with
+         pinned host arrays: every step uploads A, G, D^-1, H, b, x0 and downloads x
+         (host wall clock around the blocking call)
+
+--impl reference times the reference's own EPBiCGSTAB (oracle/_ref: the reference's
+sources compiled against the project's MKL shim, OpenMP on all host cores) on the same
+system with the reference's own pdfiim factors; each step is a bounded sample (a capped
+number of iterations), scaled to solves/s by the full solve's iteration count.
+
+Multi-GPU (torchrun): one full replica per rank (the 128^3 system is one unit; nothing
+is exchanged during a solve), value = total solves / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "computational-mathematics_b200")
+ORACLE = os.path.join(ROOT, "oracle")
+sys.path.insert(0, PKG)
+
+METRIC = "BiCGSTAB solves/sec to 1e-8 rel. residual + HBM GB/s; mixed/batched vs FP64"
+SEED = 20261203
+PDFIIM_PARAMS = dict(ftol=0.05, prefill=2, lfill=2, postfill=1, warpsize=-1, filttype="I", patt="B")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def workload(N):
+    import fiim_b200 as FB
+    A = FB.gen_convdiff3d(N, 0.5)
+    b = FB.rand_normal(N ** 3, SEED)
+    return A, b
+
+
+def config(N, nnz, extra=None):
+    c = {"workload": f"convdiff3d_{N} (n={N ** 3:,}, nnz={nnz:,}) PDFIIM eps 0.05 (2,2,1) FP64 BiCGSTAB",
+         "n": N ** 3, "nnz": int(nnz), "tol": 1e-8, "nmax": 1200,
+         "l2": "inputs larger than L2 (A+G+H+vectors >> 126 MB), no flush"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.p:
+            self.p.terminate()
+            try:
+                out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws == 1:
+        return 0, 1, None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    rank, local = int(os.environ["RANK"]), int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return rank, ws, dist
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(dist, v):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------- CPU reference
+def reference_sample(A, b, F, iters_full, sample_its, kind):
+    """Time the reference's own EPBiCGSTAB (or the oracle port) for `sample_its` iterations."""
+    sys.path.insert(0, ORACLE)
+    import pyoracle as O
+    n = len(b)
+    if kind == "reference":
+        threads = os.cpu_count() or 1
+        O.set_threads(threads, "pdfiim")
+        t0 = time.perf_counter()
+        x, res, it, info = O.ref_solve("pdfiim", A, b, F, tol=1e-8, nmax=sample_its)
+        dt = time.perf_counter() - t0
+    else:
+        threads = 1
+        t0 = time.perf_counter()
+        x, res, it, info = O.bicgstab("pdfiim", A, b, F, tol=1e-8, nmax=sample_its)
+        dt = time.perf_counter() - t0
+    per_iter = dt / max(it, 1)
+    return {"value": 1.0 / (per_iter * iters_full), "per_iter_s": per_iter, "threads": threads, "its": it, "dt": dt}
+
+
+def cpu_kind():
+    sys.path.insert(0, ORACLE)
+    import pyoracle as O
+    if O.have_ref("pdfiim"):
+        return "reference"
+    subprocess.run(["make", "-s", "-C", ORACLE, "restatement"], check=True)
+    return "port"
+
+
+def run_reference(args):
+    rank, ws, dist = (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), None)
+    if rank != 0:
+        return 0
+    sys.path.insert(0, ORACLE)
+    import pyoracle as O
+    kind = cpu_kind()
+    A, b = workload(args.size)
+    nnz = int(A[0][-1])
+    threads = os.cpu_count() or 1
+    if kind == "reference":
+        O.set_threads(threads, "pdfiim")
+        F = O.pdfiim_build(A, **PDFIIM_PARAMS)
+        # iterations of the full solve: the reference's own count on this system
+        iters_full = args.ref_iters
+    else:
+        import fiim_b200 as FB
+        F = FB.pdfiim_build(A, **PDFIIM_PARAMS)
+        iters_full = args.ref_iters
+    sample_its = args.ref_sample_its
+    for _ in range(args.warmup):
+        reference_sample(A, b, F, iters_full, max(2, sample_its // 4), kind)
+    vals, dts = [], []
+    for _ in range(args.steps):
+        r = reference_sample(A, b, F, iters_full, sample_its, kind)
+        vals.append(r["value"])
+        dts.append(r["dt"])
+    v = float(np.median(vals))
+    sample = (f"{sample_its} BiCGSTAB iterations of the {args.size}^3 system per step, scaled by the full solve's "
+              f"{iters_full} iterations")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * float(np.mean(dts)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config(args.size, nnz, {"iterations_per_solve": iters_full}),
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads if kind == "reference" else 1,
+                             "kind": kind, "sample": sample},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------- GPU arm
+def run_ours(args):
+    import torch
+    import fiim_b200 as FB
+    rank, ws, dist = dist_init()
+    dev = torch.device("cuda", torch.cuda.current_device() if ws > 1 else 0)
+    torch.cuda.set_device(dev)
+    t0 = time.perf_counter()
+    A, b = workload(args.size)
+    n, nnz = len(b), int(A[0][-1])
+    F = FB.pdfiim_build(A, **PDFIIM_PARAMS)
+    t_setup = time.perf_counter() - t0
+
+    # ---- value: device-resident inputs, handle API
+    tA = tuple(torch.from_numpy(a).to(dev) for a in A)
+    tF = {k: torch.from_numpy(v).to(dev) for k, v in F.items()}
+    tb = torch.from_numpy(b).to(dev)
+    tx = torch.zeros(n, dtype=torch.float64, device=dev)
+    S = FB.Solver(tA, tF, variant="pdfiim", memory="device")
+    for _ in range(args.warmup):
+        tx.zero_()
+        r = S.solve(tb, tx, tol=1e-8, nmax=1200)
+    torch.cuda.synchronize()
+    barrier(dist)
+    results = []
+    with Clocks(dev.index) as clk:
+        torch.cuda.synchronize()
+        barrier(dist)
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            tx.zero_()
+            results.append(S.solve(tb, tx, tol=1e-8, nmax=1200))
+        torch.cuda.synchronize()
+        barrier(dist)
+        wall = time.perf_counter() - w0
+    dev_ms = sum(r["device_ms"] for r in results)
+    dev_ms_max = max_over_ranks(dist, dev_ms)
+    iters = [r["iter"] for r in results]
+    assert all(r["info"] == 0 for r in results), results[0]
+    value = args.steps * ws / (dev_ms_max / 1000.0)
+    it_bytes = S.iteration_bytes()
+    hbm_gbs = sum(iters) * it_bytes / (dev_ms / 1000.0) / 1e9
+    launches = sum(r["launches"] for r in results)
+
+    # ---- roofline of the dominant kernel (each launch replayed alone, CUDA events on its stream)
+    ktimes = S.kernel_times(reps=20)
+    # share of an iteration: launches per iteration x mean time
+    per_iter_ms = {}
+    for name, ms, by in ktimes:
+        per_iter_ms[name] = per_iter_ms.get(name, 0.0) + ms * (2 if name in ("H_spmv_scale",) else 1)
+    dom = max(ktimes, key=lambda t: t[1] * (2 if t[0] == "H_spmv_scale" else 1))
+    peak, peak_kind = peaks()
+    achieved = dom[2] / (dom[1] / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom[0], "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": peak_kind, "traffic": args.ncu_traffic,
+                "algorithmic_bytes_per_launch": dom[2], "launch_ms": round(dom[1], 5),
+                "per_kernel": [{"kernel": k, "ms": round(m, 5), "gbs": round(by / (m / 1000) / 1e9, 1)}
+                               for k, m, by in ktimes]}
+    S.close()
+
+    # ---- e2e: reference-facing C-ABI call with pinned host arrays
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    hA = [pin(a) for a in A]
+    hG = [pin(F[k]) for k in ("Gi", "Gj", "Gv")]
+    hH = [pin(F[k]) for k in ("Hi", "Hj", "Hv")]
+    hD, hb = pin(F["IDv"]), pin(b)
+    hx = torch.zeros(n, dtype=torch.float64).pin_memory()
+    L = FB.lib()
+    resval, it, info = C.c_double(0), C.c_int(0), C.c_int(0)
+    P = lambda t: C.c_void_p(t.data_ptr())
+
+    def e2e_call():
+        hx.zero_()
+        rc = L.fiim_EPBiCGSTAB_pdfiim(C.c_int(n), 0, P(hA[2]), P(hA[1]), P(hA[0]), P(hb), C.c_double(1e-8), 1200,
+                                      P(hG[2]), P(hG[1]), P(hG[0]), P(hD), P(hH[2]), P(hH[1]), P(hH[0]), P(hx),
+                                      C.byref(resval), C.byref(it), 0, C.byref(info))
+        FB._check(rc)
+    for _ in range(args.warmup):
+        e2e_call()
+    barrier(dist)
+    e_times = []
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        e2e_call()
+        e_times.append(time.perf_counter() - t1)
+    e_tot = max_over_ranks(dist, sum(e_times))
+    h2d = sum(int(t.numel() * t.element_size()) for t in hA + hG + hH + [hD, hb, hx])
+    e2e = {"value": args.steps * ws / e_tot, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": 8 * n, "timing": "host wall clock around the blocking call",
+           "iter": it.value, "info": info.value}
+
+    # ---- CPU baseline (rank 0, N = 1): bounded sample of the reference's solve
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        kind = cpu_kind()
+        Fc = F
+        if kind == "reference":
+            sys.path.insert(0, ORACLE)
+            import pyoracle as O
+            O.set_threads(os.cpu_count() or 1, "pdfiim")
+            Fc = O.pdfiim_build(A, **PDFIIM_PARAMS)
+        its = int(np.median(iters))
+        r = reference_sample(A, b, Fc, its, args.cpu_sample_its, kind)
+        cpu = {"value": r["value"], "unit": "solves/s", "cores": r["threads"], "kind": kind,
+               "sample": f"{r['its']} BiCGSTAB iterations of the full {args.size}^3 solve ({r['dt']:.1f} s), "
+                         f"scaled by the GPU solve's {its} iterations"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 4), "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(dev_ms_max / args.steps, 4), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config(args.size, nnz, {"iterations": iters[0], "parallelism": f"replicas x{ws}",
+                                                  "setup_s": round(t_setup, 2)}),
+                "hbm_gbs": round(hbm_gbs, 1), "hbm_frac": round(hbm_gbs / peak, 4),
+                "iteration_bytes": it_bytes, "true_relres": results[-1]["true_relres"],
+                "resval": results[-1]["resval"], "wall_ms_per_step": round(1000 * wall / args.steps, 4),
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=128, help="grid side of the 3D convection-diffusion system")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--cpu-sample-its", type=int, default=12)
+    ap.add_argument("--ref-sample-its", type=int, default=10)
+    ap.add_argument("--ref-iters", type=int, default=99,
+                    help="iterations of the full 128^3 solve (the reference's own count, for scaling samples)")
+    ap.add_argument("--ncu-traffic", type=float, default=None,
+                    help="dram bytes per launch of the dominant kernel from an ncu capture, if known")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    return run_reference(args) if args.impl == "reference" else run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

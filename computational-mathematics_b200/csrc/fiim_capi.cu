@@ -178,6 +178,17 @@ int fiim_solver_spmv_shape(fiim_solver_t h, int which, int *vec) {
     return FIIM_OK;
 }
 
+int fiim_solver_kernel_times(fiim_solver_t h, int reps, int max_kernels, double *ms, double *bytes,
+                             char *names, int name_len) {
+    if (!h || fiim_is_mixed(h) || !ms || !bytes || reps < 1) return fiim::set_error(FIIM_EARG, "bad argument");
+    return reinterpret_cast<fiim::Solver *>(h)->kernel_times(reps, max_kernels, ms, bytes, names, name_len);
+}
+
+double fiim_solver_iteration_bytes(fiim_solver_t h) {
+    if (!h || fiim_is_mixed(h)) return -1.0;
+    return reinterpret_cast<fiim::Solver *>(h)->iteration_bytes();
+}
+
 int fiim_solver_destroy(fiim_solver_t h) {
     if (!h) return FIIM_OK;
     if (fiim_is_mixed(h)) return fiim_mixed_destroy(h);

@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <iostream>
 #include <map>
 #include <mutex>
@@ -406,6 +407,16 @@ int Solver::build_graph() {
         graph = nullptr;
     }
     use_cond = false;
+    // Run the body once with the state marked done (every kernel returns at once) so
+    // launch shapes are resolved before capture begins.
+    {
+        DState h = {};
+        h.done = 1;
+        *hst = h;
+        FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
+        FIIM_TRY(enqueue_iteration(false, cudaGraphConditionalHandle{}));
+        FIIM_CUDA(cudaStreamSynchronize(stream));
+    }
     // Preferred: one graph whose WHILE node repeats the iteration body on the device.
     do {
         cudaGraph_t g = nullptr;
@@ -609,6 +620,7 @@ int Solver::solve(const double *b_in, double *x_io, double tol, int nmax, fiim_r
     const bool dev_src = (opt.memory == FIIM_MEM_DEVICE);
     const cudaMemcpyKind in_kind = dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     const cudaMemcpyKind out_kind = dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    FIIM_CUDA(cudaEventRecord(ev0, stream));
     FIIM_CUDA(cudaMemcpyAsync(b, b_in, sizeof(double) * n, in_kind, stream));
     FIIM_CUDA(cudaMemcpyAsync(x, x_io, sizeof(double) * n, in_kind, stream));
 
@@ -622,7 +634,6 @@ int Solver::solve(const double *b_in, double *x_io, double tol, int nmax, fiim_r
     h.alpha_guard = (opt.variant == FIIM_ACIFIM);
     *hst = h;
     FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
-    FIIM_CUDA(cudaEventRecord(ev0, stream));
     // Start: r = b - A x, r0 = r, p = r, ro = ||r0|| (AFIIM/src/bicgstab.cpp:151-165).
     FIIM_CUDA(launch_spmv(A.vec, stream, view(A), x, EpiInit{b, p, r0, r}, st, partials));
     int launches = 1;
@@ -647,10 +658,10 @@ int Solver::solve(const double *b_in, double *x_io, double tol, int nmax, fiim_r
     // FP64 true residual ||b - A x|| / ||b||.
     FIIM_CUDA(launch_spmv(A.vec, stream, view(A), x, EpiResid{b, nullptr}, st, partials));
     launches += 1;
-    FIIM_CUDA(cudaEventRecord(ev1, stream));
     const int fallback_loops = hst->loops;
     FIIM_CUDA(cudaMemcpyAsync(hst, st, sizeof(DState), cudaMemcpyDeviceToHost, stream));
     FIIM_CUDA(cudaMemcpyAsync(x_io, x, sizeof(double) * n, out_kind, stream));
+    FIIM_CUDA(cudaEventRecord(ev1, stream));
     FIIM_CUDA(cudaStreamSynchronize(stream));
     if (!use_cond) hst->loops = fallback_loops;
     float ms = 0.f;
@@ -702,6 +713,60 @@ void Solver::destroy() {
     if (hst) cudaFreeHost(hst);
     hst = nullptr;
     arena.release();
+}
+
+// ------------------------------------------------------------------ per-kernel timing
+// Replays each launch of the iteration body on its own, `reps` times, between CUDA
+// events on the solver's stream, after a solve has left the vectors populated. The
+// scalars are reset so no kernel takes its early exit. Reports the mean device ms of
+// each launch and its algorithmic bytes: a matrix pass S(M) = nnz*(8+4) + 4*(n+1),
+// one read of the gathered vector, and every other vector read or written once.
+int Solver::kernel_times(int reps, int max_k, double *ms, double *bytes, char *names, int name_len) {
+    FIIM_CUDA(cudaSetDevice(device));
+    const bool combined = (opt.variant == FIIM_ACIFIM && opt.mode == 'C' && opt.nr > 1);
+    if (combined) return set_error(FIIM_EARG, "kernel timing covers mode 'E' bodies");
+    struct Item { const char *name; double bytes; std::function<cudaError_t()> go; };
+    const double nv = 8.0 * n;
+    auto S = [&](const DevCsr &M) { return 12.0 * M.nnz + 4.0 * (M.n + 1); };
+    const long nn = n;
+    std::vector<Item> items = {
+        {"H_spmv_scale", S(H) + 3 * nv, [&] { return launch_spmv(H.vec, stream, view(H), p, EpiScale{tm, IDv}, st, partials); }},
+        {"G_spmv_norm", S(G) + 2 * nv, [&] { return launch_spmv(G.vec, stream, view(G), tm, EpiNorm{pc}, st, partials); }},
+        {"A_spmv_alpha", S(A) + 3 * nv, [&] { return launch_spmv(A.vec, stream, view(A), pc, EpiAlpha{v, r0}, st, partials); }},
+        {"update_s", 4 * nv, [&] { k_update_s<<<stream_grid(k_update_s, nn), kThreads, 0, stream>>>(nn, r, v, x, sv, st, partials); return cudaGetLastError(); }},
+        {"G_spmv", S(G) + 2 * nv, [&] { return launch_spmv(G.vec, stream, view(G), tm, EpiStore{sc}, st, partials); }},
+        {"A_spmv_omega", S(A) + 3 * nv, [&] { return launch_spmv(A.vec, stream, view(A), sc, EpiOmega{t, sv}, st, partials); }},
+        {"update_xr", 8 * nv, [&] { k_update_xr<<<stream_grid(k_update_xr, nn), kThreads, 0, stream>>>(nn, pc, sc, sv, t, r0, x, r, st, partials); return cudaGetLastError(); }},
+        {"update_p", 4 * nv, [&] { k_update_p<<<stream_grid(k_update_p, nn), kThreads, 0, stream>>>(nn, r, v, p, st, cudaGraphConditionalHandle{}, 0); return cudaGetLastError(); }},
+    };
+    // Scalars that keep every kernel on its full path; the solver's vectors are
+    // scratch here (each solve starts from the caller's x and b).
+    DState h = {};
+    h.tol = 0.0; h.eps = 0.0; h.nmax = 1 << 30; h.maxmsteps = 1 << 30; h.info = -1;
+    h.m1 = 1.0; h.alpha = 1e-30; h.omega = 1e-30; h.beta = 1e-30; h.ro = 1.0; h.rc = 1.0;
+    *hst = h;
+    FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
+    const int k = std::min<int>((int)items.size(), max_k);
+    for (int i = 0; i < k; ++i) {
+        FIIM_CUDA(items[i].go());   // warm
+        FIIM_CUDA(cudaEventRecord(ev0, stream));
+        for (int rr = 0; rr < reps; ++rr) FIIM_CUDA(items[i].go());
+        FIIM_CUDA(cudaEventRecord(ev1, stream));
+        FIIM_CUDA(cudaEventSynchronize(ev1));
+        float t_ms = 0.f;
+        FIIM_CUDA(cudaEventElapsedTime(&t_ms, ev0, ev1));
+        ms[i] = t_ms / reps;
+        bytes[i] = items[i].bytes;
+        if (names) std::snprintf(names + (size_t)i * name_len, name_len, "%s", items[i].name);
+    }
+    return k;
+}
+
+double Solver::iteration_bytes() const {
+    // One iteration of the reference's algorithm: every matrix streamed twice, 32 vector
+    // passes (the compulsory reads and writes of AFIIM/src/bicgstab.cpp:170-271).
+    auto S = [&](const DevCsr &M) { return 12.0 * M.nnz + 4.0 * (M.n + 1); };
+    return 2 * S(A) + 2 * S(G) + 2 * S(H) + 32.0 * 8.0 * n;
 }
 
 // ------------------------------------------------------------------ kernel-level API

@@ -37,7 +37,7 @@ _PRECISIONS = {"fp64": FP64, "fp32": MIXED_FP32, "bf16": MIXED_BF16}
 EXPORTS = (
     "fiim_last_error", "fiim_options_default", "fiim_EPBiCGSTAB_afiim", "fiim_EPBiCGSTAB_pdfiim",
     "fiim_PBiCGSTAB_acifim", "fiim_solver_create", "fiim_solver_solve", "fiim_solver_device_bytes",
-    "fiim_solver_spmv_shape", "fiim_solver_destroy", "fiim_spmv", "fiim_prec_apply",
+    "fiim_solver_spmv_shape", "fiim_solver_kernel_times", "fiim_solver_iteration_bytes", "fiim_solver_destroy", "fiim_spmv", "fiim_prec_apply",
     "fiim_gen_poisson2d", "fiim_gen_convdiff3d", "fiim_gen_convdiff2d", "fiim_gen_batch_params",
     "fiim_gen_zipf", "fiim_gen_zipf_mean", "fiim_rand_normal", "fiim_model_rhs", "fiim_pdfiim_build",
 )
@@ -78,6 +78,7 @@ def lib() -> C.CDLL:
         for name in ("fiim_gen_poisson2d", "fiim_gen_convdiff3d", "fiim_gen_convdiff2d", "fiim_gen_zipf"):
             getattr(L, name).restype = C.c_long
         L.fiim_gen_zipf_mean.restype = C.c_double
+        L.fiim_solver_iteration_bytes.restype = C.c_double
         _lib = L
     return _lib
 
@@ -206,6 +207,20 @@ class Solver:
         v = C.c_int(0)
         _check(lib().fiim_solver_spmv_shape(self._h, C.c_int(which), C.byref(v)))
         return v.value
+
+    def kernel_times(self, reps=20, max_kernels=16):
+        """Mean device ms and algorithmic bytes of each launch of the iteration body."""
+        ms, by = np.zeros(max_kernels), np.zeros(max_kernels)
+        names = C.create_string_buffer(max_kernels * 32)
+        k = lib().fiim_solver_kernel_times(self._h, C.c_int(reps), C.c_int(max_kernels), _ptr(ms), _ptr(by),
+                                           names, C.c_int(32))
+        if k < 0:
+            _check(k)
+        raw = names.raw
+        return [(raw[i * 32:(i + 1) * 32].split(b"\0")[0].decode(), float(ms[i]), float(by[i])) for i in range(k)]
+
+    def iteration_bytes(self) -> float:
+        return float(lib().fiim_solver_iteration_bytes(self._h))
 
     def close(self):
         if self._h and self._h.value:

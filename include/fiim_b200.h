@@ -128,8 +128,19 @@ int fiim_solver_solve(fiim_solver_t s, const double *b, double *x, double tol, i
 /* Bytes of device memory the solver holds. */
 int64_t fiim_solver_device_bytes(fiim_solver_t s);
 
-/* Kernel timing of the last solve: per kernel family, launches and summed device ms. */
+/* Lanes per row chosen for matrix `which` (0 A, 1 G, 2 H, 3 L, 4 U). */
 int fiim_solver_spmv_shape(fiim_solver_t s, int which, int *vec);
+
+/* Profiling aid (no counterpart in the reference): replays each launch of the FP64
+ * iteration body alone `reps` times between CUDA events on the solver's stream and
+ * writes the mean ms per launch, its algorithmic bytes and (if names != NULL) its name
+ * into names[i * name_len]. Call after a solve. Returns the number of kernels (<= max). */
+int fiim_solver_kernel_times(fiim_solver_t s, int reps, int max_kernels, double *ms, double *bytes,
+                             char *names, int name_len);
+
+/* Algorithmic bytes of one FP64 iteration: 2 S(A) + 2 S(G) + 2 S(H) + 32 * 8n, where
+ * S(M) = 12 nnz(M) + 4 (n + 1). */
+double fiim_solver_iteration_bytes(fiim_solver_t s);
 
 int fiim_solver_destroy(fiim_solver_t s);
 

@@ -1,0 +1,220 @@
+"""GPU parity of the FP64 solve phase against the oracle (B200 only).
+
+Every check goes through the C-ABI of libfiim_b200.so. Tolerances:
+  * SpMV and preconditioner application on the same vector: 1e-12 relative (FP64; the
+    GPU sums each row as a lane tree with FMA, the oracle left to right).
+  * Solves: the same info code, iteration count within +-2, the tolerance reached
+    (resval < tol when converged), and the solution close to the reference's.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import fiim_b200 as FB
+import pyoracle as O
+from conftest import sub
+from test_oracle import identity_factors, skew_system
+
+pytestmark = pytest.mark.gpu
+
+FIXTURE_PRODUCTS = [("sherman2", "afiim9e-6_"), ("sherman2", "afiim0.1_"), ("sherman2", "acifim_"),
+                    ("poisson128_afiim", ""), ("convdiff16_pdfiim", ""), ("convdiff2d48_acifim", "")]
+
+
+def _t(a, dev):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(np.asarray(b)), 1e-300)
+
+
+@pytest.mark.parametrize("name,prefix", FIXTURE_PRODUCTS)
+@pytest.mark.parametrize("vec", [0, 2, 4, 8, 16, 32])
+def test_spmv_matches_oracle(golden, cuda, name, prefix, vec):
+    import torch
+    g = golden(name)
+    u = sub(g, prefix)["u"]
+    Ai, Aj, Av = (_t(g[k], cuda) for k in ("Ai", "Aj", "Av"))
+    y = torch.zeros(len(g["b"]), dtype=torch.float64, device=cuda)
+    FB.spmv(Ai, Aj, Av, _t(u, cuda), y, vec=vec)
+    torch.cuda.synchronize()
+    ref = sub(g, prefix)["Au"]
+    absA = sp.csr_matrix((np.abs(g["Av"]), g["Aj"], g["Ai"])) @ np.abs(u)
+    assert np.all(np.abs(y.cpu().numpy() - ref) <= 1e-12 * absA + 1e-300)
+    assert rel(y.cpu().numpy(), ref) <= 1e-12
+
+
+@pytest.mark.parametrize("name,prefix", FIXTURE_PRODUCTS)
+def test_prec_apply_matches_oracle(golden, cuda, name, prefix):
+    import torch
+    g = golden(name)
+    F = sub(g, prefix)
+    n = len(g["b"])
+    d = {k: _t(F[k], cuda) for k in ("Gi", "Gj", "Gv", "IDv", "Hi", "Hj", "Hv")}
+    z = torch.zeros(n, dtype=torch.float64, device=cuda)
+    tm = torch.zeros_like(z)
+    FB.prec_apply(d["Gi"], d["Gj"], d["Gv"], d["IDv"], d["Hi"], d["Hj"], d["Hv"], _t(F["u"], cuda), z, tm)
+    torch.cuda.synchronize()
+    assert rel(z.cpu().numpy(), F["Mu"]) <= 1e-12
+
+
+def test_prec_apply_ignores_entries_outside_triangles(cuda):
+    """MKL TRIANGULAR descriptors read one triangle (AFIIM/src/bicgstab.cpp:140-147)."""
+    import torch
+    rng = np.random.default_rng(3)
+    n = 300
+    M = sp.random(n, n, density=0.05, random_state=4, format="csr") + sp.eye(n)
+    M.sort_indices()
+    F = {"Gi": M.indptr, "Gj": M.indices, "Gv": M.data, "IDv": rng.uniform(0.5, 2, n),
+         "Hi": M.indptr, "Hj": M.indices, "Hv": M.data}
+    u = rng.standard_normal(n)
+    want = O.prec_apply(F, u)
+    d = {k: _t(np.asarray(F[k], np.int32 if k[1] in "ij" else np.float64), cuda) for k in F}
+    z = torch.zeros(n, dtype=torch.float64, device=cuda)
+    FB.prec_apply(d["Gi"], d["Gj"], d["Gv"], d["IDv"], d["Hi"], d["Hj"], d["Hv"], _t(u, cuda), z,
+                  torch.zeros_like(z))
+    torch.cuda.synchronize()
+    assert rel(z.cpu().numpy(), want) <= 1e-12
+
+
+SOLVES = [
+    ("sherman2", "afiim9e-6_", "afiim9e-6_", "afiim", {}, 500, 1e-6),
+    ("sherman2", "afiim0.1_", "afiim0.1_", "afiim", {}, 500, 1e-4),
+    ("sherman2", "acifim_", "acifimE_", "acifim", {"mode": "E", "nr": 2}, 2000, 1e-4),
+    ("sherman2", "acifim_", "acifimC_", "acifim", {"mode": "C", "nr": 2}, 2000, 1e-4),
+    ("sherman2", "pdfiim_", "pdfiim_", "pdfiim", {}, 1200, 1e-3),
+    ("poisson128_afiim", "", "", "afiim", {}, 1000, 1e-6),
+    ("convdiff16_pdfiim", "", "", "pdfiim", {}, 1200, 1e-6),
+    ("convdiff2d48_acifim", "", "E_", "acifim", {"mode": "E", "nr": 2}, 2000, 1e-6),
+    ("convdiff2d48_acifim", "", "C_", "acifim", {"mode": "C", "nr": 2}, 2000, 1e-6),
+    ("poisson32_sym_pdfiim", "", "", "pdfiim", {"issym": True}, 1200, 1e-6),
+]
+
+
+def dropin(variant, g, F, nmax, x, tol=1e-8, mode="E", nr=1, issym=False):
+    n = len(g["b"])
+    if variant == "afiim":
+        return FB.EPBiCGSTAB(n, g["Av"], g["Aj"], g["Ai"], g["b"], tol, nmax, F["Gv"], F["Gj"], F["Gi"], F["IDv"],
+                             F["Hv"], F["Hj"], F["Hi"], x)
+    if variant == "pdfiim":
+        H = None if issym else (F["Hi"], F["Hj"], F["Hv"])
+        return FB.EPBiCGSTAB_pdfiim((g["Ai"], g["Aj"], g["Av"]), g["b"], tol, nmax, (F["Gi"], F["Gj"], F["Gv"]),
+                                    F["IDv"], H, x, issym=issym)
+    return FB.PBiCGSTAB(n, g["Av"], g["Aj"], g["Ai"], g["b"], tol, nmax, F["Gv"], F["Gj"], F["Gi"], F["IDv"],
+                        F["Hv"], F["Hj"], F["Hi"], F.get("Lv"), F.get("Lj"), F.get("Li"), F.get("Uv"), F.get("Uj"),
+                        F.get("Ui"), nr, mode, x)
+
+
+@pytest.mark.parametrize("name,fprefix,rprefix,variant,kw,nmax,xtol", SOLVES)
+def test_dropin_solve_matches_reference(golden, name, fprefix, rprefix, variant, kw, nmax, xtol):
+    g = golden(name)
+    F = sub(g, fprefix)
+    x = np.zeros(len(g["b"]))
+    resval, it, info = dropin(variant, g, F, nmax, x, **kw)
+    ref_it, ref_info = int(g[rprefix + "iter"]), int(g[rprefix + "info"])
+    print(f"{name}/{rprefix or variant}: gpu iter {it} info {info} resval {resval:.3e} | "
+          f"ref iter {ref_it} info {ref_info} resval {float(g[rprefix + 'resval']):.3e} | "
+          f"x rel diff {rel(x, g[rprefix + 'x']):.2e}")
+    assert info == ref_info
+    assert abs(it - ref_it) <= 2
+    if ref_info == 0:
+        assert resval < 1e-8
+    assert rel(x, g[rprefix + "x"]) <= xtol
+
+
+@pytest.mark.parametrize("memory", ["host", "device"])
+def test_handle_api_matches_dropin(golden, cuda, memory):
+    import torch
+    g = golden("poisson128_afiim")
+    F = {k: g[k] for k in ("Gi", "Gj", "Gv", "IDv", "Hi", "Hj", "Hv")}
+    A = (g["Ai"], g["Aj"], g["Av"])
+    x0 = np.zeros(len(g["b"]))
+    r_drop = FB.EPBiCGSTAB(len(g["b"]), g["Av"], g["Aj"], g["Ai"], g["b"], 1e-8, 1000, F["Gv"], F["Gj"], F["Gi"],
+                           F["IDv"], F["Hv"], F["Hj"], F["Hi"], x0)
+    if memory == "device":
+        A = tuple(_t(a, cuda) for a in A)
+        F = {k: _t(v, cuda) for k, v in F.items()}
+        b, x = _t(g["b"], cuda), torch.zeros(len(g["b"]), dtype=torch.float64, device=cuda)
+    else:
+        b, x = g["b"], np.zeros(len(g["b"]))
+    S = FB.Solver(A, F, variant="afiim", memory=memory)
+    r = S.solve(b, x, tol=1e-8, nmax=1000)
+    xs = x.cpu().numpy() if memory == "device" else x
+    assert (r["resval"], r["iter"], r["info"]) == r_drop
+    assert np.array_equal(xs, x0)
+    assert r["true_relres"] < 1e-7 and r["device_ms"] > 0 and r["launches"] > r["iter"] * 9
+    S.close()
+
+
+def test_repeated_solves_are_bitwise_deterministic(golden):
+    g = golden("convdiff16_pdfiim")
+    F = {k: g[k] for k in ("Gi", "Gj", "Gv", "IDv", "Hi", "Hj", "Hv")}
+    S = FB.Solver((g["Ai"], g["Aj"], g["Av"]), F, variant="pdfiim")
+    xs = []
+    for _ in range(3):
+        x = np.zeros(len(g["b"]))
+        r = S.solve(g["b"], x, tol=1e-8, nmax=1200)
+        xs.append((x, r["resval"], r["iter"]))
+    assert all(np.array_equal(xs[0][0], o[0]) and xs[0][1:] == o[1:] for o in xs[1:])
+
+
+def test_edge_cases_match_oracle(golden):
+    g = golden("poisson128_afiim")
+    A = (g["Ai"], g["Aj"], g["Av"])
+    F = {k: g[k] for k in ("Gi", "Gj", "Gv", "IDv", "Hi", "Hj", "Hv")}
+    S = FB.Solver(A, F, variant="afiim")
+    n = len(g["b"])
+    for nmax in (0, 1, 2, 5):
+        x = np.zeros(n)
+        r = S.solve(g["b"], x, tol=1e-8, nmax=nmax)
+        xo, res, it, info = O.bicgstab("afiim", A, g["b"], F, tol=1e-8, nmax=nmax)
+        assert (r["iter"], r["info"]) == (it, info)
+        assert rel(x, xo) <= 1e-10 if nmax > 0 else np.array_equal(x, xo)
+    # nonzero initial guess
+    x0 = FB.rand_normal(n, 11)
+    x = x0.copy()
+    r = S.solve(g["b"], x, tol=1e-8, nmax=1000)
+    xo, res, it, info = O.bicgstab("afiim", A, g["b"], F, tol=1e-8, nmax=1000, x0=x0)
+    assert r["info"] == info == 0 and abs(r["iter"] - it) <= 2
+    # zero right-hand side: ro = 0; the reference runs to NMAX on NaNs
+    x = np.zeros(n)
+    r = S.solve(np.zeros(n), x, tol=1e-8, nmax=6)
+    assert (r["iter"], r["info"]) == (6, 3) and np.isnan(r["resval"])
+    # unreachable tolerance: the oracle's stagnation / divergence exit
+    x = np.zeros(n)
+    r = S.solve(g["b"], x, tol=1e-30, nmax=1000)
+    xo, res, it, info = O.bicgstab("afiim", A, g["b"], F, tol=1e-30, nmax=1000)
+    assert r["info"] == info and info in (1, 2)
+    S.close()
+
+
+def test_acifim_nonfinite_alpha_guard():
+    """ACIFIM/src/bicgstab.cpp:208-213: alpha = m1 / 0 ends the solve with iter = NMAX, info 3."""
+    A = skew_system(64)
+    F = identity_factors(64)
+    F.update(Li=F["Hi"], Lj=F["Hj"], Lv=F["Hv"], Ui=F["Gi"], Uj=F["Gj"], Uv=F["Gv"])
+    b = np.ones(64)
+    for mode in "EC":
+        x = np.zeros(64)
+        res, it, info = FB.PBiCGSTAB(64, A[2], A[1], A[0], b, 1e-8, 25, F["Gv"], F["Gj"], F["Gi"], F["IDv"], F["Hv"],
+                                     F["Hj"], F["Hi"], F["Lv"], F["Lj"], F["Li"], F["Uv"], F["Uj"], F["Ui"], 2, mode, x)
+        xo, reso, ito, infoo = O.bicgstab("acifim", A, b, F, nmax=25, mode=mode, nr=2)
+        assert (it, info) == (ito, infoo) == (25, 3)
+        assert not x.any()
+
+
+def test_convdiff64_host_factors_match_oracle():
+    """The 128^3 workload's stencil at 64^3 with the product's own PDFIIM factors."""
+    A = FB.gen_convdiff3d(64, 0.5)
+    b = FB.rand_normal(64 ** 3, 20261203)
+    F = FB.pdfiim_build(A, 0.05, 2, 2, 1, -1, "I", "B")
+    x = np.zeros(64 ** 3)
+    S = FB.Solver(A, F, variant="pdfiim")
+    r = S.solve(b, x, tol=1e-8, nmax=1200)
+    xo, reso, ito, infoo = O.bicgstab("pdfiim", A, b, F, tol=1e-8, nmax=1200)
+    print("64^3:", r, "oracle", ito, infoo, reso)
+    assert r["info"] == infoo == 0 and abs(r["iter"] - ito) <= 2
+    assert r["true_relres"] < 1e-7 and rel(x, xo) < 1e-6
+    S.close()

@@ -1,0 +1,190 @@
+"""Host-side logic (CPU only): generators, the host PDFIIM construction, the C-ABI surface.
+
+No GPU compute is called here; on a machine without a B200 the GPU entry points must
+fail loudly with FIIM_ENODEV instead of computing anything on the CPU.
+"""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import fiim_b200 as FB
+import pyoracle as O
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "fiim_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fiim_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = FB.lib()
+    names = declared_functions()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(lib, name), f"{name} declared in include/fiim_b200.h but not exported"
+    assert sorted(FB.EXPORTS) == names
+
+
+def test_reference_signature_overloads_exported():
+    """The C++ drop-ins carry the reference's mangled names (AFIIM/ACIFIM/PDFIIM bicgstab.hpp)."""
+    out = subprocess.run(["nm", "-D", "--defined-only", FB.LIB_PATH], capture_output=True, text=True).stdout
+    syms = subprocess.run(["c++filt"], input=out, capture_output=True, text=True).stdout
+    assert "EPBiCGSTAB(int, double*, int*, int*, double*, double, int, double*, int*, int*, double*, " \
+           "double*, int*, int*, double*, double*, int*, int, int*)" in syms
+    assert "PBiCGSTAB(int, double*, int*, int*, double*, double, int, double*, int*, int*, double*, double*, " \
+           "int*, int*, double*, int*, int*, double*, int*, int*, int, char, double*, double*, int*, int, int*)" in syms
+    assert "EPBiCGSTAB(sparseMatrix<int, int, double>&, std::vector<double, std::allocator<double> >&, double, " \
+           "int, sparseMatrix<int, int, double>&, std::vector<double, std::allocator<double> >&, " \
+           "sparseMatrix<int, int, double>&, std::vector<double, std::allocator<double> >&, double*, int*, int, " \
+           "int*)" in syms
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-GPU error path")
+def test_no_gpu_fails_loudly():
+    A = FB.gen_poisson2d(8)
+    F = {"Gi": A[0], "Gj": A[1], "Gv": A[2], "IDv": np.ones(64), "Hi": A[0], "Hj": A[1], "Hv": A[2]}
+    with pytest.raises(FB.FiimError) as e:
+        FB.Solver(A, F)
+    assert e.value.rc == FB.FIIM_ENODEV
+    x = np.zeros(64)
+    with pytest.raises(FB.FiimError):
+        FB.EPBiCGSTAB(64, A[2], A[1], A[0], np.ones(64), 1e-8, 10, A[2], A[1], A[0], np.ones(64), A[2], A[1],
+                      A[0], x)
+    assert not x.any()
+
+
+def test_bad_arguments_rejected_before_device():
+    lib = FB.lib()
+    h = C.c_void_p(0)
+    assert lib.fiim_solver_create(C.byref(h), 0, None, None, None, None, None, None, None, None, None, None,
+                                  None, None, None, None, None, None, None) == FB.FIIM_EARG
+    assert "n <= 0" in lib.fiim_last_error().decode()
+    x = np.zeros(4)
+    r = FB.Result()
+    assert lib.fiim_solver_solve(None, x.ctypes, x.ctypes, C.c_double(1e-8), 10, C.byref(r)) == FB.FIIM_EARG
+    # ACIFIM modes 'I' and 'J' are triangular solves, not the factored inverse
+    A = FB.gen_poisson2d(2)
+    rc = lib.fiim_PBiCGSTAB_acifim(4, *[a.ctypes for a in (A[2], A[1], A[0])], x.ctypes, C.c_double(1e-8), 5,
+                                   *[a.ctypes for a in (A[2], A[1], A[0], x, A[2], A[1], A[0])],
+                                   *[a.ctypes for a in (A[2], A[1], A[0], A[2], A[1], A[0])], 1, C.c_char(b"I"),
+                                   x.ctypes, C.byref(C.c_double()), C.byref(C.c_int()), 0, C.byref(C.c_int()))
+    assert rc == FB.FIIM_EARG
+
+
+# ----------------------------------------------------------------------------- generators
+def test_poisson2d():
+    Ai, Aj, Av = FB.gen_poisson2d(128)
+    n = 128 * 128
+    assert len(Ai) == n + 1 and Ai[-1] == 81408
+    assert np.all(np.diff(Ai) >= 3)
+    for i in (0, 77, n - 1):
+        cols = Aj[Ai[i]:Ai[i + 1]]
+        assert np.all(np.diff(cols) > 0)
+        assert Av[Ai[i] + list(cols).index(i)] == 4.0
+    assert FB.model_rhs((Ai, Aj, Av))[200] == 0.0      # interior row sum
+
+
+def test_convdiff3d_structure():
+    N = 12
+    Ai, Aj, Av = FB.gen_convdiff3d(N, 0.5)
+    n = N ** 3
+    assert Ai[-1] == 7 * n - 6 * N * N
+    rows = np.repeat(np.arange(n), np.diff(Ai))
+    assert np.all(np.diff(Aj)[np.diff(rows) == 0] > 0)               # ascending columns
+    assert np.all(Av[Aj == rows] == 7.5)
+    assert np.all(Av[Aj < rows] == -1.5) and np.all(Av[Aj > rows] == -1.0)
+    interior = N * N * (N // 2) + N * (N // 2) + N // 2
+    assert abs(Av[Ai[interior]:Ai[interior + 1]].sum()) < 1e-15
+    # the 128^3 workload's size without building it
+    assert FB.lib().fiim_gen_convdiff3d(128, C.c_double(0.5), None, None, None) == 14581760
+
+
+def test_convdiff2d_and_batch_params():
+    sides = []
+    for k in range(256):
+        side, diff, theta, pe = FB.batch_params(20261203, k)
+        assert 32 <= side <= 256 and 0.1 <= diff <= 10 and 0 <= theta < 6.2832 and 0 < pe <= 1
+        sides.append(side)
+    assert FB.batch_params(20261203, 5) == FB.batch_params(20261203, 5)
+    assert 100 < np.mean(sides) < 190
+    side, diff, theta, pe = FB.batch_params(20261203, 3)
+    Ai, Aj, Av = FB.gen_convdiff2d(20, diff, theta, pe)
+    assert Ai[-1] == 5 * 400 - 80
+    rows = np.repeat(np.arange(400), np.diff(Ai))
+    off = Av[Aj != rows]
+    assert np.all(off < 0)                                           # M-matrix sign pattern
+    s = np.zeros(400)
+    np.add.at(s, rows, Av)
+    assert np.all(s > -1e-12)                                        # weak diagonal dominance
+
+
+def test_zipf_rows():
+    n = 20000
+    scale = FB.zipf_scale(n, sample=n)
+    Ai, Aj, Av = FB.gen_zipf(n, scale)
+    lens = np.diff(Ai)
+    assert abs(lens.mean() - 16) < 0.25 and lens.min() >= 1 and lens.max() <= 512
+    rows = np.repeat(np.arange(n), lens)
+    d = Av[Aj == rows]
+    assert len(d) == n
+    off = np.zeros(n)
+    np.add.at(off, rows[Aj != rows], np.abs(Av[Aj != rows]))
+    nz = off > 0
+    assert np.allclose(d[nz], 1.1 * off[nz])
+    assert np.all(np.diff(Aj)[np.diff(rows) == 0] > 0)
+
+
+def test_rand_normal():
+    x = FB.rand_normal(200000, 7)
+    assert abs(x.mean()) < 0.01 and abs(x.std() - 1) < 0.01
+    assert np.array_equal(x[:10], FB.rand_normal(10, 7))
+
+
+# ----------------------------------------------------------------------------- construction
+def test_host_pdfiim_matches_golden_factors(golden):
+    g = golden("convdiff16_pdfiim")
+    F = FB.pdfiim_build((g["Ai"], g["Aj"], g["Av"]), 0.05, 2, 2, 1, -1, "I", "B")
+    for k in ("Gi", "Gj", "Gv", "Hi", "Hj", "Hv", "IDv"):
+        assert np.array_equal(F[k], g[k]), k
+
+
+def test_host_pdfiim_matches_golden_sherman2(golden):
+    g = golden("sherman2")
+    F = FB.pdfiim_build((g["Ai"], g["Aj"], g["Av"]), 0.01, 2, 2, 1, -1, "I", "B")
+    for k in ("Gi", "Gj", "Gv", "Hi", "Hj", "Hv", "IDv"):
+        assert np.array_equal(F[k], g["pdfiim_" + k]), k
+
+
+@pytest.mark.skipif(not O.have_ref("pdfiim"), reason="oracle/_ref not built")
+@pytest.mark.parametrize("params", [(1, 1, 1, -1, "I"), (3, 2, 2, -1, "1"), (2, 3, 2, 9, "2"), (2, 2, 1, 5, "I")])
+def test_host_pdfiim_matches_live_reference(params):
+    pf, lf, po, ws, ft = params
+    rng = np.random.default_rng(pf * 7 + lf)
+    A = FB.gen_convdiff2d(30, float(rng.uniform(0.2, 4)), float(rng.uniform(0, 6.2)), 0.9)
+    R = O.pdfiim_build(A, 0.05, pf, lf, po, ws, ft, "B")
+    M = FB.pdfiim_build(A, 0.05, pf, lf, po, ws, ft, "B")
+    for k in ("Gi", "Gj", "Gv", "Hi", "Hj", "Hv", "IDv"):
+        assert np.array_equal(R[k], M[k]), k
+
+
+def test_host_pdfiim_rejects_unserved_patterns():
+    A = FB.gen_poisson2d(4)
+    for patt in "LU":
+        with pytest.raises(FB.FiimError):
+            FB.pdfiim_build(A, 0.05, patt=patt)
