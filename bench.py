@@ -216,6 +216,42 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------- GPU arm
+def run_e2e(args, A, F, b, n, ws, dist):
+    """Steps through fiim_EPBiCGSTAB_pdfiim with pinned host arrays (uploads and download inside)."""
+    import torch
+    import fiim_b200 as FB
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    hA = [pin(a) for a in A]
+    hG = [pin(F[k]) for k in ("Gi", "Gj", "Gv")]
+    hH = [pin(F[k]) for k in ("Hi", "Hj", "Hv")]
+    hD, hb = pin(F["IDv"]), pin(b)
+    hx = torch.zeros(n, dtype=torch.float64).pin_memory()
+    L = FB.lib()
+    resval, it, info = C.c_double(0), C.c_int(0), C.c_int(0)
+    P = lambda t: C.c_void_p(t.data_ptr())
+
+    def e2e_call():
+        hx.zero_()
+        rc = L.fiim_EPBiCGSTAB_pdfiim(C.c_int(n), 0, P(hA[2]), P(hA[1]), P(hA[0]), P(hb), C.c_double(1e-8), 1200,
+                                      P(hG[2]), P(hG[1]), P(hG[0]), P(hD), P(hH[2]), P(hH[1]), P(hH[0]), P(hx),
+                                      C.byref(resval), C.byref(it), 0, C.byref(info))
+        FB._check(rc)
+    for _ in range(args.warmup):
+        e2e_call()
+    barrier(dist)
+    e_times = []
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        e2e_call()
+        e_times.append(time.perf_counter() - t1)
+    e_tot = max_over_ranks(dist, sum(e_times))
+    h2d = sum(int(t.numel() * t.element_size()) for t in hA + hG + hH + [hD, hb, hx])
+    return {"value": args.steps * ws / e_tot, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": 8 * n, "timing": "host wall clock around the blocking call",
+           "iter": it.value, "info": info.value}
+
+
+
 def run_ours(args):
     import torch
     import fiim_b200 as FB
@@ -276,35 +312,9 @@ def run_ours(args):
     S.close()
 
     # ---- e2e: reference-facing C-ABI call with pinned host arrays
-    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
-    hA = [pin(a) for a in A]
-    hG = [pin(F[k]) for k in ("Gi", "Gj", "Gv")]
-    hH = [pin(F[k]) for k in ("Hi", "Hj", "Hv")]
-    hD, hb = pin(F["IDv"]), pin(b)
-    hx = torch.zeros(n, dtype=torch.float64).pin_memory()
-    L = FB.lib()
-    resval, it, info = C.c_double(0), C.c_int(0), C.c_int(0)
-    P = lambda t: C.c_void_p(t.data_ptr())
-
-    def e2e_call():
-        hx.zero_()
-        rc = L.fiim_EPBiCGSTAB_pdfiim(C.c_int(n), 0, P(hA[2]), P(hA[1]), P(hA[0]), P(hb), C.c_double(1e-8), 1200,
-                                      P(hG[2]), P(hG[1]), P(hG[0]), P(hD), P(hH[2]), P(hH[1]), P(hH[0]), P(hx),
-                                      C.byref(resval), C.byref(it), 0, C.byref(info))
-        FB._check(rc)
-    for _ in range(args.warmup):
-        e2e_call()
-    barrier(dist)
-    e_times = []
-    for _ in range(args.steps):
-        t1 = time.perf_counter()
-        e2e_call()
-        e_times.append(time.perf_counter() - t1)
-    e_tot = max_over_ranks(dist, sum(e_times))
-    h2d = sum(int(t.numel() * t.element_size()) for t in hA + hG + hH + [hD, hb, hx])
-    e2e = {"value": args.steps * ws / e_tot, "unit": "solves/s", "h2d_bytes_per_step": h2d,
-           "d2h_bytes_per_step": 8 * n, "timing": "host wall clock around the blocking call",
-           "iter": it.value, "info": info.value}
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, A, F, b, n, ws, dist)
 
     # ---- CPU baseline (rank 0, N = 1): bounded sample of the reference's solve
     cpu = None
@@ -347,6 +357,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=128, help="grid side of the 3D convection-diffusion system")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI leg")
     ap.add_argument("--cpu-sample-its", type=int, default=12)
     ap.add_argument("--ref-sample-its", type=int, default=10)
     ap.add_argument("--ref-iters", type=int, default=99,

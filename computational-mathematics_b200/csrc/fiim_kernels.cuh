@@ -126,6 +126,7 @@ __device__ __forceinline__ void grid_reduce(double (&v)[NR], double *__restrict_
 struct EpiStore {
     static constexpr int NR = 1;   // unused slot (arrays need a positive size)
     static constexpr bool REDUCES = false;
+    static constexpr bool GATED = true;    // returns at once when the solve is done
     double *y;
     __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = s; }
     __device__ void finish(DState *, const double *) const {}
@@ -133,6 +134,7 @@ struct EpiStore {
 struct EpiScale {                  // y = d o (M x): the D^{-1} scaling of the preconditioner
     static constexpr int NR = 1;
     static constexpr bool REDUCES = false;
+    static constexpr bool GATED = true;    // returns at once when the solve is done
     double *y;
     const double *__restrict__ d;
     __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = __ldg(d + i) * s; }
@@ -141,6 +143,7 @@ struct EpiScale {                  // y = d o (M x): the D^{-1} scaling of the p
 struct EpiNorm {                   // y = M x, ||y||^2 -> st->pc2 (stagnation test)
     static constexpr int NR = 1;
     static constexpr bool REDUCES = true;
+    static constexpr bool GATED = true;    // returns at once when the solve is done
     double *y;
     __device__ void emit(long i, double s, double (&r)[NR]) const { y[i] = s; r[0] += s * s; }
     __device__ void finish(DState *st, const double *t) const { st->pc2 = t[0]; }
@@ -148,6 +151,7 @@ struct EpiNorm {                   // y = M x, ||y||^2 -> st->pc2 (stagnation te
 struct EpiAlpha {                  // v = A pc, alpha = m1 / (r0 . v)
     static constexpr int NR = 1;
     static constexpr bool REDUCES = true;
+    static constexpr bool GATED = true;    // returns at once when the solve is done
     double *y;
     const double *__restrict__ r0;
     __device__ void emit(long i, double s, double (&r)[NR]) const {
@@ -168,6 +172,7 @@ struct EpiAlpha {                  // v = A pc, alpha = m1 / (r0 . v)
 struct EpiOmega {                  // t = A sc, omega = (t . s) / (t . t)
     static constexpr int NR = 2;
     static constexpr bool REDUCES = true;
+    static constexpr bool GATED = true;    // returns at once when the solve is done
     double *y;
     const double *__restrict__ sv;
     __device__ void emit(long i, double s, double (&r)[NR]) const {
@@ -188,6 +193,7 @@ struct FinInit;
 struct EpiInit {
     static constexpr int NR = 1;
     static constexpr bool REDUCES = true;
+    static constexpr bool GATED = true;    // returns at once when the solve is done
     const double *__restrict__ b;
     double *p, *r0, *r;
     __device__ void emit(long i, double s, double (&red)[NR]) const {
@@ -203,6 +209,7 @@ struct EpiInit {
 struct EpiResid {
     static constexpr int NR = 2;
     static constexpr bool REDUCES = true;
+    static constexpr bool GATED = false;  // runs after the solve has finished
     const double *__restrict__ b;
     double *r;
     __device__ void emit(long i, double s, double (&red)[NR]) const {
@@ -221,6 +228,7 @@ struct EpiResid {
 struct EpiSubFrom {                // y = a - (M x)            (vdSub after a product)
     static constexpr int NR = 1;
     static constexpr bool REDUCES = false;
+    static constexpr bool GATED = true;    // returns at once when the solve is done
     double *y;
     const double *__restrict__ a;
     __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = a[i] - s; }
@@ -229,6 +237,7 @@ struct EpiSubFrom {                // y = a - (M x)            (vdSub after a pr
 struct EpiAccum {                  // y = (M x) + y            (mkl_sparse_d_mv with beta = 1)
     static constexpr int NR = 1;
     static constexpr bool REDUCES = false;
+    static constexpr bool GATED = true;    // returns at once when the solve is done
     double *y;
     __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = s + y[i]; }
     __device__ void finish(DState *, const double *) const {}
@@ -236,6 +245,7 @@ struct EpiAccum {                  // y = (M x) + y            (mkl_sparse_d_mv 
 struct EpiAccumScale {             // y = (M x) + y; z = y o d (last relaxation step, then vdMul)
     static constexpr int NR = 1;
     static constexpr bool REDUCES = false;
+    static constexpr bool GATED = true;    // returns at once when the solve is done
     double *y, *z;
     const double *__restrict__ d;
     __device__ void emit(long i, double s, double (&)[NR]) const {
@@ -248,6 +258,7 @@ struct EpiAccumScale {             // y = (M x) + y; z = y o d (last relaxation 
 struct EpiAccumNorm {              // y = (M x) + y, ||y||^2 -> st->pc2
     static constexpr int NR = 1;
     static constexpr bool REDUCES = true;
+    static constexpr bool GATED = true;    // returns at once when the solve is done
     double *y;
     __device__ void emit(long i, double s, double (&r)[NR]) const {
         const double t = s + y[i];
@@ -267,7 +278,7 @@ template <int VEC, typename V, typename Epi, int FILL = 0>
 static __global__ void __launch_bounds__(kThreads)
 k_spmv(CsrView<V> M, const double *__restrict__ x, Epi epi, DState *st,
        double *__restrict__ partials) {
-    if (st != nullptr && st->done) return;
+    if (Epi::GATED && st != nullptr && st->done) return;
     constexpr int RPW = 32 / VEC;
     const int lane = threadIdx.x & 31;
     const int sub = lane / VEC, lir = lane % VEC;

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <iostream>
@@ -418,7 +419,12 @@ int Solver::build_graph() {
         FIIM_CUDA(cudaStreamSynchronize(stream));
     }
     // Preferred: one graph whose WHILE node repeats the iteration body on the device.
+    // FIIM_GRAPH=host selects the host-driven graph (same kernels, same shapes), e.g.
+    // for profilers that replay graph kernel nodes one by one.
+    const char *mode_env = std::getenv("FIIM_GRAPH");
+    const bool want_cond = !(mode_env && std::strcmp(mode_env, "host") == 0);
     do {
+        if (!want_cond) break;
         cudaGraph_t g = nullptr;
         if (cudaGraphCreate(&g, 0) != cudaSuccess) break;
         cudaGraphConditionalHandle h;

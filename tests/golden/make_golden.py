@@ -50,11 +50,26 @@ def probe(A, F, n, sym=False, nr=None):
 
 
 def solved(prefix, variant, A, b, F, tol, nmax, **kw):
+    """One-thread reference run (bit-identical to the restatement) plus its rounding envelope:
+    the same solve with the shim's reductions split over 2..8 OpenMP threads, which changes
+    only the summation order of the dot products and norms."""
+    O.set_threads(1, variant)
     x, res, it, info = O.ref_solve(variant, A, b, F, tol=tol, nmax=nmax, **kw)
     xr, resr, itr, infor = O.bicgstab(variant, A, b, F, tol=tol, nmax=nmax, **kw)
     assert np.array_equal(x, xr) and res == resr and it == itr and info == infor, "restatement drifted"
+    its, spread, infos = [it], 0.0, {info}
+    for t in range(2, 9):
+        O.set_threads(t, variant)
+        xt, _, itt, inft = O.ref_solve(variant, A, b, F, tol=tol, nmax=nmax, **kw)
+        its.append(itt)
+        infos.add(inft)
+        spread = max(spread, float(np.linalg.norm(xt - x) / np.linalg.norm(x)))
+    O.set_threads(1, variant)
     return {f"{prefix}x": x, f"{prefix}resval": np.float64(res), f"{prefix}iter": np.int32(it),
-            f"{prefix}info": np.int32(info)}, {"resval": res, "iter": it, "info": info}
+            f"{prefix}info": np.int32(info), f"{prefix}iter_env": np.array([min(its), max(its)], np.int32),
+            f"{prefix}x_spread": np.float64(spread)}, \
+        {"resval": res, "iter": it, "info": info, "iter_env": [min(its), max(its)], "x_spread": spread,
+         "infos": sorted(infos)}
 
 
 def save(name, arrays, meta):
@@ -135,7 +150,8 @@ def main():
           "factors": "acifim dtol1 0.1 dtol2 0.05 (driver defaults otherwise), nr 2", "results": res})
 
     # 5. PDFIIM symmetric input: Poisson 32x32 stored as its upper triangle (mtype SYMMETRIC);
-    #    G from pdfiim on the full matrix, applied as G^T D^{-1} G... per PDFIIM/src/bicgstab.cpp:189-194.
+    #    G from pdfiim on the full matrix; the solver applies z = G (D^{-1} o (G^T r)) as
+    #    PDFIIM/src/bicgstab.cpp:189-194 does.
     Af = FB.gen_poisson2d(32)
     F = O.pdfiim_build(Af, 0.05, 2, 2, 1, -1, "I", "B")
     Ai, Aj, Av = Af

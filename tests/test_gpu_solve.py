@@ -3,8 +3,12 @@
 Every check goes through the C-ABI of libfiim_b200.so. Tolerances:
   * SpMV and preconditioner application on the same vector: 1e-12 relative (FP64; the
     GPU sums each row as a lane tree with FMA, the oracle left to right).
-  * Solves: the same info code, iteration count within +-2, the tolerance reached
-    (resval < tol when converged), and the solution close to the reference's.
+  * Solves: the same info code; the iteration count within +-2 of the reference's
+    rounding envelope (the reference's own counts when only the summation order of its
+    dot products changes: the MKL shim's reductions split over 1..8 OpenMP threads,
+    recorded in tests/golden); the tolerance reached (resval < tol when converged); the
+    solution within 10x the reference's own solution spread, and a true residual no
+    worse than 10x the reference's.
 """
 import numpy as np
 import pytest
@@ -80,16 +84,16 @@ def test_prec_apply_ignores_entries_outside_triangles(cuda):
 
 
 SOLVES = [
-    ("sherman2", "afiim9e-6_", "afiim9e-6_", "afiim", {}, 500, 1e-6),
-    ("sherman2", "afiim0.1_", "afiim0.1_", "afiim", {}, 500, 1e-4),
-    ("sherman2", "acifim_", "acifimE_", "acifim", {"mode": "E", "nr": 2}, 2000, 1e-4),
-    ("sherman2", "acifim_", "acifimC_", "acifim", {"mode": "C", "nr": 2}, 2000, 1e-4),
-    ("sherman2", "pdfiim_", "pdfiim_", "pdfiim", {}, 1200, 1e-3),
-    ("poisson128_afiim", "", "", "afiim", {}, 1000, 1e-6),
-    ("convdiff16_pdfiim", "", "", "pdfiim", {}, 1200, 1e-6),
-    ("convdiff2d48_acifim", "", "E_", "acifim", {"mode": "E", "nr": 2}, 2000, 1e-6),
-    ("convdiff2d48_acifim", "", "C_", "acifim", {"mode": "C", "nr": 2}, 2000, 1e-6),
-    ("poisson32_sym_pdfiim", "", "", "pdfiim", {"issym": True}, 1200, 1e-6),
+    ("sherman2", "afiim9e-6_", "afiim9e-6_", "afiim", {}, 500),
+    ("sherman2", "afiim0.1_", "afiim0.1_", "afiim", {}, 500),
+    ("sherman2", "acifim_", "acifimE_", "acifim", {"mode": "E", "nr": 2}, 2000),
+    ("sherman2", "acifim_", "acifimC_", "acifim", {"mode": "C", "nr": 2}, 2000),
+    ("sherman2", "pdfiim_", "pdfiim_", "pdfiim", {}, 1200),
+    ("poisson128_afiim", "", "", "afiim", {}, 1000),
+    ("convdiff16_pdfiim", "", "", "pdfiim", {}, 1200),
+    ("convdiff2d48_acifim", "", "E_", "acifim", {"mode": "E", "nr": 2}, 2000),
+    ("convdiff2d48_acifim", "", "C_", "acifim", {"mode": "C", "nr": 2}, 2000),
+    ("poisson32_sym_pdfiim", "", "", "pdfiim", {"issym": True}, 1200),
 ]
 
 
@@ -107,21 +111,35 @@ def dropin(variant, g, F, nmax, x, tol=1e-8, mode="E", nr=1, issym=False):
                         F.get("Ui"), nr, mode, x)
 
 
-@pytest.mark.parametrize("name,fprefix,rprefix,variant,kw,nmax,xtol", SOLVES)
-def test_dropin_solve_matches_reference(golden, name, fprefix, rprefix, variant, kw, nmax, xtol):
+def true_relres(g, x):
+    n = len(g["b"])
+    A = sp.csr_matrix((g["Av"], g["Aj"], g["Ai"]), shape=(n, n))
+    if "sym" in g["meta"]["system"].lower() or "SYMMETRIC" in g["meta"]["system"]:
+        A = A + sp.triu(A, 1).T
+    return np.linalg.norm(g["b"] - A @ x) / np.linalg.norm(g["b"])
+
+
+@pytest.mark.parametrize("name,fprefix,rprefix,variant,kw,nmax", SOLVES)
+def test_dropin_solve_matches_reference(golden, name, fprefix, rprefix, variant, kw, nmax):
+    """Same info; iterations within +-2 of the reference's rounding envelope (its own counts
+    when only the summation order of its reductions changes, OpenMP 1..8 threads); the
+    tolerance reached; x within the reference's own solution spread (x 10, floor 1e-9) and
+    a true residual no worse than 10x the reference's."""
     g = golden(name)
     F = sub(g, fprefix)
     x = np.zeros(len(g["b"]))
     resval, it, info = dropin(variant, g, F, nmax, x, **kw)
     ref_it, ref_info = int(g[rprefix + "iter"]), int(g[rprefix + "info"])
-    print(f"{name}/{rprefix or variant}: gpu iter {it} info {info} resval {resval:.3e} | "
-          f"ref iter {ref_it} info {ref_info} resval {float(g[rprefix + 'resval']):.3e} | "
-          f"x rel diff {rel(x, g[rprefix + 'x']):.2e}")
+    lo, hi = (int(v) for v in g[rprefix + "iter_env"])
+    dx = rel(x, g[rprefix + "x"])
+    print(f"{name}/{rprefix or variant}: gpu iter {it} info {info} resval {resval:.3e} | ref iter {ref_it} "
+          f"envelope [{lo},{hi}] info {ref_info} | x rel diff {dx:.2e} (ref spread {float(g[rprefix + 'x_spread']):.2e})")
     assert info == ref_info
-    assert abs(it - ref_it) <= 2
+    assert lo - 2 <= it <= hi + 2
     if ref_info == 0:
         assert resval < 1e-8
-    assert rel(x, g[rprefix + "x"]) <= xtol
+    assert dx <= 10 * float(g[rprefix + "x_spread"]) + 1e-9
+    assert true_relres(g, x) <= 10 * true_relres(g, g[rprefix + "x"]) + 1e-12
 
 
 @pytest.mark.parametrize("memory", ["host", "device"])
@@ -217,4 +235,6 @@ def test_convdiff64_host_factors_match_oracle():
     print("64^3:", r, "oracle", ito, infoo, reso)
     assert r["info"] == infoo == 0 and abs(r["iter"] - ito) <= 2
     assert r["true_relres"] < 1e-7 and rel(x, xo) < 1e-6
+    tr = np.linalg.norm(b - sp.csr_matrix((A[2], A[1], A[0])) @ x) / np.linalg.norm(b)
+    assert abs(tr - r["true_relres"]) <= 1e-3 * tr
     S.close()
