@@ -178,6 +178,11 @@ int fiim_solver_spmv_shape(fiim_solver_t h, int which, int *vec) {
     return FIIM_OK;
 }
 
+int fiim_solver_apply(fiim_solver_t h, int op, const double *x, double *y) {
+    if (!h || fiim_is_mixed(h) || !x || !y) return fiim::set_error(FIIM_EARG, "bad argument");
+    return reinterpret_cast<fiim::Solver *>(h)->apply(op, x, y);
+}
+
 int fiim_solver_kernel_times(fiim_solver_t h, int reps, int max_kernels, double *ms, double *bytes,
                              char *names, int name_len) {
     if (!h || fiim_is_mixed(h) || !ms || !bytes || reps < 1) return fiim::set_error(FIIM_EARG, "bad argument");

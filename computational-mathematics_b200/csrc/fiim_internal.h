@@ -51,9 +51,17 @@ struct DevCsr {
     double *v = nullptr;
     float *v32 = nullptr;
     __nv_bfloat16 *v16 = nullptr;
-    int vec = 8;                 // lanes per row of the SpMV
+    int vec = 8;                 // lanes per row of the set-up-free SpMV
+    int tile = 2048;             // entries per row block of the CSR-stream SpMV
+    int *rb = nullptr;           // row-block starts (device), nblk + 1 entries
+    int nblk = 0;
+    std::vector<int> hrp;        // row offsets on the host (row blocks, tuning key)
     std::vector<long> sig;       // tuning-cache key: n, nnz, sampled row offsets
 };
+
+// Row blocks of a CSR matrix: consecutive rows, at most max_rows of them, whose entries
+// total at most tile; a row with more than tile entries forms a block by itself.
+void build_row_blocks(const std::vector<int> &rp, int tile, int max_rows, std::vector<int> &rb);
 
 // Host CSR (owning), used for symmetric expansion and transposes.
 struct HostCsr {

@@ -1,8 +1,8 @@
-// Device kernels of the BiCGSTAB solve phase (sm_100a).
+// Device kernels of the FP64 BiCGSTAB solve phase (sm_100a).
 //
 // One BiCGSTAB iteration of the reference (AFIIM/src/bicgstab.cpp:168-275) is nine
-// launches here, each a single pass over HBM with the BLAS-1 work and the scalar
-// recurrences fused in:
+// launches, each one pass over HBM with the BLAS-1 work and the scalar recurrences
+// fused in:
 //   K1 tm = IDv o (H p)                 spmv, scale epilogue        (:172-173)
 //   K2 pc = G tm,  sum pc^2             spmv, norm epilogue         (:175, :201)
 //   K3 v = A pc,   alpha = m1/(r0.v)    spmv, dot epilogue          (:178, :181)
@@ -12,10 +12,21 @@
 //   K7 t = A sc,   omega = t.s / t.t    spmv, 2-dot epilogue        (:195, :198)
 //   K8 x += alpha pc + omega sc, r = s - omega t, m1 = r0.r, tests  (:207-267)
 //   K9 p = r + beta (p - omega v)                                   (:270-271)
-// Reductions are deterministic: each block reduces in a fixed tree, writes one partial,
-// and the last block to finish (ticket counter) sums the partials in block order and
-// applies the scalar step. A kernel launched after the solve finished returns at once
-// (st->done), so iterations can be launched ahead of the host's convergence check.
+//
+// Rounding: every vector the reference computes is computed here with the same
+// operations in the same order: each SpMV row is summed left to right in storage
+// order with the product rounded before the add (as the MKL restatement in the oracle
+// and as a CSR loop without FMA contraction), and every axpy / axpby / vdMul rounds the
+// products and sums separately (explicit __dmul_rn / __dadd_rn, never FMA). Given the
+// same scalars, the GPU's vectors are bit-identical to the reference's. The scalars
+// come from dot products and norms, whose summation order is parallel here (a fixed
+// tree, deterministic run to run) and left to right in the reference; that is the only
+// source of difference.
+//
+// Reductions: each block reduces in a fixed tree and writes one partial; the last
+// block to finish (ticket counter) sums the partials in block order and applies the
+// scalar step. A gated kernel launched after the solve finished returns at once
+// (st->done), so iterations can run ahead of any host check.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -31,7 +42,7 @@ constexpr int kWarps = kThreads / 32;
 struct DState {
     double ro, rc, m1, m2, alpha, omega, beta, tol, eps;
     double pc2, x2, r2;        // ||pc||^2, ||x||^2, ||r||^2 of the current iteration
-    double ts, tt, r0v;        // last dot products (inspection)
+    double ts, tt, r0v;        // last dot products (inspection; true residual after a solve)
     int iter, nmax, stag, msteps, maxmsteps, info, done, alpha_guard;
     unsigned int ticket;       // last-block counter, reset by the last block
     int loops;                 // iteration bodies run by the device loop (guard + accounting)
@@ -121,37 +132,51 @@ __device__ __forceinline__ void grid_reduce(double (&v)[NR], double *__restrict_
     }
 }
 
+// ---------------------------------------------------------------- scalar steps
+struct FinInit {   // ro = ||r0||, m1 = ro^2, rc = ro (AFIIM/src/bicgstab.cpp:161-165)
+    __device__ void finish(DState *st, const double *t) const {
+        st->ro = sqrt(t[0]);
+        st->m1 = st->ro * st->ro;
+        st->rc = st->ro;
+        st->iter = 0;
+        st->stag = 0;
+        st->msteps = 0;
+        if (st->nmax <= 0) {
+            st->done = 1;
+            if (st->nmax == 0) st->info = 3;
+        }
+    }
+};
+
 // ---------------------------------------------------------------- SpMV epilogues
 // emit(row, sum, red) stores the row result and adds its share to the reductions.
-struct EpiStore {
-    static constexpr int NR = 1;   // unused slot (arrays need a positive size)
-    static constexpr bool REDUCES = false;
-    static constexpr bool GATED = true;    // returns at once when the solve is done
+// GATED kernels return at once once the solve is done.
+#define FIIM_EPI(nr, reduces, gated)              \
+    static constexpr int NR = nr;                 \
+    static constexpr bool REDUCES = reduces;      \
+    static constexpr bool GATED = gated
+
+struct EpiStore {                  // y = M x
+    FIIM_EPI(1, false, true);
     double *y;
     __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = s; }
     __device__ void finish(DState *, const double *) const {}
 };
-struct EpiScale {                  // y = d o (M x): the D^{-1} scaling of the preconditioner
-    static constexpr int NR = 1;
-    static constexpr bool REDUCES = false;
-    static constexpr bool GATED = true;    // returns at once when the solve is done
+struct EpiScale {                  // y = d o (M x): vdMul(n, IDv, pc, tm), AFIIM/src/bicgstab.cpp:173
+    FIIM_EPI(1, false, true);
     double *y;
     const double *__restrict__ d;
-    __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = __ldg(d + i) * s; }
+    __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = __dmul_rn(__ldg(d + i), s); }
     __device__ void finish(DState *, const double *) const {}
 };
 struct EpiNorm {                   // y = M x, ||y||^2 -> st->pc2 (stagnation test)
-    static constexpr int NR = 1;
-    static constexpr bool REDUCES = true;
-    static constexpr bool GATED = true;    // returns at once when the solve is done
+    FIIM_EPI(1, true, true);
     double *y;
     __device__ void emit(long i, double s, double (&r)[NR]) const { y[i] = s; r[0] += s * s; }
     __device__ void finish(DState *st, const double *t) const { st->pc2 = t[0]; }
 };
 struct EpiAlpha {                  // v = A pc, alpha = m1 / (r0 . v)
-    static constexpr int NR = 1;
-    static constexpr bool REDUCES = true;
-    static constexpr bool GATED = true;    // returns at once when the solve is done
+    FIIM_EPI(1, true, true);
     double *y;
     const double *__restrict__ r0;
     __device__ void emit(long i, double s, double (&r)[NR]) const {
@@ -170,9 +195,7 @@ struct EpiAlpha {                  // v = A pc, alpha = m1 / (r0 . v)
     }
 };
 struct EpiOmega {                  // t = A sc, omega = (t . s) / (t . t)
-    static constexpr int NR = 2;
-    static constexpr bool REDUCES = true;
-    static constexpr bool GATED = true;    // returns at once when the solve is done
+    FIIM_EPI(2, true, true);
     double *y;
     const double *__restrict__ sv;
     __device__ void emit(long i, double s, double (&r)[NR]) const {
@@ -186,30 +209,25 @@ struct EpiOmega {                  // t = A sc, omega = (t . s) / (t . t)
         st->omega = t[0] / t[1];
     }
 };
-
-struct FinInit;
 // Fused start of the solve (AFIIM/src/bicgstab.cpp:151-161): with s = (A x)_i,
-// p = b - s; r0 = p; r = p; sum r0^2 -> ro, m1 = ro^2, rc = ro.
+// p = b + (-1) s; r0 = p; r = p; sum r0^2 -> ro, m1 = ro^2, rc = ro.
 struct EpiInit {
-    static constexpr int NR = 1;
-    static constexpr bool REDUCES = true;
-    static constexpr bool GATED = true;    // returns at once when the solve is done
+    FIIM_EPI(1, true, true);
     const double *__restrict__ b;
     double *p, *r0, *r;
     __device__ void emit(long i, double s, double (&red)[NR]) const {
-        const double pi = b[i] + (-1.0) * s;
+        const double pi = __dadd_rn(b[i], __dmul_rn(-1.0, s));
         p[i] = pi;
         r0[i] = pi;
         r[i] = pi;
         red[0] += pi * pi;
     }
-    __device__ void finish(DState *st, const double *t) const;
+    __device__ void finish(DState *st, const double *t) const { FinInit{}.finish(st, t); }
 };
-// True residual r = b - A x in FP64, sum r^2 and sum b^2 -> st->ts, st->tt.
+// True residual r = b - A x in FP64, sum r^2 and sum b^2 -> st->ts, st->tt. Runs after
+// the solve has finished, so it is not gated.
 struct EpiResid {
-    static constexpr int NR = 2;
-    static constexpr bool REDUCES = true;
-    static constexpr bool GATED = false;  // runs after the solve has finished
+    FIIM_EPI(2, true, false);
     const double *__restrict__ b;
     double *r;
     __device__ void emit(long i, double s, double (&red)[NR]) const {
@@ -223,65 +241,106 @@ struct EpiResid {
         st->tt = t[1];
     }
 };
-
 // ACIFIM mode 'C' pieces (ACIFIM/src/bicgstab.cpp:395-420).
 struct EpiSubFrom {                // y = a - (M x)            (vdSub after a product)
-    static constexpr int NR = 1;
-    static constexpr bool REDUCES = false;
-    static constexpr bool GATED = true;    // returns at once when the solve is done
+    FIIM_EPI(1, false, true);
     double *y;
     const double *__restrict__ a;
-    __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = a[i] - s; }
+    __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = __dadd_rn(a[i], -s); }
     __device__ void finish(DState *, const double *) const {}
 };
 struct EpiAccum {                  // y = (M x) + y            (mkl_sparse_d_mv with beta = 1)
-    static constexpr int NR = 1;
-    static constexpr bool REDUCES = false;
-    static constexpr bool GATED = true;    // returns at once when the solve is done
+    FIIM_EPI(1, false, true);
     double *y;
-    __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = s + y[i]; }
+    __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = __dadd_rn(s, y[i]); }
     __device__ void finish(DState *, const double *) const {}
 };
 struct EpiAccumScale {             // y = (M x) + y; z = y o d (last relaxation step, then vdMul)
-    static constexpr int NR = 1;
-    static constexpr bool REDUCES = false;
-    static constexpr bool GATED = true;    // returns at once when the solve is done
+    FIIM_EPI(1, false, true);
     double *y, *z;
     const double *__restrict__ d;
     __device__ void emit(long i, double s, double (&)[NR]) const {
-        const double t = s + y[i];
+        const double t = __dadd_rn(s, y[i]);
         y[i] = t;
-        z[i] = t * __ldg(d + i);
+        z[i] = __dmul_rn(t, __ldg(d + i));
     }
     __device__ void finish(DState *, const double *) const {}
 };
 struct EpiAccumNorm {              // y = (M x) + y, ||y||^2 -> st->pc2
-    static constexpr int NR = 1;
-    static constexpr bool REDUCES = true;
-    static constexpr bool GATED = true;    // returns at once when the solve is done
+    FIIM_EPI(1, true, true);
     double *y;
     __device__ void emit(long i, double s, double (&r)[NR]) const {
-        const double t = s + y[i];
+        const double t = __dadd_rn(s, y[i]);
         y[i] = t;
         r[0] += t * t;
     }
     __device__ void finish(DState *st, const double *t) const { st->pc2 = t[0]; }
 };
 
-// ---------------------------------------------------------------- CSR SpMV
-// VEC lanes per row (2..32), 32/VEC rows per warp, grid-stride over row groups so a
-// fixed grid (a multiple of the SM count) covers any n. Column indices and values
-// are loaded coalesced across the lanes; x is gathered through the read-only path.
-// FILL 0 uses every stored entry; 1 keeps col >= row and 2 keeps col <= row (MKL's
-// TRIANGULAR descriptors) for callers whose factors were not filtered at upload.
-template <int VEC, typename V, typename Epi, int FILL = 0>
+// ---------------------------------------------------------------- CSR-stream SpMV
+// Rows are grouped at set-up into row blocks: consecutive rows, at most kThreads of
+// them, whose entries total at most TILE; a row longer than TILE is a block of its
+// own. A CTA takes row blocks in grid-stride order. For each block it streams the
+// entries coalesced (columns and values with evict-first loads, x gathered through the
+// read-only path), stores the rounded products v*x in shared memory, then each thread
+// sums its own row's products left to right. A long row is summed by one thread over
+// TILE-sized chunks, still in storage order.
+template <int TILE, typename Epi>
 static __global__ void __launch_bounds__(kThreads)
-k_spmv(CsrView<V> M, const double *__restrict__ x, Epi epi, DState *st,
-       double *__restrict__ partials) {
+k_spmv_rows(CsrView<double> M, const int *__restrict__ rb, int nblk, const double *__restrict__ x,
+            Epi epi, DState *st, double *__restrict__ partials) {
+    if (Epi::GATED && st != nullptr && st->done) return;
+    __shared__ double prod[TILE];
+    double red[Epi::NR];
+#pragma unroll
+    for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
+    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        const int r0 = __ldg(rb + blk), r1 = __ldg(rb + blk + 1);
+        const int e0 = __ldg(M.rp + r0), e1 = __ldg(M.rp + r1);
+        if (e1 - e0 <= TILE) {
+#pragma unroll 4
+            for (int e = e0 + (int)threadIdx.x; e < e1; e += kThreads)
+                prod[e - e0] = __dmul_rn(ldm(M.v + e), ldx(x + ldi(M.ci + e)));
+            __syncthreads();
+            const int r = r0 + (int)threadIdx.x;
+            if (r < r1) {
+                const int b = __ldg(M.rp + r) - e0, e = __ldg(M.rp + r + 1) - e0;
+                double s = 0.0;
+                for (int k = b; k < e; ++k) s = __dadd_rn(s, prod[k]);
+                epi.emit(r, s, red);
+            }
+            __syncthreads();
+        } else {
+            double s = 0.0;
+            for (int c0 = e0; c0 < e1; c0 += TILE) {
+                const int c1 = min(c0 + TILE, e1);
+                for (int e = c0 + (int)threadIdx.x; e < c1; e += kThreads)
+                    prod[e - c0] = __dmul_rn(ldm(M.v + e), ldx(x + ldi(M.ci + e)));
+                __syncthreads();
+                if (threadIdx.x == 0)
+                    for (int k = 0; k < c1 - c0; ++k) s = __dadd_rn(s, prod[k]);
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) epi.emit(r0, s, red);
+        }
+    }
+    if constexpr (Epi::REDUCES) grid_reduce<Epi::NR>(red, partials, st, epi);
+}
+
+// ---------------------------------------------------------------- CSR-vector SpMV
+// For callers without set-up (the kernel-level C-ABI): VEC lanes per row, 32/VEC rows
+// per warp, grid-stride over row groups. Each lane rounds its product; the group then
+// adds the products in storage order by broadcasting them lane by lane, so the sum is
+// the same as the left-to-right CSR loop for every VEC. FILL 0 uses every entry; 1
+// keeps col >= row and 2 keeps col <= row (MKL's TRIANGULAR descriptors).
+template <int VEC, typename Epi, int FILL = 0>
+static __global__ void __launch_bounds__(kThreads)
+k_spmv_vec(CsrView<double> M, const double *__restrict__ x, Epi epi, DState *st,
+           double *__restrict__ partials) {
     if (Epi::GATED && st != nullptr && st->done) return;
     constexpr int RPW = 32 / VEC;
     const int lane = threadIdx.x & 31;
-    const int sub = lane / VEC, lir = lane % VEC;
+    const int sub = lane / VEC, lir = lane % VEC, gbase = sub * VEC;
     const long warp = ((long)blockIdx.x * kThreads + threadIdx.x) >> 5;
     const long nwarps = ((long)gridDim.x * kThreads) >> 5;
     double red[Epi::NR];
@@ -289,19 +348,29 @@ k_spmv(CsrView<V> M, const double *__restrict__ x, Epi epi, DState *st,
     for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
     for (long base = warp * RPW; base < M.n; base += nwarps * RPW) {
         const long row = base + sub;
-        double s = 0.0;
+        int beg = 0, len = 0;
         if (row < M.n) {
-            const int beg = __ldg(M.rp + row), end = __ldg(M.rp + row + 1);
-            for (int k = beg + lir; k < end; k += VEC) {
-                const int c = ldi(M.ci + k);
-                const double a = (double)ldm(M.v + k);
-                if (FILL == 1 && c < row) continue;
-                if (FILL == 2 && c > row) continue;
-                s = fma(a, ldx(x + c), s);
+            beg = __ldg(M.rp + row);
+            len = __ldg(M.rp + row + 1) - beg;
+        }
+        const int trips = __reduce_max_sync(0xffffffffu, (len + VEC - 1) / VEC);
+        double s = 0.0;
+        for (int t = 0; t < trips; ++t) {
+            const int k = t * VEC + lir;
+            double p = 0.0;
+            int keep = 0;
+            if (k < len) {
+                const int c = ldi(M.ci + beg + k);
+                keep = !((FILL == 1 && c < row) || (FILL == 2 && c > row));
+                if (keep) p = __dmul_rn(ldm(M.v + beg + k), ldx(x + c));
+            }
+#pragma unroll
+            for (int j = 0; j < VEC; ++j) {
+                const double pj = __shfl_sync(0xffffffffu, p, gbase + j);
+                const int kj = __shfl_sync(0xffffffffu, keep, gbase + j);
+                if (kj) s = __dadd_rn(s, pj);
             }
         }
-#pragma unroll
-        for (int o = VEC / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (row < M.n && lir == 0) epi.emit(row, s, red);
     }
     if constexpr (Epi::REDUCES) grid_reduce<Epi::NR>(red, partials, st, epi);
@@ -312,23 +381,6 @@ k_spmv(CsrView<V> M, const double *__restrict__ x, Epi epi, DState *st,
 #define FIIM_FOR_ROWS(i, n) \
     for (long i = (long)blockIdx.x * kThreads + threadIdx.x; i < (n); i += (long)gridDim.x * kThreads)
 
-struct FinInit {   // ro = ||r0||, m1 = ro^2, rc = ro (AFIIM/src/bicgstab.cpp:161-165)
-    __device__ void finish(DState *st, const double *t) const {
-        st->ro = sqrt(t[0]);
-        st->m1 = st->ro * st->ro;
-        st->rc = st->ro;
-        st->iter = 0;
-        st->stag = 0;
-        st->msteps = 0;
-        if (st->nmax <= 0) {
-            st->done = 1;
-            if (st->nmax == 0) st->info = 3;
-        }
-    }
-};
-
-__device__ inline void EpiInit::finish(DState *st, const double *t) const { FinInit{}.finish(st, t); }
-
 struct FinS {
     __device__ void finish(DState *st, const double *t) const {
         st->r2 = t[0];
@@ -336,8 +388,9 @@ struct FinS {
     }
 };
 
-// s = r - alpha v; ||r||^2 (the residual norm the reference tests, before r is
-// updated: AFIIM/src/bicgstab.cpp:216) and ||x||^2 (stagnation test, :201).
+// s = r + (-alpha) v (cblas_dcopy + cblas_daxpy, AFIIM/src/bicgstab.cpp:184-185);
+// ||r||^2 (the residual norm the reference tests, taken before r is updated, :216)
+// and ||x||^2 (stagnation test, :201).
 static __global__ void __launch_bounds__(kThreads)
 k_update_s(long n, const double *__restrict__ r, const double *__restrict__ v,
            const double *__restrict__ x, double *__restrict__ s, DState *st,
@@ -347,7 +400,7 @@ k_update_s(long n, const double *__restrict__ r, const double *__restrict__ v,
     double red[2] = {0.0, 0.0};
     FIIM_FOR_ROWS(i, n) {
         const double ri = r[i], xi = x[i];
-        s[i] = ri + na * v[i];
+        s[i] = __dadd_rn(ri, __dmul_rn(na, v[i]));
         red[0] += ri * ri;
         red[1] += xi * xi;
     }
@@ -375,31 +428,33 @@ struct FinControl {
     }
 };
 
-// x += alpha pc; x += omega sc; r = s - omega t; sum r0 . r; then the tests.
+// x = x + alpha pc; x = x + omega sc; r = s + (-omega) t (AFIIM/src/bicgstab.cpp:207-259);
+// sum r0 . r; then the tests.
 static __global__ void __launch_bounds__(kThreads)
 k_update_xr(long n, const double *__restrict__ pc, const double *__restrict__ sc,
             const double *__restrict__ s, const double *__restrict__ t,
             const double *__restrict__ r0, double *__restrict__ x, double *__restrict__ r,
             DState *st, double *__restrict__ partials) {
     if (st->done) return;
-    const double a = st->alpha, om = st->omega;
+    const double a = st->alpha, om = st->omega, nom = -st->omega;
     double red[1] = {0.0};
     FIIM_FOR_ROWS(i, n) {
         double xi = x[i];
-        xi = xi + a * pc[i];
-        xi = xi + om * sc[i];
+        xi = __dadd_rn(xi, __dmul_rn(a, pc[i]));
+        xi = __dadd_rn(xi, __dmul_rn(om, sc[i]));
         x[i] = xi;
-        const double ri = s[i] + (-om) * t[i];
+        const double ri = __dadd_rn(s[i], __dmul_rn(nom, t[i]));
         r[i] = ri;
         red[0] += r0[i] * ri;
     }
     grid_reduce<1>(red, partials, st, FinControl{});
 }
 
-// p = (-beta omega) v + beta p; p += r (AFIIM/src/bicgstab.cpp:270-271).
-// In the device-driven loop this is the last kernel of the body: block 0 counts the
-// body, trips a guard (info -5) should the body ever run past nmax + 2 times, and
-// sets the WHILE node's condition to continue only while the solve is not done.
+// p = (-beta omega) v + beta p; p = p + r (cblas_daxpby + cblas_daxpy,
+// AFIIM/src/bicgstab.cpp:270-271). In the device-driven loop this is the last kernel of
+// the body: block 0 counts the body, trips a guard (info -5) should the body ever run
+// past nmax + 2 times, and sets the WHILE node's condition to continue only while the
+// solve is not done.
 static __global__ void __launch_bounds__(kThreads)
 k_update_p(long n, const double *__restrict__ r, const double *__restrict__ v,
            double *__restrict__ p, DState *st, cudaGraphConditionalHandle h, int cond) {
@@ -412,14 +467,17 @@ k_update_p(long n, const double *__restrict__ r, const double *__restrict__ v,
         cudaGraphSetConditional(h, st->done ? 0u : 1u);
     }
     if (st->done) return;
-    const double b = st->beta, c = -st->beta * st->omega;
-    FIIM_FOR_ROWS(i, n) { p[i] = (c * v[i] + b * p[i]) + r[i]; }
+    const double b = st->beta, c = __dmul_rn(-st->beta, st->omega);
+    FIIM_FOR_ROWS(i, n) {
+        const double pi = __dadd_rn(__dmul_rn(c, v[i]), __dmul_rn(b, p[i]));
+        p[i] = __dadd_rn(pi, r[i]);
+    }
 }
 
 // Count entries of a CSR matrix outside the kept triangle (upper: col < row is outside;
 // lower: col > row is outside).
 static __global__ void k_count_outside(int n, const int *__restrict__ rp, const int *__restrict__ ci,
-                                int upper, unsigned long long *count) {
+                                       int upper, unsigned long long *count) {
     unsigned long long c = 0;
     FIIM_FOR_ROWS(i, n) {
         for (int k = rp[i]; k < rp[i + 1]; ++k) {

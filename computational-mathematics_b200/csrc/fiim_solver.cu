@@ -128,24 +128,47 @@ int grid_for(K kernel, long units_per_block, long units) {
     return (int)std::min<long>(need, (long)occupancy(kernel) * num_sms());
 }
 
-template <int VEC, int FILL, typename V, typename Epi>
-static cudaError_t spmv_vec(cudaStream_t s, const CsrView<V> &M, const double *x, const Epi &epi,
+template <int VEC, int FILL, typename Epi>
+static cudaError_t spmv_vec(cudaStream_t s, const CsrView<double> &M, const double *x, const Epi &epi,
                             DState *st, double *partials) {
-    auto kern = k_spmv<VEC, V, Epi, FILL>;
+    auto kern = k_spmv_vec<VEC, Epi, FILL>;
     const int g = grid_for(kern, (32 / VEC) * kWarps, M.n);
     kern<<<g, kThreads, 0, s>>>(M, x, epi, st, partials);
     return cudaGetLastError();
 }
 
-template <int FILL = 0, typename V, typename Epi>
-cudaError_t launch_spmv(int vec, cudaStream_t s, const CsrView<V> &M, const double *x,
-                        const Epi &epi, DState *st, double *partials) {
+// Set-up-free SpMV (kernel-level C-ABI): VEC lanes per row, exact row order.
+template <int FILL = 0, typename Epi>
+cudaError_t launch_spmv_vec(int vec, cudaStream_t s, const CsrView<double> &M, const double *x,
+                            const Epi &epi, DState *st, double *partials) {
     switch (vec) {
         case 2: return spmv_vec<2, FILL>(s, M, x, epi, st, partials);
         case 4: return spmv_vec<4, FILL>(s, M, x, epi, st, partials);
         case 8: return spmv_vec<8, FILL>(s, M, x, epi, st, partials);
         case 16: return spmv_vec<16, FILL>(s, M, x, epi, st, partials);
         default: return spmv_vec<32, FILL>(s, M, x, epi, st, partials);
+    }
+}
+
+static CsrView<double> view(const DevCsr &M) { return CsrView<double>{M.rp, M.ci, M.v, (int)M.n}; }
+
+template <int TILE, typename Epi>
+static cudaError_t spmv_rows(cudaStream_t s, const DevCsr &M, const double *x, const Epi &epi,
+                             DState *st, double *partials) {
+    auto kern = k_spmv_rows<TILE, Epi>;
+    const int g = grid_for(kern, 1, M.nblk);
+    kern<<<g, kThreads, 0, s>>>(view(M), M.rb, M.nblk, x, epi, st, partials);
+    return cudaGetLastError();
+}
+
+// Solver SpMV: CSR-stream over the matrix's row blocks, exact row order.
+template <typename Epi>
+cudaError_t launch_spmv(const DevCsr &M, cudaStream_t s, const double *x, const Epi &epi, DState *st,
+                        double *partials) {
+    switch (M.tile) {
+        case 1024: return spmv_rows<1024>(s, M, x, epi, st, partials);
+        case 4096: return spmv_rows<4096>(s, M, x, epi, st, partials);
+        default: return spmv_rows<2048>(s, M, x, epi, st, partials);
     }
 }
 
@@ -159,32 +182,64 @@ int heuristic_vec(long n, long nnz) {
     return v;
 }
 
-static CsrView<double> view(const DevCsr &M) { return CsrView<double>{M.rp, M.ci, M.v, (int)M.n}; }
+void build_row_blocks(const std::vector<int> &rp, int tile, int max_rows, std::vector<int> &rb) {
+    const int n = (int)rp.size() - 1;
+    rb.clear();
+    rb.push_back(0);
+    int r = 0;
+    while (r < n) {
+        if (rp[r + 1] - rp[r] > tile) {
+            rb.push_back(++r);
+            continue;
+        }
+        const int start = r;
+        long nnz = 0;
+        while (r < n && r - start < max_rows && nnz + (rp[r + 1] - rp[r]) <= tile) {
+            nnz += rp[r + 1] - rp[r];
+            ++r;
+        }
+        rb.push_back(r);
+    }
+}
 
-// Time each lane count on this matrix and keep the fastest; cached by signature.
-static int autotune_vec(const DevCsr &M, const double *x, double *y, cudaStream_t s) {
+static int set_tile(DevCsr &M, int tile, cudaStream_t s) {
+    std::vector<int> rb;
+    build_row_blocks(M.hrp, tile, kThreads, rb);
+    M.tile = tile;
+    M.nblk = (int)rb.size() - 1;
+    FIIM_CUDA(cudaMemcpyAsync(M.rb, rb.data(), sizeof(int) * rb.size(), cudaMemcpyHostToDevice, s));
+    FIIM_CUDA(cudaStreamSynchronize(s));
+    return FIIM_OK;
+}
+
+// Time each row-block size on this matrix and keep the fastest; cached by signature.
+// The choice changes speed only: every shape sums each row in storage order.
+static int autotune_tile(DevCsr &M, const double *x, double *y, cudaStream_t s) {
     static std::mutex mu;
     static std::map<std::vector<long>, int> cache;
+    int cached = 0;
     {
         std::lock_guard<std::mutex> lk(mu);
         auto it = cache.find(M.sig);
-        if (it != cache.end()) return it->second;
+        if (it != cache.end()) cached = it->second;
     }
-    const int cands[5] = {2, 4, 8, 16, 32};
+    if (cached) return set_tile(M, cached, s);
+    const int cands[3] = {1024, 2048, 4096};
     cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    int best = heuristic_vec(M.n, M.nnz);
+    FIIM_CUDA(cudaEventCreate(&e0));
+    FIIM_CUDA(cudaEventCreate(&e1));
+    int best = 2048;
     float best_ms = 1e30f;
-    const int reps = M.nnz > 4000000 ? 3 : 8;
+    const int reps = M.nnz > 4000000 ? 5 : 10;
     for (int c : cands) {
-        launch_spmv(c, s, view(M), x, EpiStore{y}, nullptr, nullptr);
-        cudaEventRecord(e0, s);
-        for (int r = 0; r < reps; ++r) launch_spmv(c, s, view(M), x, EpiStore{y}, nullptr, nullptr);
-        cudaEventRecord(e1, s);
-        cudaEventSynchronize(e1);
+        FIIM_TRY(set_tile(M, c, s));
+        FIIM_CUDA(launch_spmv(M, s, x, EpiStore{y}, nullptr, nullptr));
+        FIIM_CUDA(cudaEventRecord(e0, s));
+        for (int r = 0; r < reps; ++r) FIIM_CUDA(launch_spmv(M, s, x, EpiStore{y}, nullptr, nullptr));
+        FIIM_CUDA(cudaEventRecord(e1, s));
+        FIIM_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
+        FIIM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
         if (ms < best_ms * 0.97f) {
             best_ms = ms;
             best = c;
@@ -192,10 +247,11 @@ static int autotune_vec(const DevCsr &M, const double *x, double *y, cudaStream_
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    cudaGetLastError();
-    std::lock_guard<std::mutex> lk(mu);
-    cache[M.sig] = best;
-    return best;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        cache[M.sig] = best;
+    }
+    return set_tile(M, best, s);
 }
 
 // ------------------------------------------------------------------ host CSR helpers
@@ -272,16 +328,15 @@ static int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *
                       int fill, bool device_src, cudaStream_t s, unsigned long long *d_count,
                       unsigned long long *h_count) {
     M.n = n;
-    long nnz;
-    std::vector<int> hrp;
+    std::vector<int> &hrp = M.hrp;
+    hrp.resize(n + 1);
     if (device_src) {
-        hrp.resize(n + 1);
         FIIM_CUDA(cudaMemcpyAsync(hrp.data(), rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
         FIIM_CUDA(cudaStreamSynchronize(s));
-        nnz = hrp[n];
     } else {
-        nnz = rp[n];
+        std::memcpy(hrp.data(), rp, sizeof(int) * (n + 1));
     }
+    const long nnz = hrp[n];
     if (nnz > nnz_cap) return set_error(FIIM_EARG, "matrix has %ld entries, capacity %ld", nnz, nnz_cap);
     if (nnz < 0) return set_error(FIIM_EARG, "negative row offset at n");
     M.nnz = nnz;
@@ -291,7 +346,7 @@ static int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *
         FIIM_CUDA(cudaMemcpyAsync(M.ci, ci, sizeof(int) * nnz, kind, s));
         FIIM_CUDA(cudaMemcpyAsync(M.v, v, sizeof(double) * nnz, kind, s));
     }
-    signature(M, device_src ? hrp.data() : rp);
+    signature(M, hrp.data());
     if (fill == 0 || nnz == 0) return FIIM_OK;
     FIIM_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s));
     const int g = std::min(num_sms() * 8, std::max(1, (n + kThreads - 1) / kThreads));
@@ -324,7 +379,8 @@ static int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *
         FIIM_CUDA(cudaMemcpy(M.ci, cci.data(), sizeof(int) * c, cudaMemcpyHostToDevice));
         FIIM_CUDA(cudaMemcpy(M.v, cv.data(), sizeof(double) * c, cudaMemcpyHostToDevice));
     }
-    signature(M, nrp.data());
+    hrp.swap(nrp);
+    signature(M, hrp.data());
     return FIIM_OK;
 }
 
@@ -332,12 +388,13 @@ static int carve_csr(Arena &ar, DevCsr &M, long n, long nnz) {
     M.rp = static_cast<int *>(ar.take(sizeof(int) * (n + 1)));
     M.ci = static_cast<int *>(ar.take(sizeof(int) * std::max<long>(nnz, 1)));
     M.v = static_cast<double *>(ar.take(sizeof(double) * std::max<long>(nnz, 1)));
-    if (!M.rp || !M.ci || !M.v) return set_error(FIIM_ENOMEM, "arena exhausted");
+    M.rb = static_cast<int *>(ar.take(sizeof(int) * (n + 1)));   // at most one block per row
+    if (!M.rp || !M.ci || !M.v || !M.rb) return set_error(FIIM_ENOMEM, "arena exhausted");
     return FIIM_OK;
 }
 
 static size_t csr_bytes(long n, long nnz) {
-    return Arena::need(sizeof(int) * (n + 1)) + Arena::need(sizeof(int) * std::max<long>(nnz, 1)) +
+    return 2 * Arena::need(sizeof(int) * (n + 1)) + Arena::need(sizeof(int) * std::max<long>(nnz, 1)) +
            Arena::need(sizeof(double) * std::max<long>(nnz, 1));
 }
 
@@ -349,27 +406,27 @@ int Solver::enqueue_prec(const double *in, double *out, bool norm) {
     const bool combined = (opt.variant == FIIM_ACIFIM && opt.mode == 'C' && opt.nr > 1);
     if (!combined) {
         // tm = IDv o (H in); out = G tm   (AFIIM/src/bicgstab.cpp:172-175)
-        FIIM_CUDA(launch_spmv(H.vec, s, view(H), in, EpiScale{tm, IDv}, st, partials));
-        if (norm) FIIM_CUDA(launch_spmv(G.vec, s, view(G), tm, EpiNorm{out}, st, partials));
-        else FIIM_CUDA(launch_spmv(G.vec, s, view(G), tm, EpiStore{out}, st, partials));
+        FIIM_CUDA(launch_spmv(H, s, in, EpiScale{tm, IDv}, st, partials));
+        if (norm) FIIM_CUDA(launch_spmv(G, s, tm, EpiNorm{out}, st, partials));
+        else FIIM_CUDA(launch_spmv(G, s, tm, EpiStore{out}, st, partials));
         return FIIM_OK;
     }
     // ACIFIM apply() mode 'C' (ACIFIM/src/bicgstab.cpp:395-404,408,411-420).
-    FIIM_CUDA(launch_spmv(H.vec, s, view(H), in, EpiStore{t1}, st, partials));
+    FIIM_CUDA(launch_spmv(H, s, in, EpiStore{t1}, st, partials));
     for (int it = 1; it < opt.nr; ++it) {
-        FIIM_CUDA(launch_spmv(L.vec, s, view(L), t1, EpiSubFrom{t3, in}, st, partials));
+        FIIM_CUDA(launch_spmv(L, s, t1, EpiSubFrom{t3, in}, st, partials));
         if (it == opt.nr - 1)
-            FIIM_CUDA(launch_spmv(H.vec, s, view(H), t3, EpiAccumScale{t1, t2, IDv}, st, partials));
+            FIIM_CUDA(launch_spmv(H, s, t3, EpiAccumScale{t1, t2, IDv}, st, partials));
         else
-            FIIM_CUDA(launch_spmv(H.vec, s, view(H), t3, EpiAccum{t1}, st, partials));
+            FIIM_CUDA(launch_spmv(H, s, t3, EpiAccum{t1}, st, partials));
     }
-    FIIM_CUDA(launch_spmv(G.vec, s, view(G), t2, EpiStore{out}, st, partials));
+    FIIM_CUDA(launch_spmv(G, s, t2, EpiStore{out}, st, partials));
     for (int it = 1; it < opt.nr; ++it) {
-        FIIM_CUDA(launch_spmv(U.vec, s, view(U), out, EpiSubFrom{t3, t2}, st, partials));
+        FIIM_CUDA(launch_spmv(U, s, out, EpiSubFrom{t3, t2}, st, partials));
         if (it == opt.nr - 1 && norm)
-            FIIM_CUDA(launch_spmv(G.vec, s, view(G), t3, EpiAccumNorm{out}, st, partials));
+            FIIM_CUDA(launch_spmv(G, s, t3, EpiAccumNorm{out}, st, partials));
         else
-            FIIM_CUDA(launch_spmv(G.vec, s, view(G), t3, EpiAccum{out}, st, partials));
+            FIIM_CUDA(launch_spmv(G, s, t3, EpiAccum{out}, st, partials));
     }
     return FIIM_OK;
 }
@@ -385,11 +442,11 @@ int Solver::enqueue_iteration(bool cond, cudaGraphConditionalHandle h) {
     cudaStream_t s = stream;
     const long nn = n;
     FIIM_TRY(enqueue_prec(p, pc, true));                                             // K1-K2
-    FIIM_CUDA(launch_spmv(A.vec, s, view(A), pc, EpiAlpha{v, r0}, st, partials));     // K3
+    FIIM_CUDA(launch_spmv(A, s, pc, EpiAlpha{v, r0}, st, partials));     // K3
     k_update_s<<<stream_grid(k_update_s, nn), kThreads, 0, s>>>(nn, r, v, x, sv, st, partials);  // K4
     FIIM_CUDA(cudaGetLastError());
     FIIM_TRY(enqueue_prec(sv, sc, false));                                           // K5-K6
-    FIIM_CUDA(launch_spmv(A.vec, s, view(A), sc, EpiOmega{t, sv}, st, partials));    // K7
+    FIIM_CUDA(launch_spmv(A, s, sc, EpiOmega{t, sv}, st, partials));    // K7
     k_update_xr<<<stream_grid(k_update_xr, nn), kThreads, 0, s>>>(nn, pc, sc, sv, t, r0, x, r, st,
                                                                   partials);          // K8
     FIIM_CUDA(cudaGetLastError());
@@ -583,13 +640,13 @@ int Solver::create(int n_, const int *Ai, const int *Aj, const double *Av, const
     DevCsr *mats[] = {&A, &G, &H, &L, &U};
     for (int k = 0; k < (combined ? 5 : 3); ++k) {
         DevCsr &M = *mats[k];
-        M.vec = heuristic_vec(M.n, M.nnz);
         if (opt.autotune) {
             FIIM_CUDA(cudaMemsetAsync(tm, 0, sizeof(double) * n, stream));
-            M.vec = autotune_vec(M, tm, t, stream);
+            FIIM_TRY(autotune_tile(M, tm, t, stream));
+        } else {
+            FIIM_TRY(set_tile(M, 2048, stream));
         }
     }
-    FIIM_CUDA(cudaStreamSynchronize(stream));
     FIIM_TRY(build_graph());
     if (!ev0) {
         FIIM_CUDA(cudaEventCreate(&ev0));
@@ -617,6 +674,15 @@ int Solver::reload(const int *Ai, const int *Aj, const double *Av, const int *Gi
     }
     FIIM_CUDA(cudaMemcpyAsync(IDv, IDv_, sizeof(double) * n,
                               dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
+    // Row blocks follow the new row offsets; the graph bakes in each block count.
+    bool regraph = false;
+    DevCsr *mats[] = {&A, &G, &H, &L, &U};
+    for (int k = 0; k < (combined ? 5 : 3); ++k) {
+        const int old = mats[k]->nblk;
+        FIIM_TRY(set_tile(*mats[k], mats[k]->tile, stream));
+        regraph |= (mats[k]->nblk != old);
+    }
+    if (regraph) FIIM_TRY(build_graph());
     return FIIM_OK;
 }
 
@@ -641,7 +707,7 @@ int Solver::solve(const double *b_in, double *x_io, double tol, int nmax, fiim_r
     *hst = h;
     FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
     // Start: r = b - A x, r0 = r, p = r, ro = ||r0|| (AFIIM/src/bicgstab.cpp:151-165).
-    FIIM_CUDA(launch_spmv(A.vec, stream, view(A), x, EpiInit{b, p, r0, r}, st, partials));
+    FIIM_CUDA(launch_spmv(A, stream, x, EpiInit{b, p, r0, r}, st, partials));
     int launches = 1;
     if (use_cond) {
         FIIM_CUDA(cudaGraphLaunch(exec, stream));
@@ -662,7 +728,7 @@ int Solver::solve(const double *b_in, double *x_io, double tol, int nmax, fiim_r
         hst->loops = launched;
     }
     // FP64 true residual ||b - A x|| / ||b||.
-    FIIM_CUDA(launch_spmv(A.vec, stream, view(A), x, EpiResid{b, nullptr}, st, partials));
+    FIIM_CUDA(launch_spmv(A, stream, x, EpiResid{b, nullptr}, st, partials));
     launches += 1;
     const int fallback_loops = hst->loops;
     FIIM_CUDA(cudaMemcpyAsync(hst, st, sizeof(DState), cudaMemcpyDeviceToHost, stream));
@@ -721,6 +787,26 @@ void Solver::destroy() {
     arena.release();
 }
 
+// ------------------------------------------------------------------ single products
+// y = A x (op 0) or y = M x with the solver's preconditioner (op 1), using the
+// solver's own tuned kernels. x and y live in opt.memory space.
+int Solver::apply(int op, const double *in, double *out) {
+    FIIM_CUDA(cudaSetDevice(device));
+    if (op != 0 && op != 1) return set_error(FIIM_EARG, "op is 0 (A) or 1 (preconditioner)");
+    const bool dev_src = (opt.memory == FIIM_MEM_DEVICE);
+    FIIM_CUDA(cudaMemcpyAsync(sv, in, sizeof(double) * n,
+                              dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
+    DState h = {};
+    *hst = h;
+    FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
+    if (op == 0) FIIM_CUDA(launch_spmv(A, stream, sv, EpiStore{t}, st, partials));
+    else FIIM_TRY(enqueue_prec(sv, t, false));
+    FIIM_CUDA(cudaMemcpyAsync(out, t, sizeof(double) * n,
+                              dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream));
+    FIIM_CUDA(cudaStreamSynchronize(stream));
+    return FIIM_OK;
+}
+
 // ------------------------------------------------------------------ per-kernel timing
 // Replays each launch of the iteration body on its own, `reps` times, between CUDA
 // events on the solver's stream, after a solve has left the vectors populated. The
@@ -736,12 +822,12 @@ int Solver::kernel_times(int reps, int max_k, double *ms, double *bytes, char *n
     auto S = [&](const DevCsr &M) { return 12.0 * M.nnz + 4.0 * (M.n + 1); };
     const long nn = n;
     std::vector<Item> items = {
-        {"H_spmv_scale", S(H) + 3 * nv, [&] { return launch_spmv(H.vec, stream, view(H), p, EpiScale{tm, IDv}, st, partials); }},
-        {"G_spmv_norm", S(G) + 2 * nv, [&] { return launch_spmv(G.vec, stream, view(G), tm, EpiNorm{pc}, st, partials); }},
-        {"A_spmv_alpha", S(A) + 3 * nv, [&] { return launch_spmv(A.vec, stream, view(A), pc, EpiAlpha{v, r0}, st, partials); }},
+        {"H_spmv_scale", S(H) + 3 * nv, [&] { return launch_spmv(H, stream, p, EpiScale{tm, IDv}, st, partials); }},
+        {"G_spmv_norm", S(G) + 2 * nv, [&] { return launch_spmv(G, stream, tm, EpiNorm{pc}, st, partials); }},
+        {"A_spmv_alpha", S(A) + 3 * nv, [&] { return launch_spmv(A, stream, pc, EpiAlpha{v, r0}, st, partials); }},
         {"update_s", 4 * nv, [&] { k_update_s<<<stream_grid(k_update_s, nn), kThreads, 0, stream>>>(nn, r, v, x, sv, st, partials); return cudaGetLastError(); }},
-        {"G_spmv", S(G) + 2 * nv, [&] { return launch_spmv(G.vec, stream, view(G), tm, EpiStore{sc}, st, partials); }},
-        {"A_spmv_omega", S(A) + 3 * nv, [&] { return launch_spmv(A.vec, stream, view(A), sc, EpiOmega{t, sv}, st, partials); }},
+        {"G_spmv", S(G) + 2 * nv, [&] { return launch_spmv(G, stream, tm, EpiStore{sc}, st, partials); }},
+        {"A_spmv_omega", S(A) + 3 * nv, [&] { return launch_spmv(A, stream, sc, EpiOmega{t, sv}, st, partials); }},
         {"update_xr", 8 * nv, [&] { k_update_xr<<<stream_grid(k_update_xr, nn), kThreads, 0, stream>>>(nn, pc, sc, sv, t, r0, x, r, st, partials); return cudaGetLastError(); }},
         {"update_p", 4 * nv, [&] { k_update_p<<<stream_grid(k_update_p, nn), kThreads, 0, stream>>>(nn, r, v, p, st, cudaGraphConditionalHandle{}, 0); return cudaGetLastError(); }},
     };
@@ -786,7 +872,7 @@ int spmv_api(int n, const int *Ai, const int *Aj, const double *Av, const double
         FIIM_CUDA(cudaStreamSynchronize(s));
         vec = heuristic_vec(n, z);
     }
-    FIIM_CUDA(launch_spmv(vec, s, CsrView<double>{Ai, Aj, Av, n}, x, EpiStore{y}, nullptr, nullptr));
+    FIIM_CUDA(launch_spmv_vec(vec, s, CsrView<double>{Ai, Aj, Av, n}, x, EpiStore{y}, nullptr, nullptr));
     return FIIM_OK;
 }
 
@@ -799,9 +885,9 @@ int prec_api(int n, const int *Gi, const int *Gj, const double *Gv, const double
     FIIM_CUDA(cudaMemcpyAsync(&zz[0], Gi + n, sizeof(int), cudaMemcpyDeviceToHost, s));
     FIIM_CUDA(cudaMemcpyAsync(&zz[1], Hi + n, sizeof(int), cudaMemcpyDeviceToHost, s));
     FIIM_CUDA(cudaStreamSynchronize(s));
-    FIIM_CUDA(launch_spmv<2>(heuristic_vec(n, zz[1]), s, CsrView<double>{Hi, Hj, Hv, n}, rr,
+    FIIM_CUDA(launch_spmv_vec<2>(heuristic_vec(n, zz[1]), s, CsrView<double>{Hi, Hj, Hv, n}, rr,
                              EpiScale{tmv, IDv_}, nullptr, nullptr));
-    FIIM_CUDA(launch_spmv<1>(heuristic_vec(n, zz[0]), s, CsrView<double>{Gi, Gj, Gv, n}, tmv,
+    FIIM_CUDA(launch_spmv_vec<1>(heuristic_vec(n, zz[0]), s, CsrView<double>{Gi, Gj, Gv, n}, tmv,
                              EpiStore{z}, nullptr, nullptr));
     return FIIM_OK;
 }

@@ -55,6 +55,7 @@ struct Solver : SolverBase {
     int build_graph();
     int kernels_per_iteration() const;
     void print_status(int info, int iter, double rel) const;
+    int apply(int op, const double *in, double *out);
     int kernel_times(int reps, int max_k, double *ms, double *bytes, char *names, int name_len);
     double iteration_bytes() const;
 };

@@ -37,7 +37,7 @@ _PRECISIONS = {"fp64": FP64, "fp32": MIXED_FP32, "bf16": MIXED_BF16}
 EXPORTS = (
     "fiim_last_error", "fiim_options_default", "fiim_EPBiCGSTAB_afiim", "fiim_EPBiCGSTAB_pdfiim",
     "fiim_PBiCGSTAB_acifim", "fiim_solver_create", "fiim_solver_solve", "fiim_solver_device_bytes",
-    "fiim_solver_spmv_shape", "fiim_solver_kernel_times", "fiim_solver_iteration_bytes", "fiim_solver_destroy", "fiim_spmv", "fiim_prec_apply",
+    "fiim_solver_spmv_shape", "fiim_solver_apply", "fiim_solver_kernel_times", "fiim_solver_iteration_bytes", "fiim_solver_destroy", "fiim_spmv", "fiim_prec_apply",
     "fiim_gen_poisson2d", "fiim_gen_convdiff3d", "fiim_gen_convdiff2d", "fiim_gen_batch_params",
     "fiim_gen_zipf", "fiim_gen_zipf_mean", "fiim_rand_normal", "fiim_model_rhs", "fiim_pdfiim_build",
 )
@@ -207,6 +207,14 @@ class Solver:
         v = C.c_int(0)
         _check(lib().fiim_solver_spmv_shape(self._h, C.c_int(which), C.byref(v)))
         return v.value
+
+    def apply(self, x, y, op="A"):
+        """y = A x (op 'A') or y = M x (op 'M', the preconditioner) with the solver's kernels."""
+        if self.memory != "device":
+            x = _d(x)
+            assert y.dtype == np.float64 and y.flags.c_contiguous
+        _check(lib().fiim_solver_apply(self._h, C.c_int(0 if op == "A" else 1), _ptr(x), _ptr(y)))
+        return y
 
     def kernel_times(self, reps=20, max_kernels=16):
         """Mean device ms and algorithmic bytes of each launch of the iteration body."""

@@ -131,6 +131,12 @@ int64_t fiim_solver_device_bytes(fiim_solver_t s);
 /* Lanes per row chosen for matrix `which` (0 A, 1 G, 2 H, 3 L, 4 U). */
 int fiim_solver_spmv_shape(fiim_solver_t s, int which, int *vec);
 
+/* y = A x (op 0) or y = M x, the preconditioner application (op 1), with the solver's
+ * own kernels; x, y in opt->memory space. Each row of every product is summed in
+ * storage order with rounded products, as mkl_sparse_d_mv is restated by the oracle
+ * (AFIIM/src/bicgstab.cpp:151,172-175), so the results are bit-identical to it. */
+int fiim_solver_apply(fiim_solver_t s, int op, const double *x, double *y);
+
 /* Profiling aid (no counterpart in the reference): replays each launch of the FP64
  * iteration body alone `reps` times between CUDA events on the solver's stream and
  * writes the mean ms per launch, its algorithmic bytes and (if names != NULL) its name

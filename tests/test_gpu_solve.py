@@ -1,8 +1,9 @@
 """GPU parity of the FP64 solve phase against the oracle (B200 only).
 
 Every check goes through the C-ABI of libfiim_b200.so. Tolerances:
-  * SpMV and preconditioner application on the same vector: 1e-12 relative (FP64; the
-    GPU sums each row as a lane tree with FMA, the oracle left to right).
+  * SpMV and preconditioner application on the same vector: bit-identical to the
+    oracle (each row summed in storage order with rounded products, no FMA), for the
+    set-up-free kernel at every lane count and for the solver's tuned kernels.
   * Solves: the same info code; the iteration count within +-2 of the reference's
     rounding envelope (the reference's own counts when only the summation order of its
     dot products changes: the MKL shim's reductions split over 1..8 OpenMP threads,
@@ -44,10 +45,7 @@ def test_spmv_matches_oracle(golden, cuda, name, prefix, vec):
     y = torch.zeros(len(g["b"]), dtype=torch.float64, device=cuda)
     FB.spmv(Ai, Aj, Av, _t(u, cuda), y, vec=vec)
     torch.cuda.synchronize()
-    ref = sub(g, prefix)["Au"]
-    absA = sp.csr_matrix((np.abs(g["Av"]), g["Aj"], g["Ai"])) @ np.abs(u)
-    assert np.all(np.abs(y.cpu().numpy() - ref) <= 1e-12 * absA + 1e-300)
-    assert rel(y.cpu().numpy(), ref) <= 1e-12
+    assert np.array_equal(y.cpu().numpy(), sub(g, prefix)["Au"])
 
 
 @pytest.mark.parametrize("name,prefix", FIXTURE_PRODUCTS)
@@ -61,7 +59,25 @@ def test_prec_apply_matches_oracle(golden, cuda, name, prefix):
     tm = torch.zeros_like(z)
     FB.prec_apply(d["Gi"], d["Gj"], d["Gv"], d["IDv"], d["Hi"], d["Hj"], d["Hv"], _t(F["u"], cuda), z, tm)
     torch.cuda.synchronize()
-    assert rel(z.cpu().numpy(), F["Mu"]) <= 1e-12
+    assert np.array_equal(z.cpu().numpy(), F["Mu"])
+
+
+@pytest.mark.parametrize("name,prefix,variant,kw", [
+    ("sherman2", "afiim9e-6_", "afiim", {}), ("sherman2", "acifim_", "acifim", {"mode": "C", "nr": 2}),
+    ("poisson128_afiim", "", "afiim", {}), ("convdiff16_pdfiim", "", "pdfiim", {}),
+    ("convdiff2d48_acifim", "", "acifim", {"mode": "C", "nr": 2}), ("poisson32_sym_pdfiim", "", "pdfiim",
+                                                                     {"issym": True})])
+def test_solver_products_bit_identical(golden, name, prefix, variant, kw):
+    """The solver's tuned CSR-stream kernels reproduce the oracle's A x and M x exactly."""
+    g = golden(name)
+    F = sub(g, prefix)
+    S = FB.Solver((g["Ai"], g["Aj"], g["Av"]), F, variant=variant, **kw)
+    n = len(g["b"])
+    y = S.apply(F["u"], np.zeros(n), op="A")
+    assert np.array_equal(y, F["Au"])
+    z = S.apply(F["u"], np.zeros(n), op="M")
+    assert np.array_equal(z, F["MuC"] if kw.get("mode") == "C" else F["Mu"])
+    S.close()
 
 
 def test_prec_apply_ignores_entries_outside_triangles(cuda):
@@ -80,7 +96,11 @@ def test_prec_apply_ignores_entries_outside_triangles(cuda):
     FB.prec_apply(d["Gi"], d["Gj"], d["Gv"], d["IDv"], d["Hi"], d["Hj"], d["Hv"], _t(u, cuda), z,
                   torch.zeros_like(z))
     torch.cuda.synchronize()
-    assert rel(z.cpu().numpy(), want) <= 1e-12
+    assert np.array_equal(z.cpu().numpy(), want)
+    # the solver path filters the triangles at upload and must agree too
+    S = FB.Solver((M.indptr.astype(np.int32), M.indices.astype(np.int32), M.data), {k: np.asarray(v) for k, v in F.items()})
+    assert np.array_equal(S.apply(u, np.zeros(n), op="M"), want)
+    S.close()
 
 
 SOLVES = [
