@@ -362,8 +362,11 @@ def main():
     ap.add_argument("--ref-sample-its", type=int, default=10)
     ap.add_argument("--ref-iters", type=int, default=99,
                     help="iterations of the full 128^3 solve (the reference's own count, for scaling samples)")
-    ap.add_argument("--ncu-traffic", type=float, default=None,
-                    help="dram bytes per launch of the dominant kernel from an ncu capture, if known")
+    # DRAM bytes per launch of the dominant kernel (H's SpMV) from the ncu capture summarised
+    # in profiles/spmv_rows_convdiff96_ncu_full.md (0.983 x algorithmic at 96^3), scaled to
+    # the 128^3 launch by units processed.
+    ap.add_argument("--ncu-traffic", type=float, default=325.6e6,
+                    help="dram bytes per launch of the dominant kernel from an ncu capture")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

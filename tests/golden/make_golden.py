@@ -51,18 +51,20 @@ def probe(A, F, n, sym=False, nr=None):
 
 def solved(prefix, variant, A, b, F, tol, nmax, **kw):
     """One-thread reference run (bit-identical to the restatement) plus its rounding envelope:
-    the same solve with the shim's reductions split over 2..8 OpenMP threads, which changes
+    the same solve with the shim's reductions split over 2..48 OpenMP threads, which changes
     only the summation order of the dot products and norms."""
     O.set_threads(1, variant)
     x, res, it, info = O.ref_solve(variant, A, b, F, tol=tol, nmax=nmax, **kw)
     xr, resr, itr, infor = O.bicgstab(variant, A, b, F, tol=tol, nmax=nmax, **kw)
     assert np.array_equal(x, xr) and res == resr and it == itr and info == infor, "restatement drifted"
     its, spread, infos = [it], 0.0, {info}
-    for t in range(2, 9):
+    for t in range(2, 49):
         O.set_threads(t, variant)
         xt, _, itt, inft = O.ref_solve(variant, A, b, F, tol=tol, nmax=nmax, **kw)
-        its.append(itt)
         infos.add(inft)
+        if inft != info:       # the envelope covers runs that end the way the one-thread run does
+            continue
+        its.append(itt)
         spread = max(spread, float(np.linalg.norm(xt - x) / np.linalg.norm(x)))
     O.set_threads(1, variant)
     return {f"{prefix}x": x, f"{prefix}resval": np.float64(res), f"{prefix}iter": np.int32(it),
