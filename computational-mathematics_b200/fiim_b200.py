@@ -37,7 +37,7 @@ _PRECISIONS = {"fp64": FP64, "fp32": MIXED_FP32, "bf16": MIXED_BF16}
 EXPORTS = (
     "fiim_last_error", "fiim_options_default", "fiim_EPBiCGSTAB_afiim", "fiim_EPBiCGSTAB_pdfiim",
     "fiim_PBiCGSTAB_acifim", "fiim_solver_create", "fiim_solver_solve", "fiim_solver_device_bytes",
-    "fiim_solver_spmv_shape", "fiim_solver_apply", "fiim_solver_kernel_times", "fiim_solver_iteration_bytes", "fiim_solver_destroy", "fiim_spmv", "fiim_prec_apply",
+    "fiim_solver_spmv_shape", "fiim_solver_apply", "fiim_solver_kernel_times", "fiim_solver_iteration_bytes", "fiim_solver_destroy", "fiim_spmv", "fiim_prec_apply", "fiim_prec_apply_noalloc",
     "fiim_gen_poisson2d", "fiim_gen_convdiff3d", "fiim_gen_convdiff2d", "fiim_gen_batch_params",
     "fiim_gen_zipf", "fiim_gen_zipf_mean", "fiim_rand_normal", "fiim_model_rhs", "fiim_pdfiim_build",
 )
@@ -253,6 +253,13 @@ def prec_apply(Gi, Gj, Gv, IDv, Hi, Hj, Hv, r, z, tm, stream=0):
     """z = G (IDv o (H r)) on device tensors."""
     _check(lib().fiim_prec_apply(C.c_int(Gi.numel() - 1), _ptr(Gi), _ptr(Gj), _ptr(Gv), _ptr(IDv), _ptr(Hi),
                                  _ptr(Hj), _ptr(Hv), _ptr(r), _ptr(z), _ptr(tm), C.c_void_p(stream)))
+
+
+def prec_apply_noalloc(Gi, Gj, Gv, IDv, Hi, Hj, Hv, r, z, stream=0):
+    """z = G (IDv o (H r)) on device tensors without caller scratch or any allocation
+    (the intermediate vector is a fixed array inside the library; n <= 1,048,576)."""
+    _check(lib().fiim_prec_apply_noalloc(C.c_int(Gi.numel() - 1), _ptr(Gi), _ptr(Gj), _ptr(Gv), _ptr(IDv),
+                                         _ptr(Hi), _ptr(Hj), _ptr(Hv), _ptr(r), _ptr(z), C.c_void_p(stream)))
 
 
 # ----------------------------------------------------------------------------- generators

@@ -168,6 +168,22 @@ int fiim_prec_apply(int n, const int *Gi, const int *Gj, const double *Gv, const
                     const int *Hi, const int *Hj, const double *Hv, const double *r, double *z,
                     double *tm, void *stream);
 
+/* Same product as fiim_prec_apply, but it allocates nothing and needs no caller scratch.
+ * No counterpart in the reference (whose CPU code allocates freely). It is for callers
+ * that cannot allocate device memory when they call: an application that gives all of
+ * the GPU's memory to its own pool at start-up and forbids allocations behind it, or a
+ * process held to a fixed device-memory budget. The intermediate vector lives in a
+ * fixed array built into the library (1,048,576 doubles, 8 MiB), which every GPU that
+ * loads the library's device code keeps until the process exits; n above 1,048,576 rows
+ * returns FIIM_EARG. The first call on each device looks up that array's device address
+ * (with the device current) and keeps it; make that first call before any stream
+ * capture. All calls on a device share the array, so calls that overlap on the GPU race
+ * on it; each call overwrites all n entries it reads. Arrays and stream as for
+ * fiim_prec_apply. */
+int fiim_prec_apply_noalloc(int n, const int *Gi, const int *Gj, const double *Gv,
+                            const double *IDv, const int *Hi, const int *Hj, const double *Hv,
+                            const double *r, double *z, void *stream);
+
 /* ===========================================================================
  * Problem generators (host; sizing pass with null arrays returns nnz).
  * ======================================================================== */
