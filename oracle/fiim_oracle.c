@@ -112,9 +112,29 @@ void orc_prec_apply_combined(int n, int nr, const int *Gi, const int *Gj, const 
     free(tmp);
 }
 
+/* Number of contiguous blocks the dot products and norms are split into. 1 (default) is
+ * the left-to-right sum of a one-thread MKL shim; B > 1 reproduces the shim's OpenMP
+ * reduction on B threads (oracle/mkl_shim/mkl_shim.cpp blocked_sum): B static blocks,
+ * each summed left to right, then the partials added in block order. Used to sample
+ * how the reference's iteration counts move with the summation order alone. */
+static int g_dot_blocks = 1;
+
+void orc_set_dot_blocks(int blocks) { g_dot_blocks = blocks > 1 ? blocks : 1; }
+
 static double dot(int n, const double *x, const double *y) {
+    if (g_dot_blocks <= 1) {
+        double s = 0.0;
+        for (int i = 0; i < n; ++i) s += x[i] * y[i];
+        return s;
+    }
+    const long T = g_dot_blocks, q = n / T, r = n % T;
     double s = 0.0;
-    for (int i = 0; i < n; ++i) s += x[i] * y[i];
+    for (long t = 0; t < T; ++t) {
+        const long lo = t * q + (t < r ? t : r), hi = lo + q + (t < r ? 1 : 0);
+        double part = 0.0;
+        for (long i = lo; i < hi; ++i) part += x[i] * y[i];
+        s += part;
+    }
     return s;
 }
 

@@ -42,6 +42,10 @@ void orc_prec_apply_combined(int n, int nr, const int *Gi, const int *Gj, const 
                              const int *Uj, const double *Uv, const double *in, double *out,
                              double *work);
 
+/* Split every dot product and norm into `blocks` contiguous blocks (see fiim_oracle.c);
+ * 1 restores the left-to-right sum. */
+void orc_set_dot_blocks(int blocks);
+
 /* One full solve. variant: ORC_*; issym (PDFIIM only): A holds its upper triangle and
  * G^T replaces H; mode (ACIFIM only): 'E' explicit or 'C' combined with nr steps.
  * Returns 0, or -1 on an unsupported argument. */

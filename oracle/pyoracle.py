@@ -116,6 +116,11 @@ def prec_apply_combined(F, r, nr):
     return out
 
 
+def set_dot_blocks(blocks: int) -> None:
+    """Sum dots and norms over `blocks` contiguous blocks, as the shim does on that many threads."""
+    _lib("oracle").orc_set_dot_blocks(C.c_int(blocks))
+
+
 def bicgstab(variant, A, b, F, tol=1e-8, nmax=500, x0=None, issym=False, mode="E", nr=1):
     """Restated EPBiCGSTAB / PBiCGSTAB. Returns (x, resval, iter, info)."""
     lib = _lib("oracle")

@@ -49,29 +49,44 @@ def probe(A, F, n, sym=False, nr=None):
     return out
 
 
+# Summation orders sampled for the rounding envelope: the dot products and norms split
+# into B contiguous blocks (the MKL shim's OpenMP reduction on B threads).
+BLOCKS = list(range(1, 49)) + [64, 96, 128, 192, 256, 384, 512, 768, 1024, 1536, 2048, 3072, 4096]
+
+
 def solved(prefix, variant, A, b, F, tol, nmax, **kw):
     """One-thread reference run (bit-identical to the restatement) plus its rounding envelope:
-    the same solve with the shim's reductions split over 2..48 OpenMP threads, which changes
-    only the summation order of the dot products and norms."""
+    the iteration counts the same solve takes when only the summation order of its dot
+    products and norms changes. The restatement with B blocks is the reference on B threads
+    (checked here for B = 2, 3, 5, 8); the envelope runs the restatement over BLOCKS and
+    counts the runs that end with the same info as the one-thread run."""
     O.set_threads(1, variant)
+    O.set_dot_blocks(1)
     x, res, it, info = O.ref_solve(variant, A, b, F, tol=tol, nmax=nmax, **kw)
     xr, resr, itr, infor = O.bicgstab(variant, A, b, F, tol=tol, nmax=nmax, **kw)
     assert np.array_equal(x, xr) and res == resr and it == itr and info == infor, "restatement drifted"
-    its, spread, infos = [it], 0.0, {info}
-    for t in range(2, 49):
-        O.set_threads(t, variant)
-        xt, _, itt, inft = O.ref_solve(variant, A, b, F, tol=tol, nmax=nmax, **kw)
+    for B in (2, 3, 5, 8):
+        O.set_threads(B, variant)
+        O.set_dot_blocks(B)
+        xa, *ra = O.ref_solve(variant, A, b, F, tol=tol, nmax=nmax, **kw)
+        xb, *rb = O.bicgstab(variant, A, b, F, tol=tol, nmax=nmax, **kw)
+        assert ra == rb and np.array_equal(xa, xb), f"blocked restatement drifted at B={B}"
+    its, spread, infos = [], 0.0, set()
+    for B in BLOCKS:
+        O.set_dot_blocks(B)
+        xt, _, itt, inft = O.bicgstab(variant, A, b, F, tol=tol, nmax=nmax, **kw)
         infos.add(inft)
-        if inft != info:       # the envelope covers runs that end the way the one-thread run does
+        if inft != info:
             continue
         its.append(itt)
         spread = max(spread, float(np.linalg.norm(xt - x) / np.linalg.norm(x)))
+    O.set_dot_blocks(1)
     O.set_threads(1, variant)
     return {f"{prefix}x": x, f"{prefix}resval": np.float64(res), f"{prefix}iter": np.int32(it),
             f"{prefix}info": np.int32(info), f"{prefix}iter_env": np.array([min(its), max(its)], np.int32),
             f"{prefix}x_spread": np.float64(spread)}, \
         {"resval": res, "iter": it, "info": info, "iter_env": [min(its), max(its)], "x_spread": spread,
-         "infos": sorted(infos)}
+         "infos": sorted(infos), "orders": len(BLOCKS), "same_info": len(its)}
 
 
 def save(name, arrays, meta):

@@ -135,6 +135,23 @@ def test_restatement_matches_live_reference(seed):
 
 
 @needs_ref
+@pytest.mark.parametrize("blocks", [2, 3, 7])
+def test_blocked_restatement_matches_reference_threads(golden, blocks):
+    """The restatement's B-block dot products equal the reference's shim on B OpenMP threads."""
+    g = golden("sherman2")
+    A, F = csr_of(g), sub(g, "afiim0.1_")
+    O.set_threads(blocks, "afiim")
+    O.set_dot_blocks(blocks)
+    try:
+        xr, *r = O.ref_solve("afiim", A, g["b"], F)
+        xo, *o = O.bicgstab("afiim", A, g["b"], F)
+    finally:
+        O.set_dot_blocks(1)
+        O.set_threads(1, "afiim")
+    assert r == o and np.array_equal(xr, xo)
+
+
+@needs_ref
 def test_restatement_matches_live_reference_edge_cases():
     O.set_threads(1, "afiim")
     O.set_threads(1, "acifim")
