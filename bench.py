@@ -309,7 +309,39 @@ def run_ours(args):
                 "algorithmic_bytes_per_launch": dom[2], "launch_ms": round(dom[1], 5),
                 "per_kernel": [{"kernel": k, "ms": round(m, 5), "gbs": round(by / (m / 1000) / 1e9, 1)}
                                for k, m, by in ktimes]}
+    # FP64 to the mixed leg's target (1e-10), the reference x for its error
+    x_ref10 = None
+    if not args.no_mixed:
+        tx.zero_()
+        r10 = S.solve(tb, tx, tol=1e-10, nmax=1200)
+        x_ref10 = tx.clone()
+        fp64_10 = {"iter": r10["iter"], "ms": r10["device_ms"], "true_relres": r10["true_relres"]}
     S.close()
+
+    # ---- mixed precision: FP64 iterative refinement around an FP32 inner BiCGSTAB
+    mixed = None
+    if not args.no_mixed:
+        mixed = {"fp64_to_1e-10": fp64_10}
+        for prec in ("fp32", "bf16"):
+            M = FB.Solver(tA, tF, variant="pdfiim", memory="device", precision=prec, inner_tol=1e-5)
+            for _ in range(args.warmup):
+                tx.zero_()
+                M.solve(tb, tx, tol=1e-10, nmax=5000)
+            torch.cuda.synchronize()
+            rr = []
+            for _ in range(args.steps):
+                tx.zero_()
+                rr.append(M.solve(tb, tx, tol=1e-10, nmax=5000))
+            ms = sum(q["device_ms"] for q in rr) / len(rr)
+            err = float(torch.linalg.norm(tx - x_ref10) / torch.linalg.norm(x_ref10))
+            mixed[prec] = {"solves_per_s": round(1000.0 / ms, 4), "ms_per_solve": round(ms, 4),
+                           "tol": 1e-10, "inner_tol": 1e-5, "refine_steps": rr[-1]["refine_steps"],
+                           "inner_iterations": rr[-1]["iter"], "true_relres": rr[-1]["true_relres"],
+                           "info": rr[-1]["info"], "rel_err_vs_fp64": err,
+                           "speedup_vs_fp64_same_tol": round(fp64_10["ms"] / ms, 3),
+                           "speedup_vs_fp64_1e-8": round((dev_ms / args.steps) / ms, 3),
+                           "a_inner": "FP32 copy of A", "factors": prec.upper(), "d_inv": "FP32"}
+            M.close()
 
     # ---- e2e: reference-facing C-ABI call with pinned host arrays
     e2e = None
@@ -341,7 +373,7 @@ def run_ours(args):
                 "hbm_gbs": round(hbm_gbs, 1), "hbm_frac": round(hbm_gbs / peak, 4),
                 "iteration_bytes": it_bytes, "true_relres": results[-1]["true_relres"],
                 "resval": results[-1]["resval"], "wall_ms_per_step": round(1000 * wall / args.steps, 4),
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed, "gpu_launches": launches,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -358,6 +390,7 @@ def main():
     ap.add_argument("--size", type=int, default=128, help="grid side of the 3D convection-diffusion system")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI leg")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--cpu-sample-its", type=int, default=12)
     ap.add_argument("--ref-sample-its", type=int, default=10)
     ap.add_argument("--ref-iters", type=int, default=99,

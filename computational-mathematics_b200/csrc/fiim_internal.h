@@ -5,7 +5,10 @@
 #include <cuda_bf16.h>
 
 #include <cstdarg>
+#include <algorithm>
 #include <cstddef>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "fiim_b200.h"
@@ -71,5 +74,41 @@ struct HostCsr {
 };
 
 int heuristic_vec(long n, long nnz);
+
+// Set-up helpers shared by the FP64 and mixed-precision solvers (fiim_solver.cu).
+void signature(DevCsr &M, const int *host_rp);
+size_t csr_bytes(long n, long nnz);
+int carve_csr(Arena &ar, DevCsr &M, long n, long nnz);
+int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, const double *v, int fill,
+               bool device_src, cudaStream_t s, unsigned long long *d_count, unsigned long long *h_count);
+int set_tile(DevCsr &M, int tile, cudaStream_t s);
+void expand_sym_upper(int n, const int *rp, const int *ci, const double *v, HostCsr &out);
+void transpose_upper(int n, const int *rp, const int *ci, const double *v, HostCsr &out);
+
+// Resident blocks per SM of a kernel launched with 256 threads, cached by kernel address.
+template <typename K>
+int occupancy(K kernel) {
+    constexpr int kBlockThreads = 256;
+    static std::mutex mu;
+    static std::map<const void *, int> occ;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = occ.find((const void *)kernel);
+    if (it != occ.end()) return it->second;
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kBlockThreads, 0) != cudaSuccess || b < 1) {
+        cudaGetLastError();
+        b = 4;
+    }
+    occ[(const void *)kernel] = b;
+    return b;
+}
+
+// Grid: enough blocks for the work, capped at one full wave of resident blocks.
+template <typename K>
+int grid_for(K kernel, long units_per_block, long units) {
+    const long need = std::max<long>(1, (units + units_per_block - 1) / units_per_block);
+    return (int)std::min<long>(need, (long)occupancy(kernel) * num_sms());
+}
+
 
 }  // namespace fiim

@@ -1,18 +1,402 @@
 // Mixed-precision solve: FP64 iterative refinement around an FP32 inner BiCGSTAB.
+//
+// Layout in HBM (one arena):
+//   A   : int32 rp/ci shared by an FP64 value array (outer residual) and an FP32 copy
+//         (inner products); row blocks for the CSR-stream kernels.
+//   G, H: int32 rp/ci + FP32 values (FIIM_MIXED_FP32) or BF16 values (FIIM_MIXED_BF16).
+//   D^-1: FP32.  Outer vectors x, b, r64: FP64.  Inner vectors e, r, r0, p, v, s, t, pc,
+//   sc, tm: FP32.  Two DState blocks (inner, outer) and the reduction partials.
+// The FP64 factor values are staged through one scratch buffer at set-up and not kept.
+//
+// Solve: r64 = b - A x (FP64, true residual); while ||r64|| > tol ||b||: inner BiCGSTAB on
+// r64/||r64|| from e = 0 to inner_tol (one CUDA graph with a device-driven WHILE node, the
+// reference's control flow), x += ||r64|| e, r64 = b - A x. The host reads two scalars per
+// refinement step.
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <iostream>
+#include <vector>
+
 #include "fiim_b200.h"
 #include "fiim_internal.h"
+#include "fiim_kernels.cuh"
+#include "fiim_mixed.cuh"
 #include "fiim_solver.h"
+
+namespace fiim {
+namespace {
+
+CsrView<double> view64(const DevCsr &M) { return CsrView<double>{M.rp, M.ci, M.v, (int)M.n}; }
+
+template <int TILE, typename V, typename Epi>
+cudaError_t rows_f(cudaStream_t s, const DevCsr &M, const V *vals, const float *x, const Epi &epi,
+                   DState *st, double *partials) {
+    auto kern = mx::k_spmv_rows_f<TILE, V, Epi>;
+    const int g = grid_for(kern, 1, M.nblk);
+    kern<<<g, kThreads, 0, s>>>(CsrView<V>{M.rp, M.ci, vals, (int)M.n}, M.rb, M.nblk, x, epi, st, partials);
+    return cudaGetLastError();
+}
+
+template <typename V, typename Epi>
+cudaError_t spmv_f(const DevCsr &M, const V *vals, cudaStream_t s, const float *x, const Epi &epi,
+                   DState *st, double *partials) {
+    switch (M.tile) {
+        case 1024: return rows_f<1024>(s, M, vals, x, epi, st, partials);
+        case 4096: return rows_f<4096>(s, M, vals, x, epi, st, partials);
+        default: return rows_f<2048>(s, M, vals, x, epi, st, partials);
+    }
+}
+
+template <int TILE, typename Epi>
+cudaError_t rows_64(cudaStream_t s, const DevCsr &M, const double *x, const Epi &epi, DState *st,
+                    double *partials) {
+    auto kern = k_spmv_rows<TILE, Epi>;
+    const int g = grid_for(kern, 1, M.nblk);
+    kern<<<g, kThreads, 0, s>>>(view64(M), M.rb, M.nblk, x, epi, st, partials);
+    return cudaGetLastError();
+}
+
+// FP64 product with A (outer residual); the row blocks were built for M.tile.
+template <typename Epi>
+cudaError_t spmv_64(const DevCsr &M, cudaStream_t s, const double *x, const Epi &epi, DState *st,
+                    double *partials) {
+    switch (M.tile) {
+        case 1024: return rows_64<1024>(s, M, x, epi, st, partials);
+        case 4096: return rows_64<4096>(s, M, x, epi, st, partials);
+        default: return rows_64<2048>(s, M, x, epi, st, partials);
+    }
+}
+
+template <typename K>
+int sgrid(K kernel, long n) { return grid_for(kernel, kThreads, n); }
+
+}  // namespace
+
+struct MixedSolver : SolverBase {
+    MixedSolver() { kind = kKindMixed; }
+    int device = -1, n = 0;
+    fiim_options opt{};
+    bool bf16 = false;
+    cudaStream_t stream = nullptr;
+    Arena arena;
+    DevCsr A, G, H;
+    float *A32 = nullptr, *G32 = nullptr, *H32 = nullptr, *D32 = nullptr;
+    __nv_bfloat16 *G16 = nullptr, *H16 = nullptr;
+    double *x = nullptr, *b = nullptr, *r64 = nullptr, *stage = nullptr;
+    float *e = nullptr, *r = nullptr, *r0 = nullptr, *p = nullptr, *v = nullptr, *s = nullptr;
+    float *t = nullptr, *pc = nullptr, *sc = nullptr, *tm = nullptr;
+    DState *st = nullptr, *sto = nullptr, *hst = nullptr;
+    double *partials = nullptr;
+    unsigned long long *d_count = nullptr, *h_count = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    template <typename Epi>
+    cudaError_t spmv_gh(const DevCsr &M, bool is_g, const float *xx, const Epi &epi) {
+        if (bf16) return spmv_f(M, is_g ? G16 : H16, stream, xx, epi, st, partials);
+        return spmv_f(M, is_g ? G32 : H32, stream, xx, epi, st, partials);
+    }
+
+    int enqueue_inner(bool cond, cudaGraphConditionalHandle h) {
+        const long nn = n;
+        FIIM_CUDA(spmv_gh(H, false, p, mx::EpiScaleF{tm, D32}));
+        FIIM_CUDA(spmv_gh(G, true, tm, mx::EpiNormF{pc}));
+        FIIM_CUDA(spmv_f(A, A32, stream, pc, mx::EpiAlphaF{v, r0}, st, partials));
+        mx::k_update_s_f<<<sgrid(mx::k_update_s_f, nn), kThreads, 0, stream>>>(nn, r, v, e, s, st, partials);
+        FIIM_CUDA(cudaGetLastError());
+        FIIM_CUDA(spmv_gh(H, false, s, mx::EpiScaleF{tm, D32}));
+        FIIM_CUDA(spmv_gh(G, true, tm, mx::EpiStoreF{sc}));
+        FIIM_CUDA(spmv_f(A, A32, stream, sc, mx::EpiOmegaF{t, s}, st, partials));
+        mx::k_update_xr_f<<<sgrid(mx::k_update_xr_f, nn), kThreads, 0, stream>>>(nn, pc, sc, s, t, r0, e, r, st,
+                                                                                   partials);
+        FIIM_CUDA(cudaGetLastError());
+        mx::k_update_p_f<<<sgrid(mx::k_update_p_f, nn), kThreads, 0, stream>>>(nn, r, v, p, st, h, cond ? 1 : 0);
+        FIIM_CUDA(cudaGetLastError());
+        return FIIM_OK;
+    }
+
+    int build_graph() {
+        // Resolve launch shapes outside capture (every kernel returns at once: done = 1).
+        DState hd = {};
+        hd.done = 1;
+        *hst = hd;
+        FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
+        FIIM_TRY(enqueue_inner(false, cudaGraphConditionalHandle{}));
+        FIIM_CUDA(cudaStreamSynchronize(stream));
+        cudaGraph_t g = nullptr;
+        FIIM_CUDA(cudaGraphCreate(&g, 0));
+        cudaGraphConditionalHandle h;
+        FIIM_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        FIIM_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        FIIM_CUDA(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue_inner(true, h);
+        cudaGraph_t captured = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(stream, &captured);
+        if (rc != FIIM_OK) return rc;
+        FIIM_CUDA(ec);
+        FIIM_CUDA(cudaGraphInstantiate(&exec, g, 0));
+        graph = g;
+        return FIIM_OK;
+    }
+
+    // Tune the FP32 kernels' row-block size per matrix (speed only).
+    template <typename V>
+    int tune(DevCsr &M, const V *vals) {
+        const int cands[3] = {1024, 2048, 4096};
+        int best = 2048;
+        float best_ms = 1e30f;
+        FIIM_CUDA(cudaMemsetAsync(tm, 0, sizeof(float) * n, stream));
+        for (int c : cands) {
+            FIIM_TRY(set_tile(M, c, stream));
+            FIIM_CUDA(spmv_f(M, vals, stream, tm, mx::EpiStoreF{t}, nullptr, nullptr));
+            FIIM_CUDA(cudaEventRecord(ev0, stream));
+            for (int k = 0; k < 5; ++k) FIIM_CUDA(spmv_f(M, vals, stream, tm, mx::EpiStoreF{t}, nullptr, nullptr));
+            FIIM_CUDA(cudaEventRecord(ev1, stream));
+            FIIM_CUDA(cudaEventSynchronize(ev1));
+            float ms = 0.f;
+            FIIM_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+            if (ms < best_ms * 0.97f) {
+                best_ms = ms;
+                best = c;
+            }
+        }
+        return set_tile(M, best, stream);
+    }
+
+    int create(int n_, const int *Ai, const int *Aj, const double *Av, const int *Gi, const int *Gj,
+               const double *Gv, const double *IDv, const int *Hi, const int *Hj, const double *Hv,
+               const fiim_options &o) {
+        opt = o;
+        n = n_;
+        bf16 = (opt.precision == FIIM_MIXED_BF16);
+        if (n <= 0 || !Ai || !Aj || !Av || !Gi || !Gj || !Gv || !IDv || !Hi || !Hj || !Hv)
+            return set_error(FIIM_EARG, "mixed precision needs A, G, IDv and H");
+        if (opt.issym) return set_error(FIIM_EARG, "mixed precision takes general (non-symmetric-storage) input");
+        if (opt.variant == FIIM_ACIFIM && opt.mode != 'E')
+            return set_error(FIIM_EARG, "mixed precision applies the explicit product (mode 'E')");
+        if (!(opt.inner_tol > 0.0) || opt.inner_nmax <= 0 || opt.max_refine <= 0)
+            return set_error(FIIM_EARG, "inner_tol > 0, inner_nmax > 0 and max_refine > 0 are required");
+        FIIM_TRY(check_device(&device));
+        FIIM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        FIIM_CUDA(cudaEventCreate(&ev0));
+        FIIM_CUDA(cudaEventCreate(&ev1));
+        const bool dev = (opt.memory == FIIM_MEM_DEVICE);
+        auto nnz_of = [&](const int *rp) -> long {
+            if (!dev) return rp[n];
+            int z = 0;
+            if (cudaMemcpy(&z, rp + n, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+            return z;
+        };
+        const long nA = nnz_of(Ai), nG = nnz_of(Gi), nH = nnz_of(Hi);
+        if (nA < 0 || nG < 0 || nH < 0) return set_error(FIIM_ECUDA, "reading row offsets failed");
+        const size_t vsz = bf16 ? sizeof(__nv_bfloat16) : sizeof(float);
+        const int max_blocks = num_sms() * 32;
+        size_t bytes = csr_bytes(n, nA) + Arena::need(sizeof(float) * std::max<long>(nA, 1));
+        // G and H: index arrays + FP64 staging share (reused) + low-precision values
+        bytes += csr_bytes(n, nG) + csr_bytes(n, nH);
+        bytes += Arena::need(vsz * std::max<long>(nG, 1)) + Arena::need(vsz * std::max<long>(nH, 1));
+        bytes += 3 * Arena::need(sizeof(double) * n) + 11 * Arena::need(sizeof(float) * n);
+        bytes += 2 * Arena::need(sizeof(DState)) + Arena::need(sizeof(double) * 4 * max_blocks) + 4096;
+        FIIM_TRY(arena.reserve(bytes));
+        FIIM_TRY(carve_csr(arena, A, n, nA));
+        FIIM_TRY(carve_csr(arena, G, n, nG));   // G.v / H.v: FP64 staging, dropped after conversion
+        FIIM_TRY(carve_csr(arena, H, n, nH));
+        A32 = static_cast<float *>(arena.take(sizeof(float) * std::max<long>(nA, 1)));
+        if (bf16) {
+            G16 = static_cast<__nv_bfloat16 *>(arena.take(vsz * std::max<long>(nG, 1)));
+            H16 = static_cast<__nv_bfloat16 *>(arena.take(vsz * std::max<long>(nH, 1)));
+        } else {
+            G32 = static_cast<float *>(arena.take(vsz * std::max<long>(nG, 1)));
+            H32 = static_cast<float *>(arena.take(vsz * std::max<long>(nH, 1)));
+        }
+        double **d64[] = {&x, &b, &r64};
+        for (auto pp : d64)
+            if (!(*pp = static_cast<double *>(arena.take(sizeof(double) * n)))) return set_error(FIIM_ENOMEM, "arena");
+        float **f32[] = {&D32, &e, &r, &r0, &p, &v, &s, &t, &pc, &sc, &tm};
+        for (auto pp : f32)
+            if (!(*pp = static_cast<float *>(arena.take(sizeof(float) * n)))) return set_error(FIIM_ENOMEM, "arena");
+        st = static_cast<DState *>(arena.take(sizeof(DState)));
+        sto = static_cast<DState *>(arena.take(sizeof(DState)));
+        partials = static_cast<double *>(arena.take(sizeof(double) * 4 * max_blocks));
+        d_count = static_cast<unsigned long long *>(arena.take(sizeof(unsigned long long)));
+        if (!A32 || !st || !sto || !partials || !d_count || (bf16 ? (!G16 || !H16) : (!G32 || !H32)))
+            return set_error(FIIM_ENOMEM, "arena exhausted");
+        FIIM_CUDA(cudaHostAlloc(&hst, 2 * sizeof(DState) + 64, cudaHostAllocDefault));
+        h_count = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(hst) + 2 * sizeof(DState) + 32);
+        FIIM_CUDA(cudaMemsetAsync(st, 0, sizeof(DState), stream));
+        FIIM_CUDA(cudaMemsetAsync(sto, 0, sizeof(DState), stream));
+
+        FIIM_TRY(upload_csr(A, nA, n, Ai, Aj, Av, 0, dev, stream, d_count, h_count));
+        FIIM_TRY(upload_csr(G, nG, n, Gi, Gj, Gv, 1, dev, stream, d_count, h_count));
+        FIIM_TRY(upload_csr(H, nH, n, Hi, Hj, Hv, 2, dev, stream, d_count, h_count));
+        auto conv = [&](const double *in, long cnt, float *o32, __nv_bfloat16 *o16) -> int {
+            if (cnt <= 0) return FIIM_OK;
+            if (o16) mx::k_to_bf16<<<sgrid(mx::k_to_bf16, cnt), kThreads, 0, stream>>>(cnt, in, o16);
+            else mx::k_to_f32<<<sgrid(mx::k_to_f32, cnt), kThreads, 0, stream>>>(cnt, in, o32);
+            FIIM_CUDA(cudaGetLastError());
+            return FIIM_OK;
+        };
+        FIIM_TRY(conv(A.v, A.nnz, A32, nullptr));
+        FIIM_TRY(conv(G.v, G.nnz, G32, G16));
+        FIIM_TRY(conv(H.v, H.nnz, H32, H16));
+        // D^-1 in FP32: stage through r64.
+        FIIM_CUDA(cudaMemcpyAsync(r64, IDv, sizeof(double) * n, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                  stream));
+        FIIM_TRY(conv(r64, n, D32, nullptr));
+        FIIM_CUDA(cudaStreamSynchronize(stream));
+        G.v = nullptr;   // the FP64 factor values are not used past set-up
+        H.v = nullptr;
+        if (opt.autotune) {
+            FIIM_TRY(tune(A, A32));
+            if (bf16) {
+                FIIM_TRY(tune(G, G16));
+                FIIM_TRY(tune(H, H16));
+            } else {
+                FIIM_TRY(tune(G, G32));
+                FIIM_TRY(tune(H, H32));
+            }
+        } else {
+            FIIM_TRY(set_tile(A, 2048, stream));
+            FIIM_TRY(set_tile(G, 2048, stream));
+            FIIM_TRY(set_tile(H, 2048, stream));
+        }
+        return build_graph();
+    }
+
+    int solve(const double *b_in, double *x_io, double tol, int nmax, fiim_result *res) {
+        FIIM_CUDA(cudaSetDevice(device));
+        const bool dev = (opt.memory == FIIM_MEM_DEVICE);
+        FIIM_CUDA(cudaEventRecord(ev0, stream));
+        FIIM_CUDA(cudaMemcpyAsync(b, b_in, sizeof(double) * n, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                  stream));
+        FIIM_CUDA(cudaMemcpyAsync(x, x_io, sizeof(double) * n, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                  stream));
+        DState hi = {};
+        hi.tol = opt.inner_tol;
+        hi.eps = 1.11022302462516e-16;
+        hi.nmax = std::min(opt.inner_nmax, std::max(nmax, 1));
+        hi.info = -1;
+        hi.maxmsteps = (opt.variant == FIIM_ACIFIM) ? std::min(std::max(n, 2000) / 50, 40)
+                                                     : std::min(std::max(n, 500) / 50, 20);
+        hi.alpha_guard = (opt.variant == FIIM_ACIFIM);
+        DState *hso = hst + 1;
+        int total_iters = 0, steps = 0, launches = 0, info = 3;
+        double nb = 0.0, nr = 0.0;
+        auto residual = [&]() -> int {
+            FIIM_CUDA(spmv_64(A, stream, x, EpiResid{b, r64}, sto, partials));
+            FIIM_CUDA(cudaMemcpyAsync(hso, sto, sizeof(DState), cudaMemcpyDeviceToHost, stream));
+            FIIM_CUDA(cudaStreamSynchronize(stream));
+            ++launches;
+            nr = std::sqrt(hso->ts);
+            nb = std::sqrt(hso->tt);
+            return FIIM_OK;
+        };
+        FIIM_TRY(residual());
+        const double r_start = nr;
+        while (true) {
+            if (nr <= tol * nb) { info = 0; break; }
+            if (steps >= opt.max_refine || total_iters >= nmax) { info = 3; break; }
+            *hst = hi;
+            hst->nmax = std::min(hi.nmax, nmax - total_iters);
+            FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
+            mx::k_inner_init<<<sgrid(mx::k_inner_init, n), kThreads, 0, stream>>>(n, r64, sto, r, r0, p, e, st, partials);
+            FIIM_CUDA(cudaGetLastError());
+            FIIM_CUDA(cudaGraphLaunch(exec, stream));
+            mx::k_promote<<<sgrid(mx::k_promote, n), kThreads, 0, stream>>>(n, e, x, sto);
+            FIIM_CUDA(cudaGetLastError());
+            FIIM_CUDA(cudaMemcpyAsync(hst, st, sizeof(DState), cudaMemcpyDeviceToHost, stream));
+            const double prev = nr;
+            FIIM_TRY(residual());
+            ++steps;
+            // iterations run: the completed ones plus the one a test stopped (info 0, 1, 2)
+            total_iters += hst->iter + ((hst->info >= 0 && hst->info <= 2) ? 1 : 0);
+            launches += 2 + hst->loops * 9;
+            if (hst->info == -5) return set_error(FIIM_ETIMEOUT, "device loop guard tripped");
+            if (!(nr < prev)) { info = (hst->info == 1 || hst->info == 2) ? hst->info : 1; break; }
+        }
+        FIIM_CUDA(cudaMemcpyAsync(x_io, x, sizeof(double) * n, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                  stream));
+        FIIM_CUDA(cudaEventRecord(ev1, stream));
+        FIIM_CUDA(cudaStreamSynchronize(stream));
+        float ms = 0.f;
+        FIIM_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        if (res) {
+            res->resval = r_start > 0 ? nr / r_start : nr;
+            res->true_relres = nb > 0 ? nr / nb : nr;
+            res->iter = total_iters;
+            res->info = info;
+            res->refine_steps = steps;
+            res->device_ms = ms;
+            res->launches = launches;
+        }
+        if (opt.verbose)
+            std::cout << "Mixed-precision refinement: " << steps << " steps, " << total_iters
+                      << " inner iterations, ||b-Ax||/||b|| = " << (nb > 0 ? nr / nb : nr) << ", info " << info << "\n";
+        return FIIM_OK;
+    }
+
+    void destroy() {
+        if (device >= 0) cudaSetDevice(device);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+        if (hst) cudaFreeHost(hst);
+        exec = nullptr;
+        graph = nullptr;
+        ev0 = ev1 = nullptr;
+        stream = nullptr;
+        hst = nullptr;
+        arena.release();
+    }
+};
+
+}  // namespace fiim
 
 int fiim_is_mixed(fiim_solver_t h) {
     return h && reinterpret_cast<fiim::SolverBase *>(h)->kind == fiim::kKindMixed;
 }
-int fiim_mixed_create(fiim_solver_t *, int, const int *, const int *, const double *, const int *,
-                      const int *, const double *, const double *, const int *, const int *,
-                      const double *, const fiim_options *) {
-    return fiim::set_error(FIIM_EARG, "mixed precision not available in this build");
+
+int fiim_mixed_create(fiim_solver_t *out, int n, const int *Ai, const int *Aj, const double *Av,
+                      const int *Gi, const int *Gj, const double *Gv, const double *IDv,
+                      const int *Hi, const int *Hj, const double *Hv, const fiim_options *opt) {
+    auto *s = new fiim::MixedSolver;
+    const int rc = s->create(n, Ai, Aj, Av, Gi, Gj, Gv, IDv, Hi, Hj, Hv, *opt);
+    if (rc != FIIM_OK) {
+        s->destroy();
+        delete s;
+        return rc;
+    }
+    *out = reinterpret_cast<fiim_solver_t>(s);
+    return FIIM_OK;
 }
-int fiim_mixed_solve(fiim_solver_t, const double *, double *, double, int, fiim_result *) {
-    return fiim::set_error(FIIM_EARG, "mixed precision not available in this build");
+
+int fiim_mixed_solve(fiim_solver_t h, const double *b, double *x, double tol, int NMAX,
+                     fiim_result *res) {
+    return reinterpret_cast<fiim::MixedSolver *>(h)->solve(b, x, tol, NMAX, res);
 }
-int64_t fiim_mixed_device_bytes(fiim_solver_t) { return -1; }
-int fiim_mixed_destroy(fiim_solver_t) { return FIIM_OK; }
+
+int64_t fiim_mixed_device_bytes(fiim_solver_t h) {
+    return (int64_t) reinterpret_cast<fiim::MixedSolver *>(h)->arena.cap;
+}
+
+int fiim_mixed_destroy(fiim_solver_t h) {
+    auto *s = reinterpret_cast<fiim::MixedSolver *>(h);
+    s->destroy();
+    delete s;
+    return FIIM_OK;
+}

@@ -1,0 +1,201 @@
+// Device kernels of the mixed-precision solve: FP64 iterative refinement around an FP32
+// inner BiCGSTAB with the same control flow as the reference's loop
+// (AFIIM/src/bicgstab.cpp:168-275), on FP32 vectors and FP32 (or BF16) matrix values.
+//
+// Inner iteration = the nine launches of the FP64 path, on 4-byte vectors:
+//   tm = D^{-1} o (H p); pc = G tm (+||pc||^2); v = A32 pc, alpha; s = r - alpha v (+||r||^2,
+//   ||e||^2); tm = D^{-1} o (H s); sc = G tm; t = A32 sc, omega; e += alpha pc + omega sc,
+//   r = s - omega t, m1 = r0.r, tests, beta; p = r + beta (p - omega v).
+// Matrix products accumulate in FP32 (rows summed in storage order from shared memory);
+// every dot product and norm accumulates FP32 products in FP64, and the recurrence scalars
+// (alpha, omega, beta, rho) are FP64 in DState.
+//
+// Outer step (FP64): r64 = b - A x with the FP64 A (the FP64 kernel's EpiResid), the inner
+// solve runs on r64 / ||r64|| from e = 0, then x += ||r64|| e.
+#pragma once
+
+#include "fiim_kernels.cuh"
+
+namespace fiim {
+namespace mx {
+
+// ---------------------------------------------------------------- FP32 epilogues
+struct EpiStoreF {
+    FIIM_EPI(1, false, true);
+    float *y;
+    __device__ void emit(long i, float s, double (&)[NR]) const { y[i] = s; }
+    __device__ void finish(DState *, const double *) const {}
+};
+struct EpiScaleF {                 // y = d o (M x)
+    FIIM_EPI(1, false, true);
+    float *y;
+    const float *__restrict__ d;
+    __device__ void emit(long i, float s, double (&)[NR]) const { y[i] = __ldg(d + i) * s; }
+    __device__ void finish(DState *, const double *) const {}
+};
+struct EpiNormF {                  // y = M x, ||y||^2 -> st->pc2
+    FIIM_EPI(1, true, true);
+    float *y;
+    __device__ void emit(long i, float s, double (&r)[NR]) const {
+        y[i] = s;
+        r[0] += (double)s * (double)s;
+    }
+    __device__ void finish(DState *st, const double *t) const { st->pc2 = t[0]; }
+};
+struct EpiAlphaF {                 // v = A pc, alpha = m1 / (r0 . v)
+    FIIM_EPI(1, true, true);
+    float *y;
+    const float *__restrict__ r0;
+    __device__ void emit(long i, float s, double (&r)[NR]) const {
+        y[i] = s;
+        r[0] += (double)__ldg(r0 + i) * (double)s;
+    }
+    __device__ void finish(DState *st, const double *t) const { EpiAlpha{nullptr, nullptr}.finish(st, t); }
+};
+struct EpiOmegaF {                 // t = A sc, omega = (t . s) / (t . t)
+    FIIM_EPI(2, true, true);
+    float *y;
+    const float *__restrict__ sv;
+    __device__ void emit(long i, float s, double (&r)[NR]) const {
+        y[i] = s;
+        r[0] += (double)s * (double)__ldg(sv + i);
+        r[1] += (double)s * (double)s;
+    }
+    __device__ void finish(DState *st, const double *t) const { EpiOmega{nullptr, nullptr}.finish(st, t); }
+};
+
+__device__ __forceinline__ float ldv(const float *p) { return __ldcs(p); }
+__device__ __forceinline__ float ldv(const __nv_bfloat16 *p) { return ldm(p); }
+
+// CSR-stream SpMV on FP32 / BF16 values and an FP32 vector (same row blocks as the FP64
+// kernel; products staged in shared memory, each row summed in storage order).
+template <int TILE, typename V, typename Epi>
+static __global__ void __launch_bounds__(kThreads)
+k_spmv_rows_f(CsrView<V> M, const int *__restrict__ rb, int nblk, const float *__restrict__ x,
+              Epi epi, DState *st, double *__restrict__ partials) {
+    if (Epi::GATED && st != nullptr && st->done) return;
+    __shared__ float prod[TILE];
+    double red[Epi::NR];
+#pragma unroll
+    for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
+    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        const int r0 = __ldg(rb + blk), r1 = __ldg(rb + blk + 1);
+        const int e0 = __ldg(M.rp + r0), e1 = __ldg(M.rp + r1);
+        if (e1 - e0 <= TILE) {
+#pragma unroll 4
+            for (int e = e0 + (int)threadIdx.x; e < e1; e += kThreads)
+                prod[e - e0] = ldv(M.v + e) * ldx(x + ldi(M.ci + e));
+            __syncthreads();
+            const int r = r0 + (int)threadIdx.x;
+            if (r < r1) {
+                const int b = __ldg(M.rp + r) - e0, e = __ldg(M.rp + r + 1) - e0;
+                float s = 0.f;
+                for (int k = b; k < e; ++k) s += prod[k];
+                epi.emit(r, s, red);
+            }
+            __syncthreads();
+        } else {
+            float s = 0.f;
+            for (int c0 = e0; c0 < e1; c0 += TILE) {
+                const int c1 = min(c0 + TILE, e1);
+                for (int e = c0 + (int)threadIdx.x; e < c1; e += kThreads)
+                    prod[e - c0] = ldv(M.v + e) * ldx(x + ldi(M.ci + e));
+                __syncthreads();
+                if (threadIdx.x == 0)
+                    for (int k = 0; k < c1 - c0; ++k) s += prod[k];
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) epi.emit(r0, s, red);
+        }
+    }
+    if constexpr (Epi::REDUCES) grid_reduce<Epi::NR>(red, partials, st, epi);
+}
+
+// ---------------------------------------------------------------- inner start / updates
+// Inner start from e = 0: r = r0 = p = r64 / ||r64|| in FP32 (||r64||^2 is sto->ts from
+// the residual kernel); ||r0||^2 accumulated in FP64 -> ro, m1, rc (FinInit).
+static __global__ void __launch_bounds__(kThreads)
+k_inner_init(long n, const double *__restrict__ r64, const DState *sto, float *__restrict__ r,
+             float *__restrict__ r0, float *__restrict__ p, float *__restrict__ e, DState *st,
+             double *__restrict__ partials) {
+    const double inv = 1.0 / sqrt(sto->ts);
+    double red[1] = {0.0};
+    FIIM_FOR_ROWS(i, n) {
+        const float ri = (float)(r64[i] * inv);
+        r[i] = ri;
+        r0[i] = ri;
+        p[i] = ri;
+        e[i] = 0.f;
+        red[0] += (double)ri * (double)ri;
+    }
+    grid_reduce<1>(red, partials, st, FinInit{});
+}
+
+static __global__ void __launch_bounds__(kThreads)
+k_update_s_f(long n, const float *__restrict__ r, const float *__restrict__ v,
+             const float *__restrict__ e, float *__restrict__ s, DState *st,
+             double *__restrict__ partials) {
+    if (st->done) return;
+    const float na = (float)(-st->alpha);
+    double red[2] = {0.0, 0.0};
+    FIIM_FOR_ROWS(i, n) {
+        const float ri = r[i], ei = e[i];
+        s[i] = fmaf(na, v[i], ri);
+        red[0] += (double)ri * (double)ri;
+        red[1] += (double)ei * (double)ei;
+    }
+    grid_reduce<2>(red, partials, st, FinS{});
+}
+
+static __global__ void __launch_bounds__(kThreads)
+k_update_xr_f(long n, const float *__restrict__ pc, const float *__restrict__ sc,
+              const float *__restrict__ s, const float *__restrict__ t,
+              const float *__restrict__ r0, float *__restrict__ e, float *__restrict__ r,
+              DState *st, double *__restrict__ partials) {
+    if (st->done) return;
+    const float a = (float)st->alpha, om = (float)st->omega;
+    double red[1] = {0.0};
+    FIIM_FOR_ROWS(i, n) {
+        e[i] = fmaf(om, sc[i], fmaf(a, pc[i], e[i]));
+        const float ri = fmaf(-om, t[i], s[i]);
+        r[i] = ri;
+        red[0] += (double)r0[i] * (double)ri;
+    }
+    grid_reduce<1>(red, partials, st, FinControl{});
+}
+
+static __global__ void __launch_bounds__(kThreads)
+k_update_p_f(long n, const float *__restrict__ r, const float *__restrict__ v,
+             float *__restrict__ p, DState *st, cudaGraphConditionalHandle h, int cond) {
+    if (cond && blockIdx.x == 0 && threadIdx.x == 0) {
+        const int loops = ++st->loops;
+        if (!st->done && loops > st->nmax + 2) {
+            st->info = -5;
+            st->done = 1;
+        }
+        cudaGraphSetConditional(h, st->done ? 0u : 1u);
+    }
+    if (st->done) return;
+    const float b = (float)st->beta, c = (float)(-st->beta * st->omega);
+    FIIM_FOR_ROWS(i, n) { p[i] = fmaf(c, v[i], fmaf(b, p[i], r[i])); }
+}
+
+// x += ||r64|| e (FP64): the refinement step.
+static __global__ void __launch_bounds__(kThreads)
+k_promote(long n, const float *__restrict__ e, double *__restrict__ x, const DState *sto) {
+    const double scale = sqrt(sto->ts);
+    FIIM_FOR_ROWS(i, n) { x[i] += scale * (double)e[i]; }
+}
+
+// Matrix values to the inner precision (round to nearest).
+static __global__ void __launch_bounds__(kThreads)
+k_to_f32(long n, const double *__restrict__ in, float *__restrict__ out) {
+    FIIM_FOR_ROWS(i, n) { out[i] = __double2float_rn(in[i]); }
+}
+static __global__ void __launch_bounds__(kThreads)
+k_to_bf16(long n, const double *__restrict__ in, __nv_bfloat16 *__restrict__ out) {
+    FIIM_FOR_ROWS(i, n) { out[i] = __double2bfloat16(in[i]); }
+}
+
+}  // namespace mx
+}  // namespace fiim

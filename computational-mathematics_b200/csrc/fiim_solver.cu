@@ -104,30 +104,6 @@ void Arena::release() {
 size_t Arena::need(size_t bytes) { return (bytes + 255) & ~size_t(255); }
 
 // ------------------------------------------------------------------ launch shapes
-// Resident blocks per SM of a kernel, cached by kernel address.
-template <typename K>
-int occupancy(K kernel) {
-    static std::mutex mu;
-    static std::map<const void *, int> occ;
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = occ.find((const void *)kernel);
-    if (it != occ.end()) return it->second;
-    int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kThreads, 0) != cudaSuccess || b < 1) {
-        cudaGetLastError();
-        b = 4;
-    }
-    occ[(const void *)kernel] = b;
-    return b;
-}
-
-// Grid: enough blocks for the work, capped at one full wave of resident blocks.
-template <typename K>
-int grid_for(K kernel, long units_per_block, long units) {
-    const long need = std::max<long>(1, (units + units_per_block - 1) / units_per_block);
-    return (int)std::min<long>(need, (long)occupancy(kernel) * num_sms());
-}
-
 template <int VEC, int FILL, typename Epi>
 static cudaError_t spmv_vec(cudaStream_t s, const CsrView<double> &M, const double *x, const Epi &epi,
                             DState *st, double *partials) {
@@ -202,7 +178,7 @@ void build_row_blocks(const std::vector<int> &rp, int tile, int max_rows, std::v
     }
 }
 
-static int set_tile(DevCsr &M, int tile, cudaStream_t s) {
+int set_tile(DevCsr &M, int tile, cudaStream_t s) {
     std::vector<int> rb;
     build_row_blocks(M.hrp, tile, kThreads, rb);
     M.tile = tile;
@@ -257,7 +233,7 @@ static int autotune_tile(DevCsr &M, const double *x, double *y, cudaStream_t s) 
 // ------------------------------------------------------------------ host CSR helpers
 // Full CSR of a symmetric matrix given by its stored upper triangle (entries with
 // col < row are ignored, as MKL's SYMMETRIC + UPPER descriptor does).
-static void expand_sym_upper(int n, const int *rp, const int *ci, const double *v, HostCsr &out) {
+void expand_sym_upper(int n, const int *rp, const int *ci, const double *v, HostCsr &out) {
     out.n = n;
     out.rp.assign(n + 1, 0);
     for (int i = 0; i < n; ++i)
@@ -293,7 +269,7 @@ static void expand_sym_upper(int n, const int *rp, const int *ci, const double *
 }
 
 // CSR of T^T where T is the upper triangle (col >= row) of (rp, ci, v).
-static void transpose_upper(int n, const int *rp, const int *ci, const double *v, HostCsr &out) {
+void transpose_upper(int n, const int *rp, const int *ci, const double *v, HostCsr &out) {
     out.n = n;
     out.rp.assign(n + 1, 0);
     for (int i = 0; i < n; ++i)
@@ -311,7 +287,7 @@ static void transpose_upper(int n, const int *rp, const int *ci, const double *v
             }
 }
 
-static void signature(DevCsr &M, const int *host_rp) {
+void signature(DevCsr &M, const int *host_rp) {
     M.sig.clear();
     M.sig.push_back(M.n);
     M.sig.push_back(M.nnz);
@@ -324,7 +300,7 @@ static void signature(DevCsr &M, const int *host_rp) {
 // TRIANGULAR fill semantics: fill 1 keeps col >= row, fill 2 keeps col <= row
 // (AFIIM/src/bicgstab.cpp:140-147). The check runs on the device; the rare matrix
 // with entries outside its triangle is compacted on the host.
-static int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, const double *v,
+int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, const double *v,
                       int fill, bool device_src, cudaStream_t s, unsigned long long *d_count,
                       unsigned long long *h_count) {
     M.n = n;
@@ -384,7 +360,7 @@ static int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *
     return FIIM_OK;
 }
 
-static int carve_csr(Arena &ar, DevCsr &M, long n, long nnz) {
+int carve_csr(Arena &ar, DevCsr &M, long n, long nnz) {
     M.rp = static_cast<int *>(ar.take(sizeof(int) * (n + 1)));
     M.ci = static_cast<int *>(ar.take(sizeof(int) * std::max<long>(nnz, 1)));
     M.v = static_cast<double *>(ar.take(sizeof(double) * std::max<long>(nnz, 1)));
@@ -393,7 +369,7 @@ static int carve_csr(Arena &ar, DevCsr &M, long n, long nnz) {
     return FIIM_OK;
 }
 
-static size_t csr_bytes(long n, long nnz) {
+size_t csr_bytes(long n, long nnz) {
     return 2 * Arena::need(sizeof(int) * (n + 1)) + Arena::need(sizeof(int) * std::max<long>(nnz, 1)) +
            Arena::need(sizeof(double) * std::max<long>(nnz, 1));
 }
