@@ -311,6 +311,11 @@ struct MixedSolver : SolverBase {
             if (steps >= opt.max_refine || total_iters >= nmax) { info = 3; break; }
             *hst = hi;
             hst->nmax = std::min(hi.nmax, nmax - total_iters);
+            // Ask the inner solve for no more than the reduction still missing (with a margin
+            // of 3x), and never for less than inner_tol: the last step of a refinement then
+            // stops as soon as the FP64 target is within reach.
+            const double missing = tol * nb / nr;
+            hst->tol = std::max(opt.inner_tol, std::min(0.5, missing / 3.0));
             FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
             mx::k_inner_init<<<sgrid(mx::k_inner_init, n), kThreads, 0, stream>>>(n, r64, sto, r, r0, p, e, st, partials);
             FIIM_CUDA(cudaGetLastError());
