@@ -1,0 +1,335 @@
+// Device kernels of the batched solve: many independent systems, concatenated as one
+// block-diagonal CSR, each running the reference's BiCGSTAB (AFIIM/src/bicgstab.cpp:168-275
+// or ACIFIM/src/bicgstab.cpp:197-304) with its own scalars and termination.
+//
+// Row blocks (<= 256 rows, <= TILE entries) never straddle two systems. Every kernel walks
+// row blocks; a block of a system that has finished is skipped. Reductions are per system:
+// each row block reduces to one partial, and the last block of a system to finish (a
+// per-system ticket) adds that system's partials in block order and applies the system's
+// scalar step. Vectors are FP64; factor values may be FP64, FP32 or BF16 (widened to FP64
+// before the rounded product), so every vector operation is the reference's, bit for bit,
+// on the factors as stored.
+#pragma once
+
+#include "fiim_kernels.cuh"
+
+namespace fiim {
+namespace bt {
+
+struct BGlobal {
+    double tol, eps;
+    int nmax, alpha_guard, active, loops;
+};
+
+// Per-system state, structure of arrays (nsys entries each).
+struct BState {
+    double *ro, *rc, *m1, *m2, *alpha, *omega, *beta, *pc2, *x2, *r2, *ts, *tt;
+    int *iter, *stag, *msteps, *maxmsteps, *info, *done;
+    unsigned int *ticket;
+    BGlobal *g;
+};
+
+__device__ __forceinline__ void retire(BState &bs, int k, int info) {
+    bs.info[k] = info;
+    bs.done[k] = 1;
+    atomicSub(&bs.g->active, 1);
+}
+
+// ---------------------------------------------------------------- per-system scalar steps
+struct BFinInit {   // ro = ||r0||, m1 = ro^2, rc = ro (AFIIM/src/bicgstab.cpp:161-165)
+    __device__ void finish(BState &bs, int k, const double *t) const {
+        bs.ro[k] = sqrt(t[0]);
+        bs.m1[k] = bs.ro[k] * bs.ro[k];
+        bs.rc[k] = bs.ro[k];
+        bs.iter[k] = 0;
+        bs.stag[k] = 0;
+        bs.msteps[k] = 0;
+        if (bs.g->nmax <= 0) retire(bs, k, bs.g->nmax == 0 ? 3 : -1);
+    }
+};
+struct BFinS {
+    __device__ void finish(BState &bs, int k, const double *t) const {
+        bs.r2[k] = t[0];
+        bs.x2[k] = t[1];
+    }
+};
+struct BFinControl {   // AFIIM/src/bicgstab.cpp:201-274, per system
+    __device__ void finish(BState &bs, int k, const double *t) const {
+        const double a = bs.alpha[k], om = bs.omega[k];
+        if (fabs(a) * sqrt(bs.pc2[k]) < bs.g->eps * sqrt(bs.x2[k])) bs.stag[k]++;
+        else bs.stag[k] = 0;
+        const double prc = bs.rc[k];
+        bs.rc[k] = sqrt(bs.r2[k]);
+        if (prc < bs.rc[k]) bs.msteps[k]++;
+        else bs.msteps[k] = 0;
+        if (bs.msteps[k] >= bs.maxmsteps[k]) { retire(bs, k, 1); return; }
+        if (bs.stag[k] >= 3) { retire(bs, k, 2); return; }
+        if (bs.rc[k] < bs.g->tol * bs.ro[k]) { retire(bs, k, 0); return; }
+        bs.m2[k] = bs.m1[k];
+        bs.m1[k] = t[0];
+        bs.beta[k] = bs.m1[k] * a / (om * bs.m2[k]);
+        bs.iter[k]++;
+        if (bs.iter[k] >= bs.g->nmax) retire(bs, k, 3);
+    }
+};
+
+// ---------------------------------------------------------------- epilogues (FP64 vectors)
+struct BEpiScale {
+    FIIM_EPI(1, false, true);
+    double *y;
+    const double *__restrict__ d;
+    __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = __dmul_rn(__ldg(d + i), s); }
+    __device__ void finish(BState &, int, const double *) const {}
+};
+struct BEpiStore {
+    FIIM_EPI(1, false, true);
+    double *y;
+    __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = s; }
+    __device__ void finish(BState &, int, const double *) const {}
+};
+struct BEpiNorm {
+    FIIM_EPI(1, true, true);
+    double *y;
+    __device__ void emit(long i, double s, double (&r)[NR]) const { y[i] = s; r[0] += s * s; }
+    __device__ void finish(BState &bs, int k, const double *t) const { bs.pc2[k] = t[0]; }
+};
+struct BEpiAlpha {
+    FIIM_EPI(1, true, true);
+    double *y;
+    const double *__restrict__ r0;
+    __device__ void emit(long i, double s, double (&r)[NR]) const {
+        y[i] = s;
+        r[0] += __ldg(r0 + i) * s;
+    }
+    __device__ void finish(BState &bs, int k, const double *t) const {
+        bs.alpha[k] = bs.m1[k] / t[0];
+        if (bs.g->alpha_guard && !isfinite(bs.alpha[k])) {   // ACIFIM/src/bicgstab.cpp:208-213
+            bs.iter[k] = bs.g->nmax;
+            retire(bs, k, 3);
+        }
+    }
+};
+struct BEpiOmega {
+    FIIM_EPI(2, true, true);
+    double *y;
+    const double *__restrict__ sv;
+    __device__ void emit(long i, double s, double (&r)[NR]) const {
+        y[i] = s;
+        r[0] += s * __ldg(sv + i);
+        r[1] += s * s;
+    }
+    __device__ void finish(BState &bs, int k, const double *t) const { bs.omega[k] = t[0] / t[1]; }
+};
+struct BEpiInit {
+    FIIM_EPI(1, true, true);
+    const double *__restrict__ b;
+    double *p, *r0, *r;
+    __device__ void emit(long i, double s, double (&red)[NR]) const {
+        const double pi = __dadd_rn(b[i], __dmul_rn(-1.0, s));
+        p[i] = pi;
+        r0[i] = pi;
+        r[i] = pi;
+        red[0] += pi * pi;
+    }
+    __device__ void finish(BState &bs, int k, const double *t) const { BFinInit{}.finish(bs, k, t); }
+};
+struct BEpiResid {
+    FIIM_EPI(2, true, false);
+    const double *__restrict__ b;
+    __device__ void emit(long i, double s, double (&red)[NR]) const {
+        const double bi = b[i], ri = bi - s;
+        red[0] += ri * ri;
+        red[1] += bi * bi;
+    }
+    __device__ void finish(BState &bs, int k, const double *t) const {
+        bs.ts[k] = t[0];
+        bs.tt[k] = t[1];
+    }
+};
+
+// ---------------------------------------------------------------- per-system reduction
+// Called by every thread of the CTA once per row block (uniformly). Reduces `v` over the
+// CTA, stores the block's partial, and, in the last block of system k, adds the system's
+// partials in block order and runs fin.finish(bs, k, totals).
+template <int NR, class Fin>
+__device__ __forceinline__ void block_to_system(double (&v)[NR], int blk, int k,
+                                                const int *__restrict__ sys_blk,
+                                                double *__restrict__ partials, BState &bs,
+                                                const Fin &fin) {
+    __shared__ double sm[kWarps][NR];
+    __shared__ int last;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NR; ++j) v[j] = warp_sum(v[j]);
+    if (lane == 0)
+#pragma unroll
+        for (int j = 0; j < NR; ++j) sm[w][j] = v[j];
+    __syncthreads();
+    const int b0 = __ldg(sys_blk + k), b1 = __ldg(sys_blk + k + 1);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int j = 0; j < NR; ++j) {
+            double s = 0.0;
+#pragma unroll
+            for (int q = 0; q < kWarps; ++q) s += sm[q][j];
+            partials[(size_t)blk * NR + j] = s;
+        }
+        __threadfence();
+        const unsigned t = atomicAdd(&bs.ticket[k], 1u);
+        last = (t == (unsigned)(b1 - b0 - 1));
+    }
+    __syncthreads();
+    if (last) {
+        __threadfence();
+        double acc[NR];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) acc[j] = 0.0;
+        for (int q = b0 + (int)threadIdx.x; q < b1; q += kThreads)
+#pragma unroll
+            for (int j = 0; j < NR; ++j) acc[j] += __ldcg(partials + (size_t)q * NR + j);
+#pragma unroll
+        for (int j = 0; j < NR; ++j) acc[j] = warp_sum(acc[j]);
+        __syncthreads();
+        if (lane == 0)
+#pragma unroll
+            for (int j = 0; j < NR; ++j) sm[w][j] = acc[j];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot[NR];
+#pragma unroll
+            for (int j = 0; j < NR; ++j) {
+                double s = 0.0;
+#pragma unroll
+                for (int q = 0; q < kWarps; ++q) s += sm[q][j];
+                tot[j] = s;
+            }
+            bs.ticket[k] = 0u;
+            fin.finish(bs, k, tot);
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ double widen(double v) { return v; }
+__device__ __forceinline__ double widen(float v) { return (double)v; }
+
+// ---------------------------------------------------------------- batched CSR-stream SpMV
+template <int TILE, typename V, typename Epi>
+static __global__ void __launch_bounds__(kThreads)
+k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ blk_sys,
+        const int *__restrict__ sys_blk, int nblk, const double *__restrict__ x, Epi epi, BState bs,
+        double *__restrict__ partials) {
+    __shared__ double prod[TILE];
+    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        const int k = __ldg(blk_sys + blk);
+        if (Epi::GATED && bs.done[k]) continue;           // uniform in the CTA
+        double red[Epi::NR];
+#pragma unroll
+        for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
+        const int r0 = __ldg(rb + blk), r1 = __ldg(rb + blk + 1);
+        const int e0 = __ldg(M.rp + r0), e1 = __ldg(M.rp + r1);
+        if (e1 - e0 <= TILE) {
+#pragma unroll 4
+            for (int e = e0 + (int)threadIdx.x; e < e1; e += kThreads)
+                prod[e - e0] = __dmul_rn(widen(ldm(M.v + e)), ldx(x + ldi(M.ci + e)));
+            __syncthreads();
+            const int r = r0 + (int)threadIdx.x;
+            if (r < r1) {
+                const int b = __ldg(M.rp + r) - e0, e = __ldg(M.rp + r + 1) - e0;
+                double s = 0.0;
+                for (int q = b; q < e; ++q) s = __dadd_rn(s, prod[q]);
+                epi.emit(r, s, red);
+            }
+            __syncthreads();
+        } else {
+            double s = 0.0;
+            for (int c0 = e0; c0 < e1; c0 += TILE) {
+                const int c1 = min(c0 + TILE, e1);
+                for (int e = c0 + (int)threadIdx.x; e < c1; e += kThreads)
+                    prod[e - c0] = __dmul_rn(widen(ldm(M.v + e)), ldx(x + ldi(M.ci + e)));
+                __syncthreads();
+                if (threadIdx.x == 0)
+                    for (int q = 0; q < c1 - c0; ++q) s = __dadd_rn(s, prod[q]);
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) epi.emit(r0, s, red);
+        }
+        if constexpr (Epi::REDUCES) block_to_system<Epi::NR>(red, blk, k, sys_blk, partials, bs, epi);
+    }
+}
+
+// ---------------------------------------------------------------- batched vector updates
+// Each walks A's row blocks (<= 256 rows each); thread t owns row rb[blk] + t.
+static __global__ void __launch_bounds__(kThreads)
+k_bupdate_s(const int *__restrict__ rb, const int *__restrict__ blk_sys, const int *__restrict__ sys_blk,
+            int nblk, const double *__restrict__ r, const double *__restrict__ v,
+            const double *__restrict__ x, double *__restrict__ s, BState bs, double *__restrict__ partials) {
+    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        const int k = __ldg(blk_sys + blk);
+        if (bs.done[k]) continue;                         // uniform in the CTA
+        const int row = __ldg(rb + blk) + (int)threadIdx.x;
+        double red[2] = {0.0, 0.0};
+        if (row < __ldg(rb + blk + 1)) {
+            const double ri = r[row], xi = x[row];
+            s[row] = __dadd_rn(ri, __dmul_rn(-bs.alpha[k], v[row]));
+            red[0] = ri * ri;
+            red[1] = xi * xi;
+        }
+        block_to_system<2>(red, blk, k, sys_blk, partials, bs, BFinS{});
+    }
+}
+
+static __global__ void __launch_bounds__(kThreads)
+k_bupdate_xr(const int *__restrict__ rb, const int *__restrict__ blk_sys, const int *__restrict__ sys_blk,
+             int nblk, const double *__restrict__ pc, const double *__restrict__ sc,
+             const double *__restrict__ s, const double *__restrict__ t, const double *__restrict__ r0,
+             double *__restrict__ x, double *__restrict__ r, BState bs, double *__restrict__ partials) {
+    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        const int k = __ldg(blk_sys + blk);
+        if (bs.done[k]) continue;
+        const int row = __ldg(rb + blk) + (int)threadIdx.x;
+        double red[1] = {0.0};
+        if (row < __ldg(rb + blk + 1)) {
+            const double a = bs.alpha[k], om = bs.omega[k];
+            double xi = x[row];
+            xi = __dadd_rn(xi, __dmul_rn(a, pc[row]));
+            xi = __dadd_rn(xi, __dmul_rn(om, sc[row]));
+            x[row] = xi;
+            const double ri = __dadd_rn(s[row], __dmul_rn(-om, t[row]));
+            r[row] = ri;
+            red[0] = r0[row] * ri;
+        }
+        block_to_system<1>(red, blk, k, sys_blk, partials, bs, BFinControl{});
+    }
+}
+
+// Last kernel of the loop body: block 0 counts the body, stops the loop should it ever run
+// past nmax + 2 times (active = -1 flags that), and keeps the WHILE node going while any
+// system is active.
+static __global__ void __launch_bounds__(kThreads)
+k_bupdate_p(const int *__restrict__ rb, const int *__restrict__ blk_sys, int nblk,
+            const double *__restrict__ r, const double *__restrict__ v, double *__restrict__ p, BState bs,
+            cudaGraphConditionalHandle h, int cond) {
+    if (cond && blockIdx.x == 0 && threadIdx.x == 0) {
+        const int loops = ++bs.g->loops;
+        if (bs.g->active > 0 && loops > bs.g->nmax + 2) bs.g->active = -1;
+        cudaGraphSetConditional(h, bs.g->active > 0 ? 1u : 0u);
+    }
+    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        const int k = __ldg(blk_sys + blk);
+        const int row = __ldg(rb + blk) + (int)threadIdx.x;
+        if (bs.done[k] || row >= __ldg(rb + blk + 1)) continue;
+        const double b = bs.beta[k], c = __dmul_rn(-bs.beta[k], bs.omega[k]);
+        const double pi = __dadd_rn(__dmul_rn(c, v[row]), __dmul_rn(b, p[row]));
+        p[row] = __dadd_rn(pi, r[row]);
+    }
+}
+
+// Factor values to FP32 / BF16 (round to nearest) for the reduced-precision factor forms.
+static __global__ void __launch_bounds__(kThreads)
+k_vals_to_f32(long n, const double *__restrict__ in, float *__restrict__ out) {
+    FIIM_FOR_ROWS(i, n) { out[i] = __double2float_rn(in[i]); }
+}
+
+}  // namespace bt
+}  // namespace fiim

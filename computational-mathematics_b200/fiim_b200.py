@@ -37,7 +37,9 @@ _PRECISIONS = {"fp64": FP64, "fp32": MIXED_FP32, "bf16": MIXED_BF16}
 EXPORTS = (
     "fiim_last_error", "fiim_options_default", "fiim_EPBiCGSTAB_afiim", "fiim_EPBiCGSTAB_pdfiim",
     "fiim_PBiCGSTAB_acifim", "fiim_solver_create", "fiim_solver_solve", "fiim_solver_device_bytes",
-    "fiim_solver_spmv_shape", "fiim_solver_apply", "fiim_solver_kernel_times", "fiim_solver_iteration_bytes", "fiim_solver_destroy", "fiim_spmv", "fiim_prec_apply", "fiim_prec_apply_noalloc",
+    "fiim_solver_spmv_shape", "fiim_solver_apply", "fiim_solver_kernel_times", "fiim_solver_iteration_bytes",
+    "fiim_solver_destroy", "fiim_batch_create", "fiim_batch_solve", "fiim_batch_destroy",
+    "fiim_spmv", "fiim_prec_apply", "fiim_prec_apply_noalloc",
     "fiim_gen_poisson2d", "fiim_gen_convdiff3d", "fiim_gen_convdiff2d", "fiim_gen_batch_params",
     "fiim_gen_zipf", "fiim_gen_zipf_mean", "fiim_rand_normal", "fiim_model_rhs", "fiim_pdfiim_build",
 )
@@ -233,6 +235,65 @@ class Solver:
     def close(self):
         if self._h and self._h.value:
             lib().fiim_solver_destroy(self._h)
+            self._h = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ----------------------------------------------------------------------------- batched API
+def block_diag(mats):
+    """Concatenate CSR triples (Ai, Aj, Av) into one block-diagonal CSR in global numbering.
+    Returns ((Ai, Aj, Av), sys_rows)."""
+    sizes = [len(m[0]) - 1 for m in mats]
+    sys_rows = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    nnz = np.concatenate([[0], np.cumsum([int(m[0][-1]) for m in mats])])
+    Ai = np.concatenate([np.asarray(m[0][:-1], np.int64) + nnz[k] for k, m in enumerate(mats)] + [[nnz[-1]]])
+    Aj = np.concatenate([np.asarray(m[1], np.int64) + sys_rows[k] for k, m in enumerate(mats)])
+    Av = np.concatenate([np.asarray(m[2], np.float64) for m in mats])
+    return (Ai.astype(np.int32), Aj.astype(np.int32), Av), sys_rows
+
+
+class BatchSolver:
+    """Many independent systems in one device-driven loop (fiim_batch_*).
+
+    systems: list of (A, F) with A = (Ai, Aj, Av) and F = {Gi, Gj, Gv, IDv, Hi, Hj, Hv}.
+    precision: 'fp64' | 'fp32' | 'bf16' storage of G and H."""
+
+    def __init__(self, systems, variant="acifim", precision="fp64", memory="host"):
+        A, sys_rows = block_diag([s[0] for s in systems])
+        G, _ = block_diag([(s[1]["Gi"], s[1]["Gj"], s[1]["Gv"]) for s in systems])
+        H, _ = block_diag([(s[1]["Hi"], s[1]["Hj"], s[1]["Hv"]) for s in systems])
+        D = np.concatenate([np.asarray(s[1]["IDv"], np.float64) for s in systems])
+        self.sys_rows, self.nsys, self.N = sys_rows, len(systems), int(sys_rows[-1])
+        o = Options()
+        lib().fiim_options_default(C.byref(o))
+        o.variant = _VARIANTS[variant]
+        o.precision = _PRECISIONS[precision]
+        o.memory = MEM_HOST
+        self._h = C.c_void_p(0)
+        arrs = [A[0], A[1], A[2], G[0], G[1], G[2], D, H[0], H[1], H[2]]
+        _check(lib().fiim_batch_create(C.byref(self._h), C.c_int(self.nsys), _ptr(sys_rows),
+                                       *[_ptr(a) for a in arrs], C.byref(o)))
+
+    def solve(self, b, x, tol=1e-8, nmax=2000):
+        """b, x: concatenated FP64 vectors (x updated in place). Returns per-system arrays."""
+        k = self.nsys
+        it, info = np.zeros(k, np.int32), np.zeros(k, np.int32)
+        rv, tr = np.zeros(k), np.zeros(k)
+        r = Result()
+        b = _d(b)
+        assert x.dtype == np.float64 and x.flags.c_contiguous and len(x) == self.N
+        _check(lib().fiim_batch_solve(self._h, _ptr(b), _ptr(x), C.c_double(tol), C.c_int(nmax), _ptr(it),
+                                      _ptr(info), _ptr(rv), _ptr(tr), C.byref(r)))
+        return {"iter": it, "info": info, "resval": rv, "true_relres": tr, "summary": r.as_dict()}
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().fiim_batch_destroy(self._h)
             self._h = C.c_void_p(0)
 
     def __del__(self):

@@ -151,6 +151,33 @@ double fiim_solver_iteration_bytes(fiim_solver_t s);
 int fiim_solver_destroy(fiim_solver_t s);
 
 /* ===========================================================================
+ * Batched solve: many independent systems of uneven size in one device-driven loop.
+ * No counterpart in the reference, whose drivers solve one system per call; each system
+ * here runs the reference's loop (variant as in fiim_options) with its own scalars,
+ * divergence window and termination.
+ * The systems are passed concatenated as one block-diagonal CSR in global numbering:
+ * system k owns rows and columns [sys_rows[k], sys_rows[k+1]) (sys_rows is a host
+ * array of nsys + 1 offsets, sys_rows[0] = 0). opt->precision selects how G and H are
+ * stored: FIIM_FP64, FIIM_MIXED_FP32 or FIIM_MIXED_BF16 (values widened to FP64 before
+ * each product; A, D^{-1}, vectors and scalars stay FP64).
+ * ======================================================================== */
+typedef struct fiim_batch_s *fiim_batch_t;
+
+int fiim_batch_create(fiim_batch_t *out, int nsys, const int *sys_rows, const int *Ai,
+                      const int *Aj, const double *Av, const int *Gi, const int *Gj,
+                      const double *Gv, const double *IDv, const int *Hi, const int *Hj,
+                      const double *Hv, const fiim_options *opt);
+
+/* Solves every system. Per-system outputs (host arrays of nsys, any may be NULL): iter,
+ * info (reference codes), resval (rc/ro, lagged as in the reference) and the FP64 true
+ * residual ||b_k - A_k x_k|| / ||b_k||. summary: max iterations, worst info, device time. */
+int fiim_batch_solve(fiim_batch_t s, const double *b, double *x, double tol, int NMAX,
+                     int *iter, int *info, double *resval, double *true_relres,
+                     fiim_result *summary);
+
+int fiim_batch_destroy(fiim_batch_t s);
+
+/* ===========================================================================
  * Kernel-level entry points (device arrays, caller's stream; asynchronous).
  * ======================================================================== */
 

@@ -1,0 +1,113 @@
+"""Batched solve on B200: independent systems of uneven size in one device-driven loop.
+
+Per system, against the oracle run on the same system alone: the same info, iterations
+within +-2 of the oracle's rounding envelope (its counts when only the summation order of
+its dot products changes; computed here with the restatement's blocked dots), the
+tolerance reached, and the solution within the oracle's own spread. With FP32 or BF16
+factor storage the oracle runs on the factor values rounded the same way, so the per-
+system vectors are again the reference's own arithmetic.
+"""
+import numpy as np
+import pytest
+import torch  # noqa: F401  (keeps CUDA initialised in the same order as the other GPU tests)
+
+import fiim_b200 as FB
+import pyoracle as O
+from conftest import sub
+from test_oracle import identity_factors, skew_system
+
+pytestmark = pytest.mark.gpu
+
+BLOCKS = list(range(1, 25)) + [32, 48, 64, 96, 128, 256, 512]
+
+
+def envelope(variant, A, b, F, nmax, tol=1e-8, **kw):
+    x1, res1, it1, info1 = O.bicgstab(variant, A, b, F, tol=tol, nmax=nmax, **kw)
+    its, spread = [it1], 0.0
+    try:
+        for B in BLOCKS:
+            O.set_dot_blocks(B)
+            x, _, it, info = O.bicgstab(variant, A, b, F, tol=tol, nmax=nmax, **kw)
+            if info == info1:
+                its.append(it)
+                spread = max(spread, np.linalg.norm(x - x1) / max(np.linalg.norm(x1), 1e-300))
+    finally:
+        O.set_dot_blocks(1)
+    return x1, info1, min(its), max(its), spread
+
+
+def rounded(F, precision):
+    if precision == "fp64":
+        return F
+    out = dict(F)
+    for k in ("Gv", "Hv"):
+        if precision == "fp32":
+            out[k] = F[k].astype(np.float32).astype(np.float64)
+        else:   # bf16, round to nearest even through torch
+            out[k] = torch.tensor(F[k], dtype=torch.float64).to(torch.bfloat16).to(torch.float64).numpy()
+    return out
+
+
+def convdiff_systems(count, seed, variant):
+    rng = np.random.default_rng(seed)
+    systems = []
+    for k in range(count):
+        N = int(rng.integers(10, 41))
+        _, diff, theta, pe = FB.batch_params(20261203, k)
+        A = FB.gen_convdiff2d(N, diff, theta, pe)
+        F = FB.pdfiim_build(A, 0.05, 2, 2, 1, -1, "I", "B")
+        b = FB.rand_normal(N * N, 1000 + k)
+        systems.append((A, F, b))
+    return systems
+
+
+def check_batch(systems, variant, precision, nmax=2000, extra=None):
+    S = FB.BatchSolver([(A, F) for A, F, _ in systems], variant=variant, precision=precision)
+    b = np.concatenate([s[2] for s in systems])
+    x = np.zeros_like(b)
+    res = S.solve(b, x, tol=1e-8, nmax=nmax)
+    S.close()
+    rows = S.sys_rows
+    for k, (A, F, bk) in enumerate(systems):
+        xk = x[rows[k]:rows[k + 1]]
+        xo, info, lo, hi, spread = envelope(variant, A, bk, rounded(F, precision), nmax, **(extra or {}))
+        it = int(res["iter"][k])
+        print(f"{variant}/{precision} system {k} n={len(bk)}: gpu iter {it} info {res['info'][k]} | "
+              f"oracle envelope [{lo},{hi}] info {info} | x diff {np.linalg.norm(xk - xo) / np.linalg.norm(xo):.2e}")
+        assert res["info"][k] == info
+        assert lo - 2 <= it <= hi + 2
+        if info == 0:
+            assert res["resval"][k] < 1e-8 and res["true_relres"][k] < 1e-6
+            assert np.linalg.norm(xk - xo) / np.linalg.norm(xo) <= 10 * spread + 1e-9
+    return res
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "bf16"])
+def test_batch_pdfiim_convdiff(precision):
+    check_batch(convdiff_systems(9, 7, "pdfiim"), "pdfiim", precision)
+
+
+def test_batch_acifim_golden_and_guard(golden):
+    """ACIFIM factors from the reference (sherman2, 2D convection-diffusion) batched with a
+    system whose alpha is non-finite at once (ACIFIM/src/bicgstab.cpp:208-213)."""
+    g1, g2 = golden("sherman2"), golden("convdiff2d48_acifim")
+    keep = ("Gi", "Gj", "Gv", "IDv", "Hi", "Hj", "Hv")
+    skew = skew_system(64)
+    systems = [((g2["Ai"], g2["Aj"], g2["Av"]), {k: g2[k] for k in keep}, g2["b"]),
+               (skew, identity_factors(64), np.ones(64)),
+               ((g1["Ai"], g1["Aj"], g1["Av"]), {k: v for k, v in sub(g1, "acifim_").items() if k in keep}, g1["b"])]
+    res = check_batch(systems, "acifim", "fp64")
+    assert res["info"][1] == 3 and res["iter"][1] == 2000
+
+
+def test_batch_matches_single_system_solver():
+    """One system in a batch and the same system through the single-system solver agree
+    (both within the oracle's envelope; here both exact for this well-conditioned case)."""
+    systems = convdiff_systems(4, 11, "pdfiim")
+    res = check_batch(systems, "pdfiim", "fp64")
+    for k, (A, F, b) in enumerate(systems):
+        S = FB.Solver(A, F, variant="pdfiim")
+        x = np.zeros(len(b))
+        r = S.solve(b, x, tol=1e-8, nmax=2000)
+        S.close()
+        assert abs(r["iter"] - int(res["iter"][k])) <= 2 and r["info"] == res["info"][k]
