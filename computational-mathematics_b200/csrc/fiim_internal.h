@@ -56,6 +56,7 @@ struct DevCsr {
     __nv_bfloat16 *v16 = nullptr;
     int vec = 8;                 // lanes per row of the set-up-free SpMV
     int tile = 2048;             // entries per row block of the CSR-stream SpMV
+    int staged = 0;              // 1: row blocks moved by bulk copies (fiim_pipe.cuh)
     int *rb = nullptr;           // row-block starts (device), nblk + 1 entries
     int nblk = 0;
     std::vector<int> hrp;        // row offsets on the host (row blocks, tuning key)

@@ -30,6 +30,7 @@
 #include "fiim_b200.h"
 #include "fiim_internal.h"
 #include "fiim_kernels.cuh"
+#include "fiim_pipe.cuh"
 #include "fiim_solver.h"
 
 namespace fiim {
@@ -137,10 +138,45 @@ static cudaError_t spmv_rows(cudaStream_t s, const DevCsr &M, const double *x, c
     return cudaGetLastError();
 }
 
-// Solver SpMV: CSR-stream over the matrix's row blocks, exact row order.
+template <int TILE, typename Epi>
+static cudaError_t spmv_pipe(cudaStream_t s, const DevCsr &M, const double *x, const Epi &epi, DState *st,
+                             double *partials, int *fault) {
+    auto kern = k_spmv_pipe<TILE, Epi>;
+    constexpr int smem = PipeSmem<TILE>::kBytes;
+    static std::mutex mu;
+    static std::map<int, int> per_sm;   // device -> resident CTAs per SM
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int occ;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = per_sm.find(dev);
+        if (it == per_sm.end()) {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+            if (e != cudaSuccess) return e;
+            int b = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kThreads, smem);
+            if (e != cudaSuccess) return e;
+            per_sm[dev] = std::max(b, 1);
+            occ = std::max(b, 1);
+        } else {
+            occ = it->second;
+        }
+    }
+    const int g = (int)std::min<long>(std::max(M.nblk, 1), (long)occ * num_sms());
+    kern<<<g, kThreads, smem, s>>>(view(M), M.rb, M.nblk, x, epi, st, partials, fault);
+    return cudaGetLastError();
+}
+
+// Solver SpMV: CSR-stream over the matrix's row blocks, exact row order; staged (bulk
+// copies) or unstaged as the tuner chose. Both give the same bits.
 template <typename Epi>
 cudaError_t launch_spmv(const DevCsr &M, cudaStream_t s, const double *x, const Epi &epi, DState *st,
-                        double *partials) {
+                        double *partials, int *fault = nullptr) {
+    if (M.staged && fault) {
+        if (M.tile == 1024) return spmv_pipe<1024>(s, M, x, epi, st, partials, fault);
+        return spmv_pipe<2048>(s, M, x, epi, st, partials, fault);
+    }
     switch (M.tile) {
         case 1024: return spmv_rows<1024>(s, M, x, epi, st, partials);
         case 4096: return spmv_rows<4096>(s, M, x, epi, st, partials);
@@ -190,28 +226,40 @@ int set_tile(DevCsr &M, int tile, cudaStream_t s) {
 
 // Time each row-block size on this matrix and keep the fastest; cached by signature.
 // The choice changes speed only: every shape sums each row in storage order.
-static int autotune_tile(DevCsr &M, const double *x, double *y, cudaStream_t s) {
+static int autotune_tile(DevCsr &M, const double *x, double *y, cudaStream_t s, int *fault) {
     static std::mutex mu;
     static std::map<std::vector<long>, int> cache;
+    // FIIM_SPMV=rows or FIIM_SPMV=staged restricts the candidates to one form (tests use
+    // it to cover both; the results are the same bits either way).
+    const char *force = std::getenv("FIIM_SPMV");
+    const int only = !force ? 0 : (std::strcmp(force, "rows") == 0 ? 1 : (std::strcmp(force, "staged") == 0 ? 2 : 0));
+    std::vector<long> key = M.sig;
+    key.push_back(only);
     int cached = 0;
     {
         std::lock_guard<std::mutex> lk(mu);
-        auto it = cache.find(M.sig);
+        auto it = cache.find(key);
         if (it != cache.end()) cached = it->second;
     }
-    if (cached) return set_tile(M, cached, s);
-    const int cands[3] = {1024, 2048, 4096};
+    if (cached) {
+        M.staged = cached < 0;
+        return set_tile(M, cached < 0 ? -cached : cached, s);
+    }
+    // Candidates: unstaged TILE 1024 / 2048 / 4096, staged TILE 1024 / 2048 (negative).
+    const int cands[5] = {1024, 2048, 4096, -1024, -2048};
     cudaEvent_t e0, e1;
     FIIM_CUDA(cudaEventCreate(&e0));
     FIIM_CUDA(cudaEventCreate(&e1));
-    int best = 2048;
+    int best = only == 2 ? -2048 : 2048;
     float best_ms = 1e30f;
     const int reps = M.nnz > 4000000 ? 5 : 10;
     for (int c : cands) {
-        FIIM_TRY(set_tile(M, c, s));
-        FIIM_CUDA(launch_spmv(M, s, x, EpiStore{y}, nullptr, nullptr));
+        if ((only == 1 && c < 0) || (only == 2 && c > 0)) continue;
+        M.staged = c < 0;
+        FIIM_TRY(set_tile(M, c < 0 ? -c : c, s));
+        FIIM_CUDA(launch_spmv(M, s, x, EpiStore{y}, nullptr, nullptr, fault));
         FIIM_CUDA(cudaEventRecord(e0, s));
-        for (int r = 0; r < reps; ++r) FIIM_CUDA(launch_spmv(M, s, x, EpiStore{y}, nullptr, nullptr));
+        for (int r = 0; r < reps; ++r) FIIM_CUDA(launch_spmv(M, s, x, EpiStore{y}, nullptr, nullptr, fault));
         FIIM_CUDA(cudaEventRecord(e1, s));
         FIIM_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
@@ -225,9 +273,10 @@ static int autotune_tile(DevCsr &M, const double *x, double *y, cudaStream_t s) 
     cudaEventDestroy(e1);
     {
         std::lock_guard<std::mutex> lk(mu);
-        cache[M.sig] = best;
+        cache[key] = best;
     }
-    return set_tile(M, best, s);
+    M.staged = best < 0;
+    return set_tile(M, best < 0 ? -best : best, s);
 }
 
 // ------------------------------------------------------------------ host CSR helpers
@@ -382,27 +431,27 @@ int Solver::enqueue_prec(const double *in, double *out, bool norm) {
     const bool combined = (opt.variant == FIIM_ACIFIM && opt.mode == 'C' && opt.nr > 1);
     if (!combined) {
         // tm = IDv o (H in); out = G tm   (AFIIM/src/bicgstab.cpp:172-175)
-        FIIM_CUDA(launch_spmv(H, s, in, EpiScale{tm, IDv}, st, partials));
-        if (norm) FIIM_CUDA(launch_spmv(G, s, tm, EpiNorm{out}, st, partials));
-        else FIIM_CUDA(launch_spmv(G, s, tm, EpiStore{out}, st, partials));
+        FIIM_CUDA(launch_spmv(H, s, in, EpiScale{tm, IDv}, st, partials, fault));
+        if (norm) FIIM_CUDA(launch_spmv(G, s, tm, EpiNorm{out}, st, partials, fault));
+        else FIIM_CUDA(launch_spmv(G, s, tm, EpiStore{out}, st, partials, fault));
         return FIIM_OK;
     }
     // ACIFIM apply() mode 'C' (ACIFIM/src/bicgstab.cpp:395-404,408,411-420).
-    FIIM_CUDA(launch_spmv(H, s, in, EpiStore{t1}, st, partials));
+    FIIM_CUDA(launch_spmv(H, s, in, EpiStore{t1}, st, partials, fault));
     for (int it = 1; it < opt.nr; ++it) {
-        FIIM_CUDA(launch_spmv(L, s, t1, EpiSubFrom{t3, in}, st, partials));
+        FIIM_CUDA(launch_spmv(L, s, t1, EpiSubFrom{t3, in}, st, partials, fault));
         if (it == opt.nr - 1)
-            FIIM_CUDA(launch_spmv(H, s, t3, EpiAccumScale{t1, t2, IDv}, st, partials));
+            FIIM_CUDA(launch_spmv(H, s, t3, EpiAccumScale{t1, t2, IDv}, st, partials, fault));
         else
-            FIIM_CUDA(launch_spmv(H, s, t3, EpiAccum{t1}, st, partials));
+            FIIM_CUDA(launch_spmv(H, s, t3, EpiAccum{t1}, st, partials, fault));
     }
-    FIIM_CUDA(launch_spmv(G, s, t2, EpiStore{out}, st, partials));
+    FIIM_CUDA(launch_spmv(G, s, t2, EpiStore{out}, st, partials, fault));
     for (int it = 1; it < opt.nr; ++it) {
-        FIIM_CUDA(launch_spmv(U, s, out, EpiSubFrom{t3, t2}, st, partials));
+        FIIM_CUDA(launch_spmv(U, s, out, EpiSubFrom{t3, t2}, st, partials, fault));
         if (it == opt.nr - 1 && norm)
-            FIIM_CUDA(launch_spmv(G, s, t3, EpiAccumNorm{out}, st, partials));
+            FIIM_CUDA(launch_spmv(G, s, t3, EpiAccumNorm{out}, st, partials, fault));
         else
-            FIIM_CUDA(launch_spmv(G, s, t3, EpiAccum{out}, st, partials));
+            FIIM_CUDA(launch_spmv(G, s, t3, EpiAccum{out}, st, partials, fault));
     }
     return FIIM_OK;
 }
@@ -418,11 +467,11 @@ int Solver::enqueue_iteration(bool cond, cudaGraphConditionalHandle h) {
     cudaStream_t s = stream;
     const long nn = n;
     FIIM_TRY(enqueue_prec(p, pc, true));                                             // K1-K2
-    FIIM_CUDA(launch_spmv(A, s, pc, EpiAlpha{v, r0}, st, partials));     // K3
+    FIIM_CUDA(launch_spmv(A, s, pc, EpiAlpha{v, r0}, st, partials, fault));     // K3
     k_update_s<<<stream_grid(k_update_s, nn), kThreads, 0, s>>>(nn, r, v, x, sv, st, partials);  // K4
     FIIM_CUDA(cudaGetLastError());
     FIIM_TRY(enqueue_prec(sv, sc, false));                                           // K5-K6
-    FIIM_CUDA(launch_spmv(A, s, sc, EpiOmega{t, sv}, st, partials));    // K7
+    FIIM_CUDA(launch_spmv(A, s, sc, EpiOmega{t, sv}, st, partials, fault));    // K7
     k_update_xr<<<stream_grid(k_update_xr, nn), kThreads, 0, s>>>(nn, pc, sc, sv, t, r0, x, r, st,
                                                                   partials);          // K8
     FIIM_CUDA(cudaGetLastError());
@@ -597,10 +646,13 @@ int Solver::create(int n_, const int *Ai, const int *Aj, const double *Av, const
     st = static_cast<DState *>(arena.take(sizeof(DState)));
     partials = static_cast<double *>(arena.take(sizeof(double) * 4 * max_blocks));
     d_count = static_cast<unsigned long long *>(arena.take(sizeof(unsigned long long)));
-    if (!st || !partials || !d_count) return set_error(FIIM_ENOMEM, "arena exhausted");
+    fault = static_cast<int *>(arena.take(sizeof(int)));
+    if (!st || !partials || !d_count || !fault) return set_error(FIIM_ENOMEM, "arena exhausted");
     if (!hst) FIIM_CUDA(cudaHostAlloc(&hst, sizeof(DState) + 64, cudaHostAllocDefault));
     h_count = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(hst) + sizeof(DState) + 32);
+    h_fault = reinterpret_cast<int *>(reinterpret_cast<char *>(hst) + sizeof(DState) + 48);
     FIIM_CUDA(cudaMemsetAsync(st, 0, sizeof(DState), stream));
+    FIIM_CUDA(cudaMemsetAsync(fault, 0, sizeof(int), stream));
 
     FIIM_TRY(upload_csr(A, capA, n, aRp, aCi, aV, 0, a_dev, stream, d_count, h_count));
     FIIM_TRY(upload_csr(G, capG, n, Gi, Gj, Gv, 1, dev_src, stream, d_count, h_count));
@@ -618,7 +670,7 @@ int Solver::create(int n_, const int *Ai, const int *Aj, const double *Av, const
         DevCsr &M = *mats[k];
         if (opt.autotune) {
             FIIM_CUDA(cudaMemsetAsync(tm, 0, sizeof(double) * n, stream));
-            FIIM_TRY(autotune_tile(M, tm, t, stream));
+            FIIM_TRY(autotune_tile(M, tm, t, stream, fault));
         } else {
             FIIM_TRY(set_tile(M, 2048, stream));
         }
@@ -669,6 +721,7 @@ int Solver::solve(const double *b_in, double *x_io, double tol, int nmax, fiim_r
     const cudaMemcpyKind in_kind = dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     const cudaMemcpyKind out_kind = dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     FIIM_CUDA(cudaEventRecord(ev0, stream));
+    FIIM_CUDA(cudaMemsetAsync(fault, 0, sizeof(int), stream));
     FIIM_CUDA(cudaMemcpyAsync(b, b_in, sizeof(double) * n, in_kind, stream));
     FIIM_CUDA(cudaMemcpyAsync(x, x_io, sizeof(double) * n, in_kind, stream));
 
@@ -683,7 +736,7 @@ int Solver::solve(const double *b_in, double *x_io, double tol, int nmax, fiim_r
     *hst = h;
     FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
     // Start: r = b - A x, r0 = r, p = r, ro = ||r0|| (AFIIM/src/bicgstab.cpp:151-165).
-    FIIM_CUDA(launch_spmv(A, stream, x, EpiInit{b, p, r0, r}, st, partials));
+    FIIM_CUDA(launch_spmv(A, stream, x, EpiInit{b, p, r0, r}, st, partials, fault));
     int launches = 1;
     if (use_cond) {
         FIIM_CUDA(cudaGraphLaunch(exec, stream));
@@ -704,10 +757,11 @@ int Solver::solve(const double *b_in, double *x_io, double tol, int nmax, fiim_r
         hst->loops = launched;
     }
     // FP64 true residual ||b - A x|| / ||b||.
-    FIIM_CUDA(launch_spmv(A, stream, x, EpiResid{b, nullptr}, st, partials));
+    FIIM_CUDA(launch_spmv(A, stream, x, EpiResid{b, nullptr}, st, partials, fault));
     launches += 1;
     const int fallback_loops = hst->loops;
     FIIM_CUDA(cudaMemcpyAsync(hst, st, sizeof(DState), cudaMemcpyDeviceToHost, stream));
+    FIIM_CUDA(cudaMemcpyAsync(h_fault, fault, sizeof(int), cudaMemcpyDeviceToHost, stream));
     FIIM_CUDA(cudaMemcpyAsync(x_io, x, sizeof(double) * n, out_kind, stream));
     FIIM_CUDA(cudaEventRecord(ev1, stream));
     FIIM_CUDA(cudaStreamSynchronize(stream));
@@ -715,6 +769,7 @@ int Solver::solve(const double *b_in, double *x_io, double tol, int nmax, fiim_r
     float ms = 0.f;
     FIIM_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
     if (hst->info == -5) return set_error(FIIM_ETIMEOUT, "device loop guard tripped");
+    if (*h_fault) return set_error(FIIM_ETIMEOUT, "a staged SpMV's bulk copy did not complete in time");
     launches += hst->loops * kernels_per_iteration();
     last_launches = launches;
     if (res) {
@@ -775,7 +830,7 @@ int Solver::apply(int op, const double *in, double *out) {
     DState h = {};
     *hst = h;
     FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
-    if (op == 0) FIIM_CUDA(launch_spmv(A, stream, sv, EpiStore{t}, st, partials));
+    if (op == 0) FIIM_CUDA(launch_spmv(A, stream, sv, EpiStore{t}, st, partials, fault));
     else FIIM_TRY(enqueue_prec(sv, t, false));
     FIIM_CUDA(cudaMemcpyAsync(out, t, sizeof(double) * n,
                               dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream));
@@ -798,12 +853,12 @@ int Solver::kernel_times(int reps, int max_k, double *ms, double *bytes, char *n
     auto S = [&](const DevCsr &M) { return 12.0 * M.nnz + 4.0 * (M.n + 1); };
     const long nn = n;
     std::vector<Item> items = {
-        {"H_spmv_scale", S(H) + 3 * nv, [&] { return launch_spmv(H, stream, p, EpiScale{tm, IDv}, st, partials); }},
-        {"G_spmv_norm", S(G) + 2 * nv, [&] { return launch_spmv(G, stream, tm, EpiNorm{pc}, st, partials); }},
-        {"A_spmv_alpha", S(A) + 3 * nv, [&] { return launch_spmv(A, stream, pc, EpiAlpha{v, r0}, st, partials); }},
+        {"H_spmv_scale", S(H) + 3 * nv, [&] { return launch_spmv(H, stream, p, EpiScale{tm, IDv}, st, partials, fault); }},
+        {"G_spmv_norm", S(G) + 2 * nv, [&] { return launch_spmv(G, stream, tm, EpiNorm{pc}, st, partials, fault); }},
+        {"A_spmv_alpha", S(A) + 3 * nv, [&] { return launch_spmv(A, stream, pc, EpiAlpha{v, r0}, st, partials, fault); }},
         {"update_s", 4 * nv, [&] { k_update_s<<<stream_grid(k_update_s, nn), kThreads, 0, stream>>>(nn, r, v, x, sv, st, partials); return cudaGetLastError(); }},
-        {"G_spmv", S(G) + 2 * nv, [&] { return launch_spmv(G, stream, tm, EpiStore{sc}, st, partials); }},
-        {"A_spmv_omega", S(A) + 3 * nv, [&] { return launch_spmv(A, stream, sc, EpiOmega{t, sv}, st, partials); }},
+        {"G_spmv", S(G) + 2 * nv, [&] { return launch_spmv(G, stream, tm, EpiStore{sc}, st, partials, fault); }},
+        {"A_spmv_omega", S(A) + 3 * nv, [&] { return launch_spmv(A, stream, sc, EpiOmega{t, sv}, st, partials, fault); }},
         {"update_xr", 8 * nv, [&] { k_update_xr<<<stream_grid(k_update_xr, nn), kThreads, 0, stream>>>(nn, pc, sc, sv, t, r0, x, r, st, partials); return cudaGetLastError(); }},
         {"update_p", 4 * nv, [&] { k_update_p<<<stream_grid(k_update_p, nn), kThreads, 0, stream>>>(nn, r, v, p, st, cudaGraphConditionalHandle{}, 0); return cudaGetLastError(); }},
     };

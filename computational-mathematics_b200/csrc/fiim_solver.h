@@ -32,6 +32,8 @@ struct Solver : SolverBase {
     DState *hst = nullptr;       // pinned host mirror
     double *partials = nullptr;  // per-block reduction partials
     unsigned long long *d_count = nullptr, *h_count = nullptr;
+    int *h_fault = nullptr;
+    int *fault = nullptr;        // raised by a staged SpMV whose bulk copy did not complete
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool use_cond = false;       // the graph holds a device-driven WHILE loop

@@ -11,6 +11,9 @@ Every check goes through the C-ABI of libfiim_b200.so. Tolerances:
     solution within 10x the reference's own solution spread, and a true residual no
     worse than 10x the reference's.
 """
+import os
+import tempfile
+
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -67,8 +70,11 @@ def test_prec_apply_matches_oracle(golden, cuda, name, prefix):
     ("poisson128_afiim", "", "afiim", {}), ("convdiff16_pdfiim", "", "pdfiim", {}),
     ("convdiff2d48_acifim", "", "acifim", {"mode": "C", "nr": 2}), ("poisson32_sym_pdfiim", "", "pdfiim",
                                                                      {"issym": True})])
-def test_solver_products_bit_identical(golden, name, prefix, variant, kw):
-    """The solver's tuned CSR-stream kernels reproduce the oracle's A x and M x exactly."""
+@pytest.mark.parametrize("form", ["rows", "staged"])
+def test_solver_products_bit_identical(golden, monkeypatch, name, prefix, variant, kw, form):
+    """The solver's tuned CSR-stream kernels, unstaged and staged by bulk copies, reproduce
+    the oracle's A x and M x exactly."""
+    monkeypatch.setenv("FIIM_SPMV", form)
     g = golden(name)
     F = sub(g, prefix)
     S = FB.Solver((g["Ai"], g["Aj"], g["Av"]), F, variant=variant, **kw)
@@ -160,6 +166,31 @@ def test_dropin_solve_matches_reference(golden, name, fprefix, rprefix, variant,
         assert resval < 1e-8
     assert dx <= 10 * float(g[rprefix + "x_spread"]) + 1e-9
     assert true_relres(g, x) <= 10 * true_relres(g, g[rprefix + "x"]) + 1e-12
+
+
+@pytest.mark.parametrize("form", ["rows", "staged"])
+def test_solver_forms_agree_on_convdiff64(monkeypatch, form):
+    """A 64^3 solve takes the same iterations and (to rounding) the same x with either SpMV form."""
+    monkeypatch.setenv("FIIM_SPMV", form)
+    A = FB.gen_convdiff3d(64, 0.5)
+    b = FB.rand_normal(64 ** 3, 20261203)
+    F = FB.pdfiim_build(A, 0.05, 2, 2, 1, -1, "I", "B")
+    S = FB.Solver(A, F, variant="pdfiim")
+    x = np.zeros(64 ** 3)
+    r = S.solve(b, x, tol=1e-8, nmax=1200)
+    S.close()
+    # The products are the same bits in both forms; the fused dot products are summed in a
+    # launch-shape-dependent tree, so x may differ in its last bits.
+    ref = np.load(_forms_cache()) if os.path.exists(_forms_cache()) else None
+    if ref is None:
+        np.save(_forms_cache(), x)
+    else:
+        assert np.linalg.norm(ref - x) <= 1e-12 * np.linalg.norm(ref)
+    assert r["info"] == 0 and r["iter"] == 58
+
+
+def _forms_cache():
+    return os.path.join(tempfile.gettempdir(), f"fiim_forms_{os.getpid()}.npy")
 
 
 @pytest.mark.parametrize("memory", ["host", "device"])
