@@ -97,7 +97,7 @@ void fiim_options_default(fiim_options *o) {
     o->memory = FIIM_MEM_HOST;
     o->mode = 'E';
     o->nr = 1;
-    o->autotune = 1;
+    o->autotune = 0;
     o->inner_tol = 1e-5;
     o->inner_nmax = 1000;
     o->max_refine = 50;

@@ -224,6 +224,11 @@ int set_tile(DevCsr &M, int tile, cudaStream_t s) {
     return FIIM_OK;
 }
 
+// Row-block size used when timing-based tuning is off: smaller blocks for longer rows.
+static int default_tile(const DevCsr &M) {
+    return (M.n > 0 && (double)M.nnz / (double)M.n > 8.0) ? 1024 : 2048;
+}
+
 // Time each row-block size on this matrix and keep the fastest; cached by signature.
 // The choice changes speed only: every shape sums each row in storage order.
 static int autotune_tile(DevCsr &M, const double *x, double *y, cudaStream_t s, int *fault) {
@@ -672,7 +677,10 @@ int Solver::create(int n_, const int *Ai, const int *Aj, const double *Av, const
             FIIM_CUDA(cudaMemsetAsync(tm, 0, sizeof(double) * n, stream));
             FIIM_TRY(autotune_tile(M, tm, t, stream, fault));
         } else {
-            FIIM_TRY(set_tile(M, 2048, stream));
+            // Deterministic shape: the same launch shape, hence the same reduction trees and
+            // the same bits, in every process on the same GPU model.
+            M.staged = 0;
+            FIIM_TRY(set_tile(M, default_tile(M), stream));
         }
     }
     FIIM_TRY(build_graph());

@@ -158,7 +158,7 @@ class Solver:
     Arrays are numpy (memory='host') or torch CUDA tensors (memory='device')."""
 
     def __init__(self, A, F, variant="afiim", issym=False, precision="fp64", mode="E", nr=1,
-                 autotune=True, memory="host", verbose=0, inner_tol=1e-5, inner_nmax=1000, max_refine=50):
+                 autotune=False, memory="host", verbose=0, inner_tol=1e-5, inner_nmax=1000, max_refine=50):
         self._h = C.c_void_p(0)
         o = Options()
         lib().fiim_options_default(C.byref(o))

@@ -91,14 +91,16 @@ typedef struct {
     int memory;        /* FIIM_MEM_HOST or FIIM_MEM_DEVICE for every array argument        */
     char mode;         /* ACIFIM preconditioner mode: 'E' (default) or 'C'                 */
     int nr;            /* ACIFIM mode 'C' relaxation steps                                 */
-    int autotune;      /* 1: time candidate SpMV shapes at set-up and keep the fastest     */
+    int autotune;      /* 1: time candidate SpMV shapes at set-up and keep the fastest;    */
+                       /* 0 (default): a fixed shape, so results repeat bit for bit across */
+                       /* processes (the fused dot products' summation tree depends on it) */
     int verbose;       /* print the reference's termination messages                       */
     double inner_tol;  /* mixed: inner FP32 BiCGSTAB relative tolerance (default 1e-5)     */
     int inner_nmax;    /* mixed: inner iteration cap per refinement step (default 1000)    */
     int max_refine;    /* mixed: outer refinement steps cap (default 50)                   */
 } fiim_options;
 
-/* Defaults: FIIM_AFIIM, FP64, host memory, mode 'E', nr 1, autotune 1. */
+/* Defaults: FIIM_AFIIM, FP64, host memory, mode 'E', nr 1, autotune 0. */
 void fiim_options_default(fiim_options *opt);
 
 typedef struct {
