@@ -1,0 +1,336 @@
+// Multi-RHS block solve: k <= 32 right-hand sides of one system in one device-driven
+// loop. Each right-hand side runs the reference's BiCGSTAB with its own scalars,
+// divergence window and termination; the sparse products are shared (SpMM over n x k
+// row-major vectors), so the matrix streams are read once per product for all k.
+//
+// Layout: A, G, H CSR (int32 indices; A values FP64, G/H values FP64 or FP32 per
+// fiim_options.precision, widened before each rounded product); D^-1 FP64[n]; the 11
+// solver vectors FP64[n x k]; per-RHS state (k entries); per-CTA partials (32 per value).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "fiim_b200.h"
+#include "fiim_block.cuh"
+#include "fiim_internal.h"
+#include "fiim_kernels.cuh"
+#include "fiim_solver.h"
+
+namespace fiim {
+
+struct BlockSolver {
+    int device = -1, n = 0, k = 0, kp = 32;
+    fiim_options opt{};
+    cudaStream_t stream = nullptr;
+    Arena arena;
+    DevCsr A, G, H;
+    float *G32 = nullptr, *H32 = nullptr;
+    double *IDv = nullptr, *x = nullptr, *b = nullptr, *r = nullptr, *r0 = nullptr, *p = nullptr;
+    double *v = nullptr, *sv = nullptr, *t = nullptr, *pc = nullptr, *sc = nullptr, *tm = nullptr;
+    double *partials = nullptr;
+    bt::BState bs{};
+    bt::BGlobal *hg = nullptr;
+    unsigned long long *d_count = nullptr, *h_count = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    bk::Shape shape() const { return bk::Shape{n, k}; }
+
+    template <int KP, typename V, typename Epi>
+    cudaError_t spmm_kp(const DevCsr &M, const V *vals, const double *X, const Epi &epi) {
+        auto kern = bk::k_spmm<KP, V, Epi>;
+        const int g = grid_for(kern, (long)kWarps * (32 / KP), n);
+        kern<<<g, kThreads, 0, stream>>>(CsrView<V>{M.rp, M.ci, vals, n}, shape(), X, epi, bs, partials);
+        return cudaGetLastError();
+    }
+    template <typename V, typename Epi>
+    cudaError_t spmm(const DevCsr &M, const V *vals, const double *X, const Epi &epi) {
+        switch (kp) {
+            case 4: return spmm_kp<4>(M, vals, X, epi);
+            case 8: return spmm_kp<8>(M, vals, X, epi);
+            case 16: return spmm_kp<16>(M, vals, X, epi);
+            default: return spmm_kp<32>(M, vals, X, epi);
+        }
+    }
+    template <typename Epi>
+    cudaError_t spmm_f(const DevCsr &M, const float *v32, const double *X, const Epi &epi) {
+        if (opt.precision == FIIM_MIXED_FP32) return spmm(M, v32, X, epi);
+        return spmm(M, M.v, X, epi);
+    }
+
+    template <int KP>
+    int updates_kp(int which, bool cond, cudaGraphConditionalHandle h) {
+        const long rows = (long)kWarps * (32 / KP);
+        if (which == 0) {
+            auto kern = bk::k_kupdate_s<KP>;
+            kern<<<grid_for(kern, rows, n), kThreads, 0, stream>>>(shape(), r, v, x, sv, bs, partials);
+        } else if (which == 1) {
+            auto kern = bk::k_kupdate_xr<KP>;
+            kern<<<grid_for(kern, rows, n), kThreads, 0, stream>>>(shape(), pc, sc, sv, t, r0, x, r, bs, partials);
+        } else {
+            auto kern = bk::k_kupdate_p<KP>;
+            kern<<<grid_for(kern, rows, n), kThreads, 0, stream>>>(shape(), r, v, p, bs, h, cond ? 1 : 0);
+        }
+        FIIM_CUDA(cudaGetLastError());
+        return FIIM_OK;
+    }
+    int updates(int which, bool cond, cudaGraphConditionalHandle h) {
+        switch (kp) {
+            case 4: return updates_kp<4>(which, cond, h);
+            case 8: return updates_kp<8>(which, cond, h);
+            case 16: return updates_kp<16>(which, cond, h);
+            default: return updates_kp<32>(which, cond, h);
+        }
+    }
+
+    int enqueue_iteration(bool cond, cudaGraphConditionalHandle h) {
+        FIIM_CUDA(spmm_f(H, H32, p, bk::KEpiScale{tm, IDv, k}));
+        FIIM_CUDA(spmm_f(G, G32, tm, bk::KEpiNorm{pc}));
+        FIIM_CUDA(spmm(A, A.v, pc, bk::KEpiAlpha{v, r0}));
+        FIIM_TRY(updates(0, cond, h));
+        FIIM_CUDA(spmm_f(H, H32, sv, bk::KEpiScale{tm, IDv, k}));
+        FIIM_CUDA(spmm_f(G, G32, tm, bk::KEpiStore{sc}));
+        FIIM_CUDA(spmm(A, A.v, sc, bk::KEpiOmega{t, sv}));
+        FIIM_TRY(updates(1, cond, h));
+        FIIM_TRY(updates(2, cond, h));
+        return FIIM_OK;
+    }
+
+    int reset_state(double tol, int nmax, int active) {
+        bt::BGlobal g = {};
+        g.tol = tol;
+        g.eps = 1.11022302462516e-16;
+        g.nmax = nmax;
+        g.alpha_guard = (opt.variant == FIIM_ACIFIM);
+        g.active = active;
+        *hg = g;
+        FIIM_CUDA(cudaMemcpyAsync(bs.g, hg, sizeof(bt::BGlobal), cudaMemcpyHostToDevice, stream));
+        FIIM_CUDA(cudaMemsetAsync(bs.done, 0, sizeof(int) * 32, stream));
+        FIIM_CUDA(cudaMemsetAsync(bs.info, 0xff, sizeof(int) * 32, stream));
+        FIIM_CUDA(cudaMemsetAsync(bs.ticket, 0, sizeof(unsigned int) * 32, stream));
+        return FIIM_OK;
+    }
+
+    int build_graph() {
+        FIIM_TRY(reset_state(0.0, 0, 0));   // active = 0: every kernel returns at once
+        FIIM_TRY(enqueue_iteration(false, cudaGraphConditionalHandle{}));
+        FIIM_CUDA(cudaStreamSynchronize(stream));
+        cudaGraph_t g = nullptr;
+        FIIM_CUDA(cudaGraphCreate(&g, 0));
+        cudaGraphConditionalHandle h;
+        FIIM_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        FIIM_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        FIIM_CUDA(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue_iteration(true, h);
+        cudaGraph_t captured = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(stream, &captured);
+        if (rc != FIIM_OK) return rc;
+        FIIM_CUDA(ec);
+        FIIM_CUDA(cudaGraphInstantiate(&exec, g, 0));
+        graph = g;
+        return FIIM_OK;
+    }
+
+    int create(int n_, int k_, const int *Ai, const int *Aj, const double *Av, const int *Gi, const int *Gj,
+               const double *Gv, const double *IDv_, const int *Hi, const int *Hj, const double *Hv,
+               const fiim_options &o) {
+        opt = o;
+        n = n_;
+        k = k_;
+        if (n <= 0 || k <= 0 || k > 32) return set_error(FIIM_EARG, "need n > 0 and 1 <= nrhs <= 32");
+        if (!Ai || !Aj || !Av || !Gi || !Gj || !Gv || !IDv_ || !Hi || !Hj || !Hv)
+            return set_error(FIIM_EARG, "block solve needs A, G, IDv and H");
+        if (opt.issym) return set_error(FIIM_EARG, "block solve takes general (non-symmetric-storage) input");
+        if (opt.variant == FIIM_ACIFIM && opt.mode != 'E')
+            return set_error(FIIM_EARG, "block solve applies the explicit product (mode 'E')");
+        if (opt.precision == FIIM_MIXED_BF16) return set_error(FIIM_EARG, "block solve stores factors in FP64 or FP32");
+        kp = 4;
+        while (kp < k) kp <<= 1;
+        FIIM_TRY(check_device(&device));
+        FIIM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        FIIM_CUDA(cudaEventCreate(&ev0));
+        FIIM_CUDA(cudaEventCreate(&ev1));
+        const bool dev = (opt.memory == FIIM_MEM_DEVICE);
+        auto nnz_of = [&](const int *rp) -> long {
+            if (!dev) return rp[n];
+            int z = 0;
+            if (cudaMemcpy(&z, rp + n, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+            return z;
+        };
+        const long nA = nnz_of(Ai), nG = nnz_of(Gi), nH = nnz_of(Hi);
+        if (nA < 0 || nG < 0 || nH < 0) return set_error(FIIM_ECUDA, "reading row offsets failed");
+        const bool f32 = (opt.precision == FIIM_MIXED_FP32);
+        const long nk = (long)n * k;
+        const int max_blocks = num_sms() * 32;
+        size_t bytes = csr_bytes(n, nA) + csr_bytes(n, nG) + csr_bytes(n, nH);
+        if (f32) bytes += Arena::need(4 * std::max<long>(nG, 1)) + Arena::need(4 * std::max<long>(nH, 1));
+        bytes += Arena::need(sizeof(double) * n) + 11 * Arena::need(sizeof(double) * nk);
+        bytes += Arena::need(sizeof(double) * 2 * 32 * max_blocks);
+        bytes += 12 * Arena::need(sizeof(double) * 32) + 7 * Arena::need(sizeof(int) * 32);
+        bytes += Arena::need(sizeof(bt::BGlobal)) + 4096;
+        FIIM_TRY(arena.reserve(bytes));
+        FIIM_TRY(carve_csr(arena, A, n, nA));
+        FIIM_TRY(carve_csr(arena, G, n, nG));
+        FIIM_TRY(carve_csr(arena, H, n, nH));
+        if (f32) {
+            G32 = static_cast<float *>(arena.take(4 * std::max<long>(nG, 1)));
+            H32 = static_cast<float *>(arena.take(4 * std::max<long>(nH, 1)));
+            if (!G32 || !H32) return set_error(FIIM_ENOMEM, "arena exhausted");
+        }
+        if (!(IDv = static_cast<double *>(arena.take(sizeof(double) * n)))) return set_error(FIIM_ENOMEM, "arena");
+        double **vecs[] = {&x, &b, &r, &r0, &p, &v, &sv, &t, &pc, &sc, &tm};
+        for (auto pp : vecs)
+            if (!(*pp = static_cast<double *>(arena.take(sizeof(double) * nk)))) return set_error(FIIM_ENOMEM, "arena");
+        partials = static_cast<double *>(arena.take(sizeof(double) * 2 * 32 * max_blocks));
+        double **ds[] = {&bs.ro, &bs.rc, &bs.m1, &bs.m2, &bs.alpha, &bs.omega, &bs.beta, &bs.pc2, &bs.x2, &bs.r2,
+                         &bs.ts, &bs.tt};
+        for (auto pp : ds)
+            if (!(*pp = static_cast<double *>(arena.take(sizeof(double) * 32)))) return set_error(FIIM_ENOMEM, "arena");
+        int **is[] = {&bs.iter, &bs.stag, &bs.msteps, &bs.maxmsteps, &bs.info, &bs.done};
+        for (auto pp : is)
+            if (!(*pp = static_cast<int *>(arena.take(sizeof(int) * 32)))) return set_error(FIIM_ENOMEM, "arena");
+        bs.ticket = static_cast<unsigned int *>(arena.take(sizeof(unsigned int) * 32));
+        bs.g = static_cast<bt::BGlobal *>(arena.take(sizeof(bt::BGlobal)));
+        d_count = static_cast<unsigned long long *>(arena.take(sizeof(unsigned long long)));
+        if (!partials || !bs.ticket || !bs.g || !d_count) return set_error(FIIM_ENOMEM, "arena exhausted");
+        FIIM_CUDA(cudaHostAlloc(&hg, sizeof(bt::BGlobal) + 64, cudaHostAllocDefault));
+        h_count = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(hg) + sizeof(bt::BGlobal) + 32);
+        FIIM_TRY(upload_csr(A, nA, n, Ai, Aj, Av, 0, dev, stream, d_count, h_count));
+        FIIM_TRY(upload_csr(G, nG, n, Gi, Gj, Gv, 1, dev, stream, d_count, h_count));
+        FIIM_TRY(upload_csr(H, nH, n, Hi, Hj, Hv, 2, dev, stream, d_count, h_count));
+        FIIM_CUDA(cudaMemcpyAsync(IDv, IDv_, sizeof(double) * n, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                  stream));
+        if (f32) {
+            if (G.nnz > 0)
+                bt::k_vals_to_f32<<<grid_for(bt::k_vals_to_f32, kThreads, G.nnz), kThreads, 0, stream>>>(G.nnz, G.v, G32);
+            if (H.nnz > 0)
+                bt::k_vals_to_f32<<<grid_for(bt::k_vals_to_f32, kThreads, H.nnz), kThreads, 0, stream>>>(H.nnz, H.v, H32);
+            FIIM_CUDA(cudaGetLastError());
+        }
+        const int mm = (opt.variant == FIIM_ACIFIM) ? std::min(std::max(n, 2000) / 50, 40)
+                                                    : std::min(std::max(n, 500) / 50, 20);
+        std::vector<int> mmv(32, mm);
+        FIIM_CUDA(cudaMemcpyAsync(bs.maxmsteps, mmv.data(), sizeof(int) * 32, cudaMemcpyHostToDevice, stream));
+        FIIM_CUDA(cudaStreamSynchronize(stream));
+        return build_graph();
+    }
+
+    int solve(const double *B, double *X, double tol, int nmax, int *iter, int *info, double *resval,
+              double *true_relres, fiim_result *summary) {
+        FIIM_CUDA(cudaSetDevice(device));
+        const bool dev = (opt.memory == FIIM_MEM_DEVICE);
+        const size_t bytes = sizeof(double) * (size_t)n * k;
+        FIIM_CUDA(cudaEventRecord(ev0, stream));
+        FIIM_CUDA(cudaMemcpyAsync(b, B, bytes, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
+        FIIM_CUDA(cudaMemcpyAsync(x, X, bytes, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
+        FIIM_TRY(reset_state(tol, nmax, k));
+        FIIM_CUDA(spmm(A, A.v, x, bk::KEpiInit{b, p, r0, r}));
+        FIIM_CUDA(cudaGraphLaunch(exec, stream));
+        FIIM_CUDA(spmm(A, A.v, x, bk::KEpiResid{b}));
+        FIIM_CUDA(cudaMemcpyAsync(X, x, bytes, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream));
+        FIIM_CUDA(cudaEventRecord(ev1, stream));
+        int hit[32], hinfo[32];
+        double hrc[32], hro[32], hts[32], htt[32];
+        FIIM_CUDA(cudaMemcpyAsync(hit, bs.iter, sizeof(int) * 32, cudaMemcpyDeviceToHost, stream));
+        FIIM_CUDA(cudaMemcpyAsync(hinfo, bs.info, sizeof(int) * 32, cudaMemcpyDeviceToHost, stream));
+        FIIM_CUDA(cudaMemcpyAsync(hrc, bs.rc, sizeof(double) * 32, cudaMemcpyDeviceToHost, stream));
+        FIIM_CUDA(cudaMemcpyAsync(hro, bs.ro, sizeof(double) * 32, cudaMemcpyDeviceToHost, stream));
+        FIIM_CUDA(cudaMemcpyAsync(hts, bs.ts, sizeof(double) * 32, cudaMemcpyDeviceToHost, stream));
+        FIIM_CUDA(cudaMemcpyAsync(htt, bs.tt, sizeof(double) * 32, cudaMemcpyDeviceToHost, stream));
+        FIIM_CUDA(cudaMemcpyAsync(hg, bs.g, sizeof(bt::BGlobal), cudaMemcpyDeviceToHost, stream));
+        FIIM_CUDA(cudaStreamSynchronize(stream));
+        if (hg->active < 0) return set_error(FIIM_ETIMEOUT, "device loop guard tripped");
+        float ms = 0.f;
+        FIIM_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        int maxit = 0, worst = 0;
+        double worst_rel = 0.0;
+        for (int j = 0; j < k; ++j) {
+            if (iter) iter[j] = hit[j];
+            if (info) info[j] = hinfo[j];
+            if (resval) resval[j] = hrc[j] / hro[j];
+            const double tr = std::sqrt(hts[j]) / std::sqrt(htt[j]);
+            if (true_relres) true_relres[j] = tr;
+            maxit = std::max(maxit, hit[j]);
+            worst = std::max(worst, hinfo[j]);
+            worst_rel = std::max(worst_rel, tr);
+        }
+        if (summary) {
+            summary->iter = maxit;
+            summary->info = worst;
+            summary->resval = 0.0;
+            summary->true_relres = worst_rel;
+            summary->refine_steps = 0;
+            summary->device_ms = ms;
+            summary->launches = 2 + hg->loops * 9;
+        }
+        return FIIM_OK;
+    }
+
+    void destroy() {
+        if (device >= 0) cudaSetDevice(device);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+        if (hg) cudaFreeHost(hg);
+        exec = nullptr;
+        graph = nullptr;
+        ev0 = ev1 = nullptr;
+        stream = nullptr;
+        hg = nullptr;
+        arena.release();
+    }
+};
+
+}  // namespace fiim
+
+extern "C" {
+
+int fiim_block_create(fiim_block_t *out, int n, int nrhs, const int *Ai, const int *Aj, const double *Av,
+                      const int *Gi, const int *Gj, const double *Gv, const double *IDv, const int *Hi,
+                      const int *Hj, const double *Hv, const fiim_options *opt) {
+    if (!out) return fiim::set_error(FIIM_EARG, "out is NULL");
+    *out = nullptr;
+    fiim_options o;
+    if (opt) o = *opt;
+    else fiim_options_default(&o);
+    auto *s = new fiim::BlockSolver;
+    const int rc = s->create(n, nrhs, Ai, Aj, Av, Gi, Gj, Gv, IDv, Hi, Hj, Hv, o);
+    if (rc != FIIM_OK) {
+        s->destroy();
+        delete s;
+        return rc;
+    }
+    *out = reinterpret_cast<fiim_block_t>(s);
+    return FIIM_OK;
+}
+
+int fiim_block_solve(fiim_block_t h, const double *B, double *X, double tol, int NMAX, int *iter, int *info,
+                     double *resval, double *true_relres, fiim_result *summary) {
+    if (!h || !B || !X) return fiim::set_error(FIIM_EARG, "null argument");
+    return reinterpret_cast<fiim::BlockSolver *>(h)->solve(B, X, tol, NMAX, iter, info, resval, true_relres,
+                                                             summary);
+}
+
+int fiim_block_destroy(fiim_block_t h) {
+    if (!h) return FIIM_OK;
+    auto *s = reinterpret_cast<fiim::BlockSolver *>(h);
+    s->destroy();
+    delete s;
+    return FIIM_OK;
+}
+
+}  // extern "C"

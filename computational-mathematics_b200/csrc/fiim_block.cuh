@@ -1,0 +1,274 @@
+// Device kernels of the multi-RHS block solve: k <= 32 right-hand sides of one system,
+// each running the reference's BiCGSTAB (AFIIM/src/bicgstab.cpp:168-275) with its own
+// scalars and termination, sharing every sparse product.
+//
+// Vectors are n x k, row-major (entry (i, j) at i*k + j), so the k values a gathered
+// column index needs are contiguous. Work mapping shared by all kernels: a lane group of
+// KP = next power of two >= k lanes takes one row, lane j of the group owns right-hand side
+// j; a warp holds 32/KP row groups; warps walk rows in grid-stride order.
+// Sparse products: the group loads the row's entries KP at a time (coalesced) and
+// broadcasts them lane by lane, so each right-hand side's row sum is formed left to right
+// in storage order with rounded products (the reference's arithmetic, bit for bit).
+// Reductions are per right-hand side: lanes of equal j are combined within the warp and
+// the CTA in a fixed tree, the CTA writes k partials, and the last CTA (ticket) adds them
+// in CTA order and runs each right-hand side's scalar step.
+#pragma once
+
+#include "fiim_batch.cuh"
+#include "fiim_kernels.cuh"
+
+namespace fiim {
+namespace bk {
+
+using bt::BState;
+
+struct Shape {
+    long n;
+    int k;        // right-hand sides
+};
+
+// Per-RHS reduction over the CTA and the grid; every thread calls it (uniformly).
+template <int KP, int NR, class Fin>
+__device__ __forceinline__ void rhs_reduce(double (&v)[NR], int k, double *__restrict__ partials, BState &bs,
+                                           const Fin &fin) {
+    __shared__ double sm[kWarps][32][NR];
+    __shared__ int last;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    // combine the row groups of the warp (lanes with the same j)
+#pragma unroll
+    for (int j = 0; j < NR; ++j)
+#pragma unroll
+        for (int o = KP; o < 32; o <<= 1) v[j] += __shfl_xor_sync(0xffffffffu, v[j], o);
+    if (lane < KP)
+#pragma unroll
+        for (int j = 0; j < NR; ++j) sm[w][lane][j] = v[j];
+    __syncthreads();
+    if (threadIdx.x < k) {
+        const int jj = threadIdx.x;
+#pragma unroll
+        for (int j = 0; j < NR; ++j) {
+            double s = 0.0;
+#pragma unroll
+            for (int q = 0; q < kWarps; ++q) s += sm[q][jj][j];
+            partials[((size_t)blockIdx.x * 32 + jj) * NR + j] = s;
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned t = atomicAdd(bs.ticket, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    if (threadIdx.x < k) {
+        const int jj = threadIdx.x;
+        double tot[NR];
+#pragma unroll
+        for (int j = 0; j < NR; ++j) tot[j] = 0.0;
+        for (int c = 0; c < (int)gridDim.x; ++c)
+#pragma unroll
+            for (int j = 0; j < NR; ++j) tot[j] += __ldcg(partials + ((size_t)c * 32 + jj) * NR + j);
+        if (!bs.done[jj] || !Fin::GATED) fin.finish(bs, jj, tot);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *bs.ticket = 0u;
+}
+
+// Row groups of the calling thread: (first row, stride) and its lane in the group.
+#define FIIM_ROW_GROUPS(KP, row)                                                              \
+    const int lane_ = threadIdx.x & 31, j_ = lane_ % (KP), grp_ = lane_ / (KP);               \
+    const long gw_ = ((long)blockIdx.x * kThreads + threadIdx.x) >> 5;                        \
+    const long nw_ = ((long)gridDim.x * kThreads) >> 5;                                       \
+    for (long row = gw_ * (32 / (KP)) + grp_, base_ = gw_ * (32 / (KP));                      \
+         base_ < sh.n; base_ += nw_ * (32 / (KP)), row = base_ + grp_)
+
+// ---------------------------------------------------------------- epilogues
+#define FIIM_BEPI(nr, reduces, gated)            \
+    static constexpr int NR = nr;                \
+    static constexpr bool REDUCES = reduces;     \
+    static constexpr bool GATED = gated
+
+struct KEpiStore {
+    FIIM_BEPI(1, false, true);
+    double *y;
+    __device__ void emit(size_t at, double s, double (&)[NR]) const { y[at] = s; }
+    __device__ void finish(BState &, int, const double *) const {}
+};
+struct KEpiScale {                 // y = d o (M x), d per row
+    FIIM_BEPI(1, false, true);
+    double *y;
+    const double *__restrict__ d;
+    int k;
+    __device__ void emit(size_t at, double s, double (&)[NR]) const { y[at] = __dmul_rn(__ldg(d + at / k), s); }
+    __device__ void finish(BState &, int, const double *) const {}
+};
+struct KEpiNorm {
+    FIIM_BEPI(1, true, true);
+    double *y;
+    __device__ void emit(size_t at, double s, double (&r)[NR]) const { y[at] = s; r[0] += s * s; }
+    __device__ void finish(BState &bs, int j, const double *t) const { bs.pc2[j] = t[0]; }
+};
+struct KEpiAlpha {
+    FIIM_BEPI(1, true, true);
+    double *y;
+    const double *__restrict__ r0;
+    __device__ void emit(size_t at, double s, double (&r)[NR]) const {
+        y[at] = s;
+        r[0] += __ldg(r0 + at) * s;
+    }
+    __device__ void finish(BState &bs, int j, const double *t) const { bt::BEpiAlpha{}.finish(bs, j, t); }
+};
+struct KEpiOmega {
+    FIIM_BEPI(2, true, true);
+    double *y;
+    const double *__restrict__ sv;
+    __device__ void emit(size_t at, double s, double (&r)[NR]) const {
+        y[at] = s;
+        r[0] += s * __ldg(sv + at);
+        r[1] += s * s;
+    }
+    __device__ void finish(BState &bs, int j, const double *t) const { bs.omega[j] = t[0] / t[1]; }
+};
+struct KEpiInit {
+    FIIM_BEPI(1, true, true);
+    const double *__restrict__ b;
+    double *p, *r0, *r;
+    __device__ void emit(size_t at, double s, double (&red)[NR]) const {
+        const double pi = __dadd_rn(b[at], __dmul_rn(-1.0, s));
+        p[at] = pi;
+        r0[at] = pi;
+        r[at] = pi;
+        red[0] += pi * pi;
+    }
+    __device__ void finish(BState &bs, int j, const double *t) const { bt::BFinInit{}.finish(bs, j, t); }
+};
+struct KEpiResid {
+    FIIM_BEPI(2, true, false);
+    const double *__restrict__ b;
+    __device__ void emit(size_t at, double s, double (&red)[NR]) const {
+        const double bi = b[at], ri = bi - s;
+        red[0] += ri * ri;
+        red[1] += bi * bi;
+    }
+    __device__ void finish(BState &bs, int j, const double *t) const {
+        bs.ts[j] = t[0];
+        bs.tt[j] = t[1];
+    }
+};
+
+__device__ __forceinline__ double wide(double v) { return v; }
+__device__ __forceinline__ double wide(float v) { return (double)v; }
+
+// ---------------------------------------------------------------- SpMM
+template <int KP, typename V, typename Epi>
+static __global__ void __launch_bounds__(kThreads)
+k_spmm(CsrView<V> M, Shape sh, const double *__restrict__ X, Epi epi, BState bs, double *__restrict__ partials) {
+    if (Epi::GATED && bs.g->active <= 0) return;
+    double red[Epi::NR];
+#pragma unroll
+    for (int q = 0; q < Epi::NR; ++q) red[q] = 0.0;
+    const unsigned gmask = (KP == 32) ? 0xffffffffu : (((1u << KP) - 1u) << ((threadIdx.x & 31) / KP * KP));
+    (void)gmask;
+    FIIM_ROW_GROUPS(KP, row) {
+        const bool live = row < sh.n;
+        int beg = 0, len = 0;
+        if (live) {
+            beg = __ldg(M.rp + row);
+            len = __ldg(M.rp + row + 1) - beg;
+        }
+        // every group of the warp walks the longest row of the warp (uniform shuffles)
+        const int trips = __reduce_max_sync(0xffffffffu, (len + KP - 1) / KP);
+        double s = 0.0;
+        for (int t = 0; t < trips; ++t) {
+            const int q = t * KP + j_;
+            int c = 0;
+            double a = 0.0;
+            if (q < len) {
+                c = ldi(M.ci + beg + q);
+                a = wide(ldm(M.v + beg + q));
+            }
+#pragma unroll 8
+            for (int e = 0; e < KP; ++e) {
+                const int ce = __shfl_sync(0xffffffffu, c, grp_ * KP + e);
+                const double ae = __shfl_sync(0xffffffffu, a, grp_ * KP + e);
+                if (t * KP + e < len && j_ < sh.k)
+                    s = __dadd_rn(s, __dmul_rn(ae, __ldg(X + (size_t)ce * sh.k + j_)));
+            }
+        }
+        if (live && j_ < sh.k && !(Epi::GATED && bs.done[j_])) epi.emit((size_t)row * sh.k + j_, s, red);
+    }
+    if constexpr (Epi::REDUCES) rhs_reduce<KP, Epi::NR>(red, sh.k, partials, bs, epi);
+}
+
+// ---------------------------------------------------------------- updates (n x k)
+struct KFinS {
+    static constexpr bool GATED = true;
+    __device__ void finish(BState &bs, int j, const double *t) const { bt::BFinS{}.finish(bs, j, t); }
+};
+struct KFinControl {
+    static constexpr bool GATED = true;
+    __device__ void finish(BState &bs, int j, const double *t) const { bt::BFinControl{}.finish(bs, j, t); }
+};
+
+template <int KP>
+static __global__ void __launch_bounds__(kThreads)
+k_kupdate_s(Shape sh, const double *__restrict__ r, const double *__restrict__ v, const double *__restrict__ x,
+            double *__restrict__ s, BState bs, double *__restrict__ partials) {
+    if (bs.g->active <= 0) return;
+    double red[2] = {0.0, 0.0};
+    FIIM_ROW_GROUPS(KP, row) {
+        if (row >= sh.n || j_ >= sh.k || bs.done[j_]) continue;
+        const size_t at = (size_t)row * sh.k + j_;
+        const double ri = r[at], xi = x[at];
+        s[at] = __dadd_rn(ri, __dmul_rn(-bs.alpha[j_], v[at]));
+        red[0] += ri * ri;
+        red[1] += xi * xi;
+    }
+    rhs_reduce<KP, 2>(red, sh.k, partials, bs, KFinS{});
+}
+
+template <int KP>
+static __global__ void __launch_bounds__(kThreads)
+k_kupdate_xr(Shape sh, const double *__restrict__ pc, const double *__restrict__ sc, const double *__restrict__ s,
+             const double *__restrict__ t, const double *__restrict__ r0, double *__restrict__ x,
+             double *__restrict__ r, BState bs, double *__restrict__ partials) {
+    if (bs.g->active <= 0) return;
+    double red[1] = {0.0};
+    FIIM_ROW_GROUPS(KP, row) {
+        if (row >= sh.n || j_ >= sh.k || bs.done[j_]) continue;
+        const size_t at = (size_t)row * sh.k + j_;
+        const double a = bs.alpha[j_], om = bs.omega[j_];
+        double xi = x[at];
+        xi = __dadd_rn(xi, __dmul_rn(a, pc[at]));
+        xi = __dadd_rn(xi, __dmul_rn(om, sc[at]));
+        x[at] = xi;
+        const double ri = __dadd_rn(s[at], __dmul_rn(-om, t[at]));
+        r[at] = ri;
+        red[0] += r0[at] * ri;
+    }
+    rhs_reduce<KP, 1>(red, sh.k, partials, bs, KFinControl{});
+}
+
+template <int KP>
+static __global__ void __launch_bounds__(kThreads)
+k_kupdate_p(Shape sh, const double *__restrict__ r, const double *__restrict__ v, double *__restrict__ p, BState bs,
+            cudaGraphConditionalHandle h, int cond) {
+    if (cond && blockIdx.x == 0 && threadIdx.x == 0) {
+        const int loops = ++bs.g->loops;
+        if (bs.g->active > 0 && loops > bs.g->nmax + 2) bs.g->active = -1;
+        cudaGraphSetConditional(h, bs.g->active > 0 ? 1u : 0u);
+    }
+    if (bs.g->active <= 0) return;
+    FIIM_ROW_GROUPS(KP, row) {
+        if (row >= sh.n || j_ >= sh.k || bs.done[j_]) continue;
+        const size_t at = (size_t)row * sh.k + j_;
+        const double b = bs.beta[j_], c = __dmul_rn(-bs.beta[j_], bs.omega[j_]);
+        const double pi = __dadd_rn(__dmul_rn(c, v[at]), __dmul_rn(b, p[at]));
+        p[at] = __dadd_rn(pi, r[at]);
+    }
+}
+
+}  // namespace bk
+}  // namespace fiim

@@ -39,6 +39,7 @@ EXPORTS = (
     "fiim_PBiCGSTAB_acifim", "fiim_solver_create", "fiim_solver_solve", "fiim_solver_device_bytes",
     "fiim_solver_spmv_shape", "fiim_solver_apply", "fiim_solver_kernel_times", "fiim_solver_iteration_bytes",
     "fiim_solver_destroy", "fiim_batch_create", "fiim_batch_solve", "fiim_batch_destroy",
+    "fiim_block_create", "fiim_block_solve", "fiim_block_destroy",
     "fiim_spmv", "fiim_prec_apply", "fiim_prec_apply_noalloc",
     "fiim_gen_poisson2d", "fiim_gen_convdiff3d", "fiim_gen_convdiff2d", "fiim_gen_batch_params",
     "fiim_gen_zipf", "fiim_gen_zipf_mean", "fiim_rand_normal", "fiim_model_rhs", "fiim_pdfiim_build",
@@ -294,6 +295,48 @@ class BatchSolver:
     def close(self):
         if self._h and self._h.value:
             lib().fiim_batch_destroy(self._h)
+            self._h = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BlockSolver:
+    """k <= 32 right-hand sides of one system, sharing the sparse products (fiim_block_*).
+    B, X: n x k row-major FP64 (numpy, or torch CUDA tensors with memory='device')."""
+
+    def __init__(self, A, F, nrhs, variant="afiim", precision="fp64", memory="host"):
+        o = Options()
+        lib().fiim_options_default(C.byref(o))
+        o.variant = _VARIANTS[variant]
+        o.precision = _PRECISIONS[precision]
+        o.memory = MEM_DEVICE if memory == "device" else MEM_HOST
+        self.memory, self.k, self.n = memory, nrhs, len(A[0]) - 1
+        conv = (lambda a, ints: a) if memory == "device" else (lambda a, ints: _i(a) if ints else _d(a))
+        arrs = [conv(A[0], 1), conv(A[1], 1), conv(A[2], 0), conv(F["Gi"], 1), conv(F["Gj"], 1), conv(F["Gv"], 0),
+                conv(F["IDv"], 0), conv(F["Hi"], 1), conv(F["Hj"], 1), conv(F["Hv"], 0)]
+        self._h = C.c_void_p(0)
+        _check(lib().fiim_block_create(C.byref(self._h), C.c_int(self.n), C.c_int(nrhs),
+                                       *[_ptr(a) for a in arrs], C.byref(o)))
+
+    def solve(self, B, X, tol=1e-8, nmax=1000):
+        k = self.k
+        it, info = np.zeros(k, np.int32), np.zeros(k, np.int32)
+        rv, tr = np.zeros(k), np.zeros(k)
+        r = Result()
+        if self.memory != "device":
+            B = _d(B)
+            assert X.dtype == np.float64 and X.flags.c_contiguous
+        _check(lib().fiim_block_solve(self._h, _ptr(B), _ptr(X), C.c_double(tol), C.c_int(nmax), _ptr(it),
+                                      _ptr(info), _ptr(rv), _ptr(tr), C.byref(r)))
+        return {"iter": it, "info": info, "resval": rv, "true_relres": tr, "summary": r.as_dict()}
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().fiim_block_destroy(self._h)
             self._h = C.c_void_p(0)
 
     def __del__(self):

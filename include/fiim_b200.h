@@ -180,6 +180,27 @@ int fiim_batch_solve(fiim_batch_t s, const double *b, double *x, double tol, int
 int fiim_batch_destroy(fiim_batch_t s);
 
 /* ===========================================================================
+ * Multi-RHS block solve: 1..32 right-hand sides of one system. No counterpart in the
+ * reference (one right-hand side per call); each right-hand side runs the reference's
+ * loop with its own scalars and termination, and the sparse products are shared (SpMM).
+ * B and X are n x nrhs, row-major (entry (i, j) at i * nrhs + j), in opt->memory space.
+ * opt->precision: G, H stored in FP64 (FIIM_FP64) or FP32 (FIIM_MIXED_FP32).
+ * ======================================================================== */
+typedef struct fiim_block_s *fiim_block_t;
+
+int fiim_block_create(fiim_block_t *out, int n, int nrhs, const int *Ai, const int *Aj,
+                      const double *Av, const int *Gi, const int *Gj, const double *Gv,
+                      const double *IDv, const int *Hi, const int *Hj, const double *Hv,
+                      const fiim_options *opt);
+
+/* Per-RHS outputs (host arrays of nrhs, any may be NULL) as for fiim_batch_solve. */
+int fiim_block_solve(fiim_block_t s, const double *B, double *X, double tol, int NMAX,
+                     int *iter, int *info, double *resval, double *true_relres,
+                     fiim_result *summary);
+
+int fiim_block_destroy(fiim_block_t s);
+
+/* ===========================================================================
  * Kernel-level entry points (device arrays, caller's stream; asynchronous).
  * ======================================================================== */
 

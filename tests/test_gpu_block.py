@@ -1,0 +1,77 @@
+"""Multi-RHS block solve on B200: k right-hand sides of one system sharing the sparse
+products, each with its own BiCGSTAB scalars and termination.
+
+Every right-hand side is checked against the oracle solving it alone: same info,
+iterations within +-2 of the oracle's rounding envelope, tolerance reached, solution within
+the oracle's own spread. With FP32 factor storage the oracle runs on the same rounded
+factor values.
+"""
+import numpy as np
+import pytest
+
+import fiim_b200 as FB
+from test_gpu_batch import envelope, rounded
+
+pytestmark = pytest.mark.gpu
+
+
+def zipf_system(n, seed):
+    scale = FB.zipf_scale(n, sample=n, seed=seed)
+    A = FB.gen_zipf(n, scale, seed=seed)
+    F = FB.pdfiim_build(A, 0.1, 1, 1, 1, 32, "I", "B")
+    return A, F
+
+
+def check_block(A, F, k, precision, variant="afiim", seed=5, nmax=1000):
+    n = len(A[0]) - 1
+    B = np.stack([FB.rand_normal(n, seed + j) for j in range(k)], axis=1).copy()
+    X = np.zeros((n, k))
+    S = FB.BlockSolver(A, F, k, variant=variant, precision=precision)
+    res = S.solve(B, X, tol=1e-8, nmax=nmax)
+    S.close()
+    for j in range(k):
+        xo, info, lo, hi, spread = envelope(variant, A, B[:, j].copy(), rounded(F, precision), nmax)
+        it = int(res["iter"][j])
+        dx = np.linalg.norm(X[:, j] - xo) / np.linalg.norm(xo)
+        print(f"k={k} {precision} rhs {j}: gpu iter {it} info {res['info'][j]} | oracle [{lo},{hi}] info {info} | "
+              f"x diff {dx:.2e}")
+        assert res["info"][j] == info
+        assert lo - 2 <= it <= hi + 2
+        if info == 0:
+            assert res["resval"][j] < 1e-8
+            assert dx <= 10 * spread + 1e-9
+    return res
+
+
+def test_block_zipf_8_rhs():
+    A, F = zipf_system(3000, 11)
+    check_block(A, F, 8, "fp64")
+
+
+def test_block_zipf_5_rhs_fp32_factors():
+    """k = 5: four rows per warp, three idle lanes per row group."""
+    A, F = zipf_system(2000, 13)
+    check_block(A, F, 5, "fp32", seed=40)
+
+
+def test_block_convdiff_32_rhs():
+    A = FB.gen_convdiff3d(12, 0.5)
+    F = FB.pdfiim_build(A, 0.05, 2, 2, 1, -1, "I", "B")
+    res = check_block(A, F, 32, "fp32", variant="pdfiim", seed=100)
+    assert (res["info"] == 0).all()
+
+
+def test_block_one_rhs_equals_single_solver():
+    """k = 1 through the block path agrees with the single-system solver."""
+    A, F = zipf_system(1500, 17)
+    b = FB.rand_normal(1500, 3)
+    X = np.zeros((1500, 1))
+    S = FB.BlockSolver(A, F, 1)
+    r = S.solve(b.reshape(-1, 1), X)
+    S.close()
+    S1 = FB.Solver(A, F)
+    x = np.zeros(1500)
+    r1 = S1.solve(b, x)
+    S1.close()
+    assert r["info"][0] == r1["info"] == 0 and abs(int(r["iter"][0]) - r1["iter"]) <= 2
+    assert np.linalg.norm(X[:, 0] - x) <= 1e-6 * np.linalg.norm(x)
