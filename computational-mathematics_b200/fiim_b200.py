@@ -245,6 +245,24 @@ class Solver:
             pass
 
 
+# ----------------------------------------------------------------------------- sharding
+def shard_by_nnz(weights, world, rank):
+    """Contiguous shard of independent units (systems, right-hand sides) for `rank` of
+    `world`, balanced by weight (e.g. nnz): the cut after unit i lies where the running
+    total first reaches (r + 1) / world of the whole. Deterministic, no communication;
+    every unit goes to exactly one rank. Returns (first, last) with last exclusive."""
+    w = np.asarray(weights, dtype=np.float64)
+    if world <= 1 or len(w) == 0:
+        return 0, len(w)
+    c = np.cumsum(w)
+    total = c[-1]
+    cuts = [0] + [int(np.searchsorted(c, total * (r + 1) / world, side="left")) + 1 for r in range(world - 1)] + [len(w)]
+    cuts = [min(max(x, 0), len(w)) for x in cuts]
+    for r in range(1, len(cuts)):
+        cuts[r] = max(cuts[r], cuts[r - 1])
+    return cuts[rank], cuts[rank + 1]
+
+
 # ----------------------------------------------------------------------------- batched API
 def block_diag(mats):
     """Concatenate CSR triples (Ai, Aj, Av) into one block-diagonal CSR in global numbering.
