@@ -57,7 +57,8 @@ struct DevCsr {
     int vec = 8;                 // lanes per row of the set-up-free SpMV
     int tile = 2048;             // entries per row block of the CSR-stream SpMV
     int staged = 0;              // 1: row blocks moved by bulk copies (fiim_pipe.cuh)
-    int *rb = nullptr;           // row-block starts (device), nblk + 1 entries
+    int *rb = nullptr;           // row-block first rows (device), nblk + 1 entries
+    int *eb = nullptr;           // row-block first entries (device), nblk + 1 entries
     int nblk = 0;
     std::vector<int> hrp;        // row offsets on the host (row blocks, tuning key)
     std::vector<long> sig;       // tuning-cache key: n, nnz, sampled row offsets

@@ -56,6 +56,14 @@ struct CsrView {
     int n;
 };
 
+// ---------------------------------------------------------------- launch dependencies
+// Programmatic dependent launch: pdl_enter waits for the previous kernel in the stream to
+// complete (its writes visible) before anything it produced is touched; pdl_release, once
+// a CTA's main loop is done, lets the next kernel's CTAs be scheduled during this kernel's
+// tail. Both are no-ops in a launch without the programmatic-serialization attribute.
+__device__ __forceinline__ void pdl_enter() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // ---------------------------------------------------------------- loads
 // Matrix streams are read once per pass: evict-first so the vectors stay in L2.
 __device__ __forceinline__ double ldm(const double *p) { return __ldcs(p); }
@@ -280,50 +288,88 @@ struct EpiAccumNorm {              // y = (M x) + y, ||y||^2 -> st->pc2
 // ---------------------------------------------------------------- CSR-stream SpMV
 // Rows are grouped at set-up into row blocks: consecutive rows, at most kThreads of
 // them, whose entries total at most TILE; a row longer than TILE is a block of its
-// own. A CTA takes row blocks in grid-stride order. For each block it streams the
-// entries coalesced (columns and values with evict-first loads, x gathered through the
-// read-only path), stores the rounded products v*x in shared memory, then each thread
-// sums its own row's products left to right. A long row is summed by one thread over
-// TILE-sized chunks, still in storage order.
+// own. rb holds each block's first row and eb its first entry (nblk + 1 of each). A CTA
+// takes row blocks in grid-stride order. For each block it streams the entries coalesced
+// (columns and values with evict-first loads, x gathered through the read-only path),
+// stores the rounded products v*x in shared memory, then each thread sums its own row's
+// products left to right. A long row is summed by one thread over TILE-sized chunks,
+// still in storage order.
+//
+// The loop is software-pipelined by one block: the next block's bounds, this thread's
+// row offsets in it and its share of the column/value stream are loaded into registers
+// before the barrier, so they are in flight while the current block's rows are summed.
 template <int TILE, typename Epi>
 static __global__ void __launch_bounds__(kThreads)
-k_spmv_rows(CsrView<double> M, const int *__restrict__ rb, int nblk, const double *__restrict__ x,
-            Epi epi, DState *st, double *__restrict__ partials) {
+k_spmv_rows(CsrView<double> M, const int *__restrict__ rb, const int *__restrict__ eb, int nblk,
+            const double *__restrict__ x, Epi epi, DState *st, double *__restrict__ partials) {
+    pdl_enter();
     if (Epi::GATED && st != nullptr && st->done) return;
     __shared__ double prod[TILE];
+    constexpr int PER = TILE / kThreads;
+    const int tid = (int)threadIdx.x;
     double red[Epi::NR];
 #pragma unroll
     for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
-    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
-        const int r0 = __ldg(rb + blk), r1 = __ldg(rb + blk + 1);
-        const int e0 = __ldg(M.rp + r0), e1 = __ldg(M.rp + r1);
+    int r0 = 0, r1 = 0, e0 = 0, e1 = 0, rbeg = 0, rend = 0;
+    int c[PER];
+    double a[PER];
+    auto fetch = [&](int blk) {
+        r0 = __ldg(rb + blk);
+        r1 = __ldg(rb + blk + 1);
+        e0 = __ldg(eb + blk);
+        e1 = __ldg(eb + blk + 1);
+        rbeg = rend = 0;
+        if (r0 + tid < r1) {
+            rbeg = __ldg(M.rp + r0 + tid);
+            rend = __ldg(M.rp + r0 + tid + 1);
+        }
         if (e1 - e0 <= TILE) {
-#pragma unroll 4
-            for (int e = e0 + (int)threadIdx.x; e < e1; e += kThreads)
-                prod[e - e0] = __dmul_rn(ldm(M.v + e), ldx(x + ldi(M.ci + e)));
+#pragma unroll
+            for (int u = 0; u < PER; ++u) {
+                const int e = e0 + tid + u * kThreads;
+                c[u] = 0;
+                a[u] = 0.0;
+                if (e < e1) {
+                    c[u] = ldi(M.ci + e);
+                    a[u] = ldm(M.v + e);
+                }
+            }
+        }
+    };
+    if ((int)blockIdx.x < nblk) fetch(blockIdx.x);
+    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        const int nxt = blk + (int)gridDim.x;
+        const int cr0 = r0, cr1 = r1, ce0 = e0, ce1 = e1, cb = rbeg - e0, ce = rend - e0;
+        if (ce1 - ce0 <= TILE) {
+#pragma unroll
+            for (int u = 0; u < PER; ++u) {
+                const int q = tid + u * kThreads;
+                if (ce0 + q < ce1) prod[q] = __dmul_rn(a[u], ldx(x + c[u]));
+            }
+            if (nxt < nblk) fetch(nxt);
             __syncthreads();
-            const int r = r0 + (int)threadIdx.x;
-            if (r < r1) {
-                const int b = __ldg(M.rp + r) - e0, e = __ldg(M.rp + r + 1) - e0;
+            if (cr0 + tid < cr1) {
                 double s = 0.0;
-                for (int k = b; k < e; ++k) s = __dadd_rn(s, prod[k]);
-                epi.emit(r, s, red);
+                for (int k = cb; k < ce; ++k) s = __dadd_rn(s, prod[k]);
+                epi.emit(cr0 + tid, s, red);
             }
             __syncthreads();
         } else {
             double s = 0.0;
-            for (int c0 = e0; c0 < e1; c0 += TILE) {
-                const int c1 = min(c0 + TILE, e1);
-                for (int e = c0 + (int)threadIdx.x; e < c1; e += kThreads)
+            for (int c0 = ce0; c0 < ce1; c0 += TILE) {
+                const int c1 = min(c0 + TILE, ce1);
+                for (int e = c0 + tid; e < c1; e += kThreads)
                     prod[e - c0] = __dmul_rn(ldm(M.v + e), ldx(x + ldi(M.ci + e)));
                 __syncthreads();
-                if (threadIdx.x == 0)
+                if (tid == 0)
                     for (int k = 0; k < c1 - c0; ++k) s = __dadd_rn(s, prod[k]);
                 __syncthreads();
             }
-            if (threadIdx.x == 0) epi.emit(r0, s, red);
+            if (tid == 0) epi.emit(cr0, s, red);
+            if (nxt < nblk) fetch(nxt);
         }
     }
+    pdl_release();
     if constexpr (Epi::REDUCES) grid_reduce<Epi::NR>(red, partials, st, epi);
 }
 
@@ -395,6 +441,7 @@ static __global__ void __launch_bounds__(kThreads)
 k_update_s(long n, const double *__restrict__ r, const double *__restrict__ v,
            const double *__restrict__ x, double *__restrict__ s, DState *st,
            double *__restrict__ partials) {
+    pdl_enter();
     if (st->done) return;
     const double na = -st->alpha;
     double red[2] = {0.0, 0.0};
@@ -404,6 +451,7 @@ k_update_s(long n, const double *__restrict__ r, const double *__restrict__ v,
         red[0] += ri * ri;
         red[1] += xi * xi;
     }
+    pdl_release();
     grid_reduce<2>(red, partials, st, FinS{});
 }
 
@@ -435,6 +483,7 @@ k_update_xr(long n, const double *__restrict__ pc, const double *__restrict__ sc
             const double *__restrict__ s, const double *__restrict__ t,
             const double *__restrict__ r0, double *__restrict__ x, double *__restrict__ r,
             DState *st, double *__restrict__ partials) {
+    pdl_enter();
     if (st->done) return;
     const double a = st->alpha, om = st->omega, nom = -st->omega;
     double red[1] = {0.0};
@@ -447,6 +496,7 @@ k_update_xr(long n, const double *__restrict__ pc, const double *__restrict__ sc
         r[i] = ri;
         red[0] += r0[i] * ri;
     }
+    pdl_release();
     grid_reduce<1>(red, partials, st, FinControl{});
 }
 
@@ -458,6 +508,7 @@ k_update_xr(long n, const double *__restrict__ pc, const double *__restrict__ sc
 static __global__ void __launch_bounds__(kThreads)
 k_update_p(long n, const double *__restrict__ r, const double *__restrict__ v,
            double *__restrict__ p, DState *st, cudaGraphConditionalHandle h, int cond) {
+    pdl_enter();
     if (cond && blockIdx.x == 0 && threadIdx.x == 0) {
         const int loops = ++st->loops;
         if (!st->done && loops > st->nmax + 2) {

@@ -57,7 +57,7 @@ cudaError_t rows_64(cudaStream_t s, const DevCsr &M, const double *x, const Epi 
                     double *partials) {
     auto kern = k_spmv_rows<TILE, Epi>;
     const int g = grid_for(kern, 1, M.nblk);
-    kern<<<g, kThreads, 0, s>>>(view64(M), M.rb, M.nblk, x, epi, st, partials);
+    kern<<<g, kThreads, 0, s>>>(view64(M), M.rb, M.eb, M.nblk, x, epi, st, partials);
     return cudaGetLastError();
 }
 

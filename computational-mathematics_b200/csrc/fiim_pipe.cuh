@@ -66,6 +66,7 @@ template <int TILE, typename Epi>
 static __global__ void __launch_bounds__(kThreads)
 k_spmv_pipe(CsrView<double> M, const int *__restrict__ rb, int nblk, const double *__restrict__ x, Epi epi,
             DState *st, double *__restrict__ partials, int *fault) {
+    pdl_enter();
     if (Epi::GATED && st != nullptr && st->done) return;
     using SM = PipeSmem<TILE>;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -163,6 +164,7 @@ k_spmv_pipe(CsrView<double> M, const int *__restrict__ rb, int nblk, const doubl
             if (r < r1) epi.emit(r, 0.0, red);
         }
     }
+    pdl_release();
     if constexpr (Epi::REDUCES) grid_reduce<Epi::NR>(red, partials, st, epi);
 }
 

@@ -105,6 +105,30 @@ void Arena::release() {
 size_t Arena::need(size_t bytes) { return (bytes + 255) & ~size_t(255); }
 
 // ------------------------------------------------------------------ launch shapes
+// Launch with programmatic stream serialization (PDL) unless FIIM_PDL=0.
+static bool pdl_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("FIIM_PDL");
+        return !(e && std::strcmp(e, "0") == 0);
+    }();
+    return on;
+}
+
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_k(void (*kern)(KArgs...), int grid, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 template <int VEC, int FILL, typename Epi>
 static cudaError_t spmv_vec(cudaStream_t s, const CsrView<double> &M, const double *x, const Epi &epi,
                             DState *st, double *partials) {
@@ -134,8 +158,7 @@ static cudaError_t spmv_rows(cudaStream_t s, const DevCsr &M, const double *x, c
                              DState *st, double *partials) {
     auto kern = k_spmv_rows<TILE, Epi>;
     const int g = grid_for(kern, 1, M.nblk);
-    kern<<<g, kThreads, 0, s>>>(view(M), M.rb, M.nblk, x, epi, st, partials);
-    return cudaGetLastError();
+    return launch_k(kern, g, 0, s, view(M), M.rb, M.eb, M.nblk, x, epi, st, partials);
 }
 
 template <int TILE, typename Epi>
@@ -164,8 +187,7 @@ static cudaError_t spmv_pipe(cudaStream_t s, const DevCsr &M, const double *x, c
         }
     }
     const int g = (int)std::min<long>(std::max(M.nblk, 1), (long)occ * num_sms());
-    kern<<<g, kThreads, smem, s>>>(view(M), M.rb, M.nblk, x, epi, st, partials, fault);
-    return cudaGetLastError();
+    return launch_k(kern, g, smem, s, view(M), M.rb, M.nblk, x, epi, st, partials, fault);
 }
 
 // Solver SpMV: CSR-stream over the matrix's row blocks, exact row order; staged (bulk
@@ -219,7 +241,10 @@ int set_tile(DevCsr &M, int tile, cudaStream_t s) {
     build_row_blocks(M.hrp, tile, kThreads, rb);
     M.tile = tile;
     M.nblk = (int)rb.size() - 1;
+    std::vector<int> eb(rb.size());
+    for (size_t k = 0; k < rb.size(); ++k) eb[k] = M.hrp[rb[k]];
     FIIM_CUDA(cudaMemcpyAsync(M.rb, rb.data(), sizeof(int) * rb.size(), cudaMemcpyHostToDevice, s));
+    FIIM_CUDA(cudaMemcpyAsync(M.eb, eb.data(), sizeof(int) * eb.size(), cudaMemcpyHostToDevice, s));
     FIIM_CUDA(cudaStreamSynchronize(s));
     return FIIM_OK;
 }
@@ -418,13 +443,15 @@ int carve_csr(Arena &ar, DevCsr &M, long n, long nnz) {
     M.rp = static_cast<int *>(ar.take(sizeof(int) * (n + 1)));
     M.ci = static_cast<int *>(ar.take(sizeof(int) * std::max<long>(nnz, 1)));
     M.v = static_cast<double *>(ar.take(sizeof(double) * std::max<long>(nnz, 1)));
-    M.rb = static_cast<int *>(ar.take(sizeof(int) * (n + 1)));   // at most one block per row
+    M.rb = static_cast<int *>(ar.take(sizeof(int) * 2 * (n + 1)));   // at most one block per row
     if (!M.rp || !M.ci || !M.v || !M.rb) return set_error(FIIM_ENOMEM, "arena exhausted");
+    M.eb = M.rb + (n + 1);
     return FIIM_OK;
 }
 
 size_t csr_bytes(long n, long nnz) {
-    return 2 * Arena::need(sizeof(int) * (n + 1)) + Arena::need(sizeof(int) * std::max<long>(nnz, 1)) +
+    return Arena::need(sizeof(int) * (n + 1)) + Arena::need(sizeof(int) * 2 * (n + 1)) +
+           Arena::need(sizeof(int) * std::max<long>(nnz, 1)) +
            Arena::need(sizeof(double) * std::max<long>(nnz, 1));
 }
 
@@ -473,15 +500,12 @@ int Solver::enqueue_iteration(bool cond, cudaGraphConditionalHandle h) {
     const long nn = n;
     FIIM_TRY(enqueue_prec(p, pc, true));                                             // K1-K2
     FIIM_CUDA(launch_spmv(A, s, pc, EpiAlpha{v, r0}, st, partials, fault));     // K3
-    k_update_s<<<stream_grid(k_update_s, nn), kThreads, 0, s>>>(nn, r, v, x, sv, st, partials);  // K4
-    FIIM_CUDA(cudaGetLastError());
+    FIIM_CUDA(launch_k(k_update_s, stream_grid(k_update_s, nn), 0, s, nn, r, v, x, sv, st, partials));  // K4
     FIIM_TRY(enqueue_prec(sv, sc, false));                                           // K5-K6
     FIIM_CUDA(launch_spmv(A, s, sc, EpiOmega{t, sv}, st, partials, fault));    // K7
-    k_update_xr<<<stream_grid(k_update_xr, nn), kThreads, 0, s>>>(nn, pc, sc, sv, t, r0, x, r, st,
-                                                                  partials);          // K8
-    FIIM_CUDA(cudaGetLastError());
-    k_update_p<<<stream_grid(k_update_p, nn), kThreads, 0, s>>>(nn, r, v, p, st, h, cond ? 1 : 0);  // K9
-    FIIM_CUDA(cudaGetLastError());
+    FIIM_CUDA(launch_k(k_update_xr, stream_grid(k_update_xr, nn), 0, s, nn, pc, sc, sv, t, r0, x, r, st,
+                       partials));                                                      // K8
+    FIIM_CUDA(launch_k(k_update_p, stream_grid(k_update_p, nn), 0, s, nn, r, v, p, st, h, cond ? 1 : 0));  // K9
     return FIIM_OK;
 }
 
