@@ -29,6 +29,9 @@
 // (st->done), so iterations can run ahead of any host check.
 #pragma once
 
+#include <type_traits>
+#include <utility>
+
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
@@ -73,6 +76,8 @@ __device__ __forceinline__ float ldm(const __nv_bfloat16 *p) {
     return __bfloat162float(__ushort_as_bfloat16(u));
 }
 __device__ __forceinline__ int ldi(const int *p) { return __ldcs(p); }
+__device__ __forceinline__ int2 ldi2(const int *p) { return __ldcs(reinterpret_cast<const int2 *>(p)); }
+__device__ __forceinline__ double2 ldm2(const double *p) { return __ldcs(reinterpret_cast<const double2 *>(p)); }
 // Gathered vector entries: read-only path, cached.
 template <typename X>
 __device__ __forceinline__ X ldx(const X *p) { return __ldg(p); }
@@ -164,17 +169,26 @@ struct FinInit {   // ro = ||r0||, m1 = ro^2, rc = ro (AFIIM/src/bicgstab.cpp:16
     static constexpr bool REDUCES = reduces;      \
     static constexpr bool GATED = gated
 
+template <typename E, typename = void>
+struct HasPre : std::false_type {};
+template <typename E>
+struct HasPre<E, std::void_t<decltype(std::declval<const E &>().pre(0L))>> : std::true_type {};
+
 struct EpiStore {                  // y = M x
     FIIM_EPI(1, false, true);
     double *y;
     __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = s; }
     __device__ void finish(DState *, const double *) const {}
 };
+// Epilogues with a per-row operand also offer pre(i), its load, and emit_pre(i, s, o, red);
+// the CSR-stream SpMV loads the operand with the next row block's stream (HasPre).
 struct EpiScale {                  // y = d o (M x): vdMul(n, IDv, pc, tm), AFIIM/src/bicgstab.cpp:173
     FIIM_EPI(1, false, true);
     double *y;
     const double *__restrict__ d;
-    __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = __dmul_rn(__ldg(d + i), s); }
+    __device__ double pre(long i) const { return __ldg(d + i); }
+    __device__ void emit_pre(long i, double s, double di, double (&)[NR]) const { y[i] = __dmul_rn(di, s); }
+    __device__ void emit(long i, double s, double (&r)[NR]) const { emit_pre(i, s, pre(i), r); }
     __device__ void finish(DState *, const double *) const {}
 };
 struct EpiNorm {                   // y = M x, ||y||^2 -> st->pc2 (stagnation test)
@@ -187,10 +201,12 @@ struct EpiAlpha {                  // v = A pc, alpha = m1 / (r0 . v)
     FIIM_EPI(1, true, true);
     double *y;
     const double *__restrict__ r0;
-    __device__ void emit(long i, double s, double (&r)[NR]) const {
+    __device__ double pre(long i) const { return __ldg(r0 + i); }
+    __device__ void emit_pre(long i, double s, double r0i, double (&r)[NR]) const {
         y[i] = s;
-        r[0] += __ldg(r0 + i) * s;
+        r[0] += r0i * s;
     }
+    __device__ void emit(long i, double s, double (&r)[NR]) const { emit_pre(i, s, pre(i), r); }
     __device__ void finish(DState *st, const double *t) const {
         st->r0v = t[0];
         st->alpha = st->m1 / t[0];
@@ -206,11 +222,13 @@ struct EpiOmega {                  // t = A sc, omega = (t . s) / (t . t)
     FIIM_EPI(2, true, true);
     double *y;
     const double *__restrict__ sv;
-    __device__ void emit(long i, double s, double (&r)[NR]) const {
+    __device__ double pre(long i) const { return __ldg(sv + i); }
+    __device__ void emit_pre(long i, double s, double si, double (&r)[NR]) const {
         y[i] = s;
-        r[0] += s * __ldg(sv + i);
+        r[0] += s * si;
         r[1] += s * s;
     }
+    __device__ void emit(long i, double s, double (&r)[NR]) const { emit_pre(i, s, pre(i), r); }
     __device__ void finish(DState *st, const double *t) const {
         st->ts = t[0];
         st->tt = t[1];
@@ -287,8 +305,8 @@ struct EpiAccumNorm {              // y = (M x) + y, ||y||^2 -> st->pc2
 
 // ---------------------------------------------------------------- CSR-stream SpMV
 // Rows are grouped at set-up into row blocks: consecutive rows, at most kThreads of
-// them, whose entries total at most TILE; a row longer than TILE is a block of its
-// own. rb holds each block's first row and eb its first entry (nblk + 1 of each). A CTA
+// them, whose entries total at most TILE - 1; a row of TILE or more entries is a block
+// of its own. rb holds each block's first row and eb its first entry (nblk + 1 of each). A CTA
 // takes row blocks in grid-stride order. For each block it streams the entries coalesced
 // (columns and values with evict-first loads, x gathered through the read-only path),
 // stores the rounded products v*x in shared memory, then each thread sums its own row's
@@ -311,6 +329,11 @@ k_spmv_rows(CsrView<double> M, const int *__restrict__ rb, const int *__restrict
 #pragma unroll
     for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
     int r0 = 0, r1 = 0, e0 = 0, e1 = 0, rbeg = 0, rend = 0;
+    double opnd = 0.0;   // the epilogue's operand for this thread's row (HasPre)
+    // Entries are read in aligned pairs: thread tid holds entries a0 + 2 (tid + u kThreads)
+    // + h of the window [a0, a0 + TILE), a0 = e0 rounded down to even. Row blocks have at
+    // most TILE - 1 entries, so the window covers [e0, e1); a block that does not fit is a
+    // single long row.
     int c[PER];
     double a[PER];
     auto fetch = [&](int blk) {
@@ -322,16 +345,25 @@ k_spmv_rows(CsrView<double> M, const int *__restrict__ rb, const int *__restrict
         if (r0 + tid < r1) {
             rbeg = __ldg(M.rp + r0 + tid);
             rend = __ldg(M.rp + r0 + tid + 1);
+            if constexpr (HasPre<Epi>::value) opnd = epi.pre(r0 + tid);
         }
-        if (e1 - e0 <= TILE) {
+        if (e1 - e0 < TILE) {
+            const int a0 = e0 & ~1;
 #pragma unroll
-            for (int u = 0; u < PER; ++u) {
-                const int e = e0 + tid + u * kThreads;
-                c[u] = 0;
-                a[u] = 0.0;
-                if (e < e1) {
-                    c[u] = ldi(M.ci + e);
-                    a[u] = ldm(M.v + e);
+            for (int u = 0; u < PER / 2; ++u) {
+                const int e = a0 + 2 * (tid + u * kThreads);
+                c[2 * u] = c[2 * u + 1] = 0;
+                a[2 * u] = a[2 * u + 1] = 0.0;
+                if (e + 1 < e1) {
+                    const int2 cc = ldi2(M.ci + e);
+                    const double2 aa = ldm2(M.v + e);
+                    c[2 * u] = cc.x;
+                    c[2 * u + 1] = cc.y;
+                    a[2 * u] = aa.x;
+                    a[2 * u + 1] = aa.y;
+                } else if (e < e1) {
+                    c[2 * u] = ldi(M.ci + e);
+                    a[2 * u] = ldm(M.v + e);
                 }
             }
         }
@@ -340,18 +372,21 @@ k_spmv_rows(CsrView<double> M, const int *__restrict__ rb, const int *__restrict
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
         const int nxt = blk + (int)gridDim.x;
         const int cr0 = r0, cr1 = r1, ce0 = e0, ce1 = e1, cb = rbeg - e0, ce = rend - e0;
-        if (ce1 - ce0 <= TILE) {
+        const double copnd = opnd;
+        if (ce1 - ce0 < TILE) {
+            const int a0 = ce0 & ~1;
 #pragma unroll
             for (int u = 0; u < PER; ++u) {
-                const int q = tid + u * kThreads;
-                if (ce0 + q < ce1) prod[q] = __dmul_rn(a[u], ldx(x + c[u]));
+                const int e = a0 + 2 * (tid + (u >> 1) * kThreads) + (u & 1);
+                if (e >= ce0 && e < ce1) prod[e - ce0] = __dmul_rn(a[u], ldx(x + c[u]));
             }
             if (nxt < nblk) fetch(nxt);
             __syncthreads();
             if (cr0 + tid < cr1) {
                 double s = 0.0;
                 for (int k = cb; k < ce; ++k) s = __dadd_rn(s, prod[k]);
-                epi.emit(cr0 + tid, s, red);
+                if constexpr (HasPre<Epi>::value) epi.emit_pre(cr0 + tid, s, copnd, red);
+                else epi.emit(cr0 + tid, s, red);
             }
             __syncthreads();
         } else {

@@ -200,6 +200,7 @@ cudaError_t launch_spmv(const DevCsr &M, cudaStream_t s, const double *x, const 
         return spmv_pipe<2048>(s, M, x, epi, st, partials, fault);
     }
     switch (M.tile) {
+        case 512: return spmv_rows<512>(s, M, x, epi, st, partials);
         case 1024: return spmv_rows<1024>(s, M, x, epi, st, partials);
         case 4096: return spmv_rows<4096>(s, M, x, epi, st, partials);
         default: return spmv_rows<2048>(s, M, x, epi, st, partials);
@@ -238,7 +239,7 @@ void build_row_blocks(const std::vector<int> &rp, int tile, int max_rows, std::v
 
 int set_tile(DevCsr &M, int tile, cudaStream_t s) {
     std::vector<int> rb;
-    build_row_blocks(M.hrp, tile, kThreads, rb);
+    build_row_blocks(M.hrp, tile - 1, kThreads, rb);   // k_spmv_rows reads aligned pairs
     M.tile = tile;
     M.nblk = (int)rb.size() - 1;
     std::vector<int> eb(rb.size());
@@ -249,10 +250,10 @@ int set_tile(DevCsr &M, int tile, cudaStream_t s) {
     return FIIM_OK;
 }
 
-// Row-block size used when timing-based tuning is off: smaller blocks for longer rows.
-static int default_tile(const DevCsr &M) {
-    return (M.n > 0 && (double)M.nnz / (double)M.n > 8.0) ? 1024 : 2048;
-}
+// Row-block size used when timing-based tuning is off. With the row-block loop pipelined
+// (next block's stream and epilogue operands in registers), 2048 entries per block was the
+// fastest size for the 7-, 6- and 11-entry rows of the 3D convection-diffusion A, G and H.
+static int default_tile(const DevCsr &) { return 2048; }
 
 // Time each row-block size on this matrix and keep the fastest; cached by signature.
 // The choice changes speed only: every shape sums each row in storage order.
@@ -275,8 +276,8 @@ static int autotune_tile(DevCsr &M, const double *x, double *y, cudaStream_t s, 
         M.staged = cached < 0;
         return set_tile(M, cached < 0 ? -cached : cached, s);
     }
-    // Candidates: unstaged TILE 1024 / 2048 / 4096, staged TILE 1024 / 2048 (negative).
-    const int cands[5] = {1024, 2048, 4096, -1024, -2048};
+    // Candidates: unstaged TILE 512 / 1024 / 2048 / 4096, staged TILE 1024 / 2048 (negative).
+    const int cands[6] = {512, 1024, 2048, 4096, -1024, -2048};
     cudaEvent_t e0, e1;
     FIIM_CUDA(cudaEventCreate(&e0));
     FIIM_CUDA(cudaEventCreate(&e1));

@@ -207,6 +207,7 @@ class Solver:
         return int(lib().fiim_solver_device_bytes(self._h))
 
     def spmv_shape(self, which: int) -> int:
+        """Row-block size of matrix `which` (0 A, 1 G, 2 H); negative when bulk-copy staged."""
         v = C.c_int(0)
         _check(lib().fiim_solver_spmv_shape(self._h, C.c_int(which), C.byref(v)))
         return v.value

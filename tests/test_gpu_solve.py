@@ -72,18 +72,48 @@ def test_prec_apply_matches_oracle(golden, cuda, name, prefix):
                                                                      {"issym": True})])
 @pytest.mark.parametrize("form", ["rows", "staged"])
 def test_solver_products_bit_identical(golden, monkeypatch, name, prefix, variant, kw, form):
-    """The solver's tuned CSR-stream kernels, unstaged and staged by bulk copies, reproduce
-    the oracle's A x and M x exactly."""
+    """The solver's tuned CSR-stream kernels, register-staged or staged by bulk copies,
+    reproduce the oracle's A x and M x exactly."""
     monkeypatch.setenv("FIIM_SPMV", form)
     g = golden(name)
     F = sub(g, prefix)
-    S = FB.Solver((g["Ai"], g["Aj"], g["Av"]), F, variant=variant, **kw)
+    S = FB.Solver((g["Ai"], g["Aj"], g["Av"]), F, variant=variant, autotune=True, **kw)
     n = len(g["b"])
     y = S.apply(F["u"], np.zeros(n), op="A")
     assert np.array_equal(y, F["Au"])
     z = S.apply(F["u"], np.zeros(n), op="M")
     assert np.array_equal(z, F["MuC"] if kw.get("mode") == "C" else F["Mu"])
     S.close()
+
+
+@pytest.mark.parametrize("long_len", [0, 2046, 2047, 2048, 2500])
+def test_solver_spmv_random_rows(long_len):
+    """Random columns over the whole matrix, row blocks that start at odd entries, and a
+    few rows of about the row-block size (2048 entries for this mean row length): rows
+    that fill a block exactly, one entry short of it, or exceed it. A x through the
+    solver's row blocks equals the oracle's bit for bit."""
+    rng = np.random.default_rng(long_len)
+    n = 200000 if long_len == 0 else 20000
+    lens = rng.integers(1, 10, n)
+    rows, cols = [], []
+    for i, k in enumerate(lens):
+        if long_len and i % 1700 == 7:
+            k = long_len
+        rows.append(np.full(k, i))
+        cols.append(rng.choice(n, k, replace=False) if k > 64 else rng.integers(0, n, k))
+    rows, cols = np.concatenate(rows), np.concatenate(cols)
+    M = sp.csr_matrix((rng.uniform(-1, 1, rows.size), (rows, cols)), shape=(n, n))
+    M.sum_duplicates()
+    M.sort_indices()
+    A = (M.indptr.astype(np.int32), M.indices.astype(np.int32), M.data)
+    if long_len:
+        assert (np.diff(A[0]) == long_len).sum() == 12
+    u = rng.standard_normal(n)
+    S = FB.Solver(A, identity_factors(n))
+    assert S.spmv_shape(0) == 2048
+    y = S.apply(u, np.zeros(n), op="A")
+    S.close()
+    assert np.array_equal(y, O.csr_mv(*A, u))
 
 
 def test_prec_apply_ignores_entries_outside_triangles(cuda):
