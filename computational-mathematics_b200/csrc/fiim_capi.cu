@@ -169,12 +169,13 @@ int64_t fiim_solver_device_bytes(fiim_solver_t h) {
     return (int64_t) reinterpret_cast<fiim::Solver *>(h)->device_bytes();
 }
 
-int fiim_solver_spmv_shape(fiim_solver_t h, int which, int *shape) {
-    if (!h || !shape || fiim_is_mixed(h)) return fiim::set_error(FIIM_EARG, "bad handle");
+int fiim_solver_spmv_shape(fiim_solver_t h, int which, int *tile, int *form) {
+    if (!h || !tile || !form || fiim_is_mixed(h)) return fiim::set_error(FIIM_EARG, "bad handle");
     auto *s = reinterpret_cast<fiim::Solver *>(h);
     const fiim::DevCsr *m[] = {&s->A, &s->G, &s->H, &s->L, &s->U};
     if (which < 0 || which > 4) return fiim::set_error(FIIM_EARG, "which in 0..4 (A, G, H, L, U)");
-    *shape = m[which]->staged ? -m[which]->tile : m[which]->tile;
+    *tile = m[which]->tile;
+    *form = m[which]->form;
     return FIIM_OK;
 }
 

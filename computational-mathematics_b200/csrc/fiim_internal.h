@@ -46,6 +46,11 @@ struct Arena {
     static size_t need(size_t bytes);
 };
 
+// Forms of the CSR-stream SpMV. Both give the same bits; they differ in how a row block's
+// streams reach shared memory: through registers, pipelined by one block (fiim_kernels.cuh),
+// or by bulk copies into two buffers (fiim_pipe.cuh).
+constexpr int kFormRows = 0, kFormBulk = 1;
+
 // A CSR matrix resident on the device. v holds FP64 values; v32 / v16 are optional
 // FP32 / BF16 copies for the mixed-precision inner solve.
 struct DevCsr {
@@ -56,7 +61,7 @@ struct DevCsr {
     __nv_bfloat16 *v16 = nullptr;
     int vec = 8;                 // lanes per row of the set-up-free SpMV
     int tile = 2048;             // entries per row block of the CSR-stream SpMV
-    int staged = 0;              // 1: row blocks moved by bulk copies (fiim_pipe.cuh)
+    int form = 0;                // CSR-stream SpMV form, one of the kForm* constants
     int *rb = nullptr;           // row-block first rows (device), nblk + 1 entries
     int *eb = nullptr;           // row-block first entries (device), nblk + 1 entries
     int nblk = 0;

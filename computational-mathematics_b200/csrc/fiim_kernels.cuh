@@ -180,12 +180,14 @@ struct EpiStore {                  // y = M x
     __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = s; }
     __device__ void finish(DState *, const double *) const {}
 };
-// Epilogues with a per-row operand also offer pre(i), its load, and emit_pre(i, s, o, red);
-// the CSR-stream SpMV loads the operand with the next row block's stream (HasPre).
+// Epilogues with a per-row operand also offer pre_ptr(), the operand array, pre(i), its
+// load, and emit_pre(i, s, o, red); the CSR-stream SpMV forms load the operand together
+// with the next row block's streams (HasPre).
 struct EpiScale {                  // y = d o (M x): vdMul(n, IDv, pc, tm), AFIIM/src/bicgstab.cpp:173
     FIIM_EPI(1, false, true);
     double *y;
     const double *__restrict__ d;
+    __device__ const double *pre_ptr() const { return d; }
     __device__ double pre(long i) const { return __ldg(d + i); }
     __device__ void emit_pre(long i, double s, double di, double (&)[NR]) const { y[i] = __dmul_rn(di, s); }
     __device__ void emit(long i, double s, double (&r)[NR]) const { emit_pre(i, s, pre(i), r); }
@@ -201,6 +203,7 @@ struct EpiAlpha {                  // v = A pc, alpha = m1 / (r0 . v)
     FIIM_EPI(1, true, true);
     double *y;
     const double *__restrict__ r0;
+    __device__ const double *pre_ptr() const { return r0; }
     __device__ double pre(long i) const { return __ldg(r0 + i); }
     __device__ void emit_pre(long i, double s, double r0i, double (&r)[NR]) const {
         y[i] = s;
@@ -222,6 +225,7 @@ struct EpiOmega {                  // t = A sc, omega = (t . s) / (t . t)
     FIIM_EPI(2, true, true);
     double *y;
     const double *__restrict__ sv;
+    __device__ const double *pre_ptr() const { return sv; }
     __device__ double pre(long i) const { return __ldg(sv + i); }
     __device__ void emit_pre(long i, double s, double si, double (&r)[NR]) const {
         y[i] = s;

@@ -8,7 +8,7 @@
 // window is widened to 16-byte boundaries ([e0 & ~3, (e1 + 3) & ~3) for the int32 columns,
 // [e0 & ~1, (e1 + 1) & ~1) for the doubles) and the block's entries are read at an offset
 // of 0..3 (columns) / 0..1 (values). The widened tail reads at most 12 bytes past a matrix
-// array; the solver's arena carves every array with slack after it (see fiim_solver.cu).
+// array; carve_csr (fiim_solver.cu) leaves 16 bytes after the column and value arrays.
 //
 // Waits are bounded: an mbarrier that does not complete within the limit sets *fault and
 // the CTA stops (after a bounded wait for its own copies); the host turns the flag into

@@ -161,41 +161,45 @@ static cudaError_t spmv_rows(cudaStream_t s, const DevCsr &M, const double *x, c
     return launch_k(kern, g, 0, s, view(M), M.rb, M.eb, M.nblk, x, epi, st, partials);
 }
 
+// Resident CTAs per SM of a kernel with `smem` bytes of dynamic shared memory, with the
+// attribute that allows it set once per kernel and device.
+template <typename K>
+static int smem_occupancy(K kern, int smem, int *occ) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    const auto key = std::make_pair((const void *)kern, dev);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+        *occ = it->second;
+        return FIIM_OK;
+    }
+    FIIM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int b = 0;
+    FIIM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kThreads, smem));
+    *occ = cache[key] = std::max(b, 1);
+    return FIIM_OK;
+}
+
 template <int TILE, typename Epi>
 static cudaError_t spmv_pipe(cudaStream_t s, const DevCsr &M, const double *x, const Epi &epi, DState *st,
                              double *partials, int *fault) {
     auto kern = k_spmv_pipe<TILE, Epi>;
     constexpr int smem = PipeSmem<TILE>::kBytes;
-    static std::mutex mu;
-    static std::map<int, int> per_sm;   // device -> resident CTAs per SM
-    int dev = 0;
-    cudaGetDevice(&dev);
-    int occ;
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        auto it = per_sm.find(dev);
-        if (it == per_sm.end()) {
-            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            if (e != cudaSuccess) return e;
-            int b = 0;
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kThreads, smem);
-            if (e != cudaSuccess) return e;
-            per_sm[dev] = std::max(b, 1);
-            occ = std::max(b, 1);
-        } else {
-            occ = it->second;
-        }
-    }
+    int occ = 1;
+    if (smem_occupancy(kern, smem, &occ) != FIIM_OK) return cudaErrorInvalidConfiguration;
     const int g = (int)std::min<long>(std::max(M.nblk, 1), (long)occ * num_sms());
     return launch_k(kern, g, smem, s, view(M), M.rb, M.nblk, x, epi, st, partials, fault);
 }
 
-// Solver SpMV: CSR-stream over the matrix's row blocks, exact row order; staged (bulk
-// copies) or unstaged as the tuner chose. Both give the same bits.
+// Solver SpMV: CSR-stream over the matrix's row blocks, exact row order, in the form and
+// row-block size the tuner chose. Every form gives the same bits.
 template <typename Epi>
 cudaError_t launch_spmv(const DevCsr &M, cudaStream_t s, const double *x, const Epi &epi, DState *st,
                         double *partials, int *fault = nullptr) {
-    if (M.staged && fault) {
+    if (M.form == kFormBulk && fault) {
         if (M.tile == 1024) return spmv_pipe<1024>(s, M, x, epi, st, partials, fault);
         return spmv_pipe<2048>(s, M, x, epi, st, partials, fault);
     }
@@ -259,35 +263,39 @@ static int default_tile(const DevCsr &) { return 2048; }
 // The choice changes speed only: every shape sums each row in storage order.
 static int autotune_tile(DevCsr &M, const double *x, double *y, cudaStream_t s, int *fault) {
     static std::mutex mu;
-    static std::map<std::vector<long>, int> cache;
-    // FIIM_SPMV=rows or FIIM_SPMV=staged restricts the candidates to one form (tests use
-    // it to cover both; the results are the same bits either way).
+    static std::map<std::vector<long>, std::pair<int, int>> cache;
+    // FIIM_SPMV=rows or FIIM_SPMV=staged restricts the candidates to one form (tests use it
+    // to cover both; the results are the same bits in either form).
     const char *force = std::getenv("FIIM_SPMV");
-    const int only = !force ? 0 : (std::strcmp(force, "rows") == 0 ? 1 : (std::strcmp(force, "staged") == 0 ? 2 : 0));
+    const int only = !force ? -1
+                            : (std::strcmp(force, "rows") == 0     ? kFormRows
+                               : std::strcmp(force, "staged") == 0 ? kFormBulk
+                                                                   : -1);
     std::vector<long> key = M.sig;
     key.push_back(only);
-    int cached = 0;
+    std::pair<int, int> cached{0, 0};
     {
         std::lock_guard<std::mutex> lk(mu);
         auto it = cache.find(key);
         if (it != cache.end()) cached = it->second;
     }
-    if (cached) {
-        M.staged = cached < 0;
-        return set_tile(M, cached < 0 ? -cached : cached, s);
+    if (cached.first) {
+        M.form = cached.second;
+        return set_tile(M, cached.first, s);
     }
-    // Candidates: unstaged TILE 512 / 1024 / 2048 / 4096, staged TILE 1024 / 2048 (negative).
-    const int cands[6] = {512, 1024, 2048, 4096, -1024, -2048};
+    // Candidates (row-block size, form).
+    const std::pair<int, int> cands[] = {{512, kFormRows},  {1024, kFormRows}, {2048, kFormRows},
+                                         {4096, kFormRows},  {1024, kFormBulk}, {2048, kFormBulk}};
     cudaEvent_t e0, e1;
     FIIM_CUDA(cudaEventCreate(&e0));
     FIIM_CUDA(cudaEventCreate(&e1));
-    int best = only == 2 ? -2048 : 2048;
+    std::pair<int, int> best{0, 0};
     float best_ms = 1e30f;
     const int reps = M.nnz > 4000000 ? 5 : 10;
-    for (int c : cands) {
-        if ((only == 1 && c < 0) || (only == 2 && c > 0)) continue;
-        M.staged = c < 0;
-        FIIM_TRY(set_tile(M, c < 0 ? -c : c, s));
+    for (const auto &c : cands) {
+        if (only >= 0 && c.second != only) continue;
+        M.form = c.second;
+        FIIM_TRY(set_tile(M, c.first, s));
         FIIM_CUDA(launch_spmv(M, s, x, EpiStore{y}, nullptr, nullptr, fault));
         FIIM_CUDA(cudaEventRecord(e0, s));
         for (int r = 0; r < reps; ++r) FIIM_CUDA(launch_spmv(M, s, x, EpiStore{y}, nullptr, nullptr, fault));
@@ -295,7 +303,7 @@ static int autotune_tile(DevCsr &M, const double *x, double *y, cudaStream_t s, 
         FIIM_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
         FIIM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best_ms * 0.97f) {
+        if (!best.first || ms < best_ms * 0.97f) {
             best_ms = ms;
             best = c;
         }
@@ -306,8 +314,8 @@ static int autotune_tile(DevCsr &M, const double *x, double *y, cudaStream_t s, 
         std::lock_guard<std::mutex> lk(mu);
         cache[key] = best;
     }
-    M.staged = best < 0;
-    return set_tile(M, best < 0 ? -best : best, s);
+    M.form = best.second;
+    return set_tile(M, best.first, s);
 }
 
 // ------------------------------------------------------------------ host CSR helpers
@@ -440,10 +448,14 @@ int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, con
     return FIIM_OK;
 }
 
+// Column and value arrays get kStreamSlack bytes after their last entry: the staged SpMV
+// forms copy 16-byte aligned windows that may end up to 12 bytes past a block's last entry.
+constexpr size_t kStreamSlack = 16;
+
 int carve_csr(Arena &ar, DevCsr &M, long n, long nnz) {
     M.rp = static_cast<int *>(ar.take(sizeof(int) * (n + 1)));
-    M.ci = static_cast<int *>(ar.take(sizeof(int) * std::max<long>(nnz, 1)));
-    M.v = static_cast<double *>(ar.take(sizeof(double) * std::max<long>(nnz, 1)));
+    M.ci = static_cast<int *>(ar.take(sizeof(int) * std::max<long>(nnz, 1) + kStreamSlack));
+    M.v = static_cast<double *>(ar.take(sizeof(double) * std::max<long>(nnz, 1) + kStreamSlack));
     M.rb = static_cast<int *>(ar.take(sizeof(int) * 2 * (n + 1)));   // at most one block per row
     if (!M.rp || !M.ci || !M.v || !M.rb) return set_error(FIIM_ENOMEM, "arena exhausted");
     M.eb = M.rb + (n + 1);
@@ -452,8 +464,8 @@ int carve_csr(Arena &ar, DevCsr &M, long n, long nnz) {
 
 size_t csr_bytes(long n, long nnz) {
     return Arena::need(sizeof(int) * (n + 1)) + Arena::need(sizeof(int) * 2 * (n + 1)) +
-           Arena::need(sizeof(int) * std::max<long>(nnz, 1)) +
-           Arena::need(sizeof(double) * std::max<long>(nnz, 1));
+           Arena::need(sizeof(int) * std::max<long>(nnz, 1) + kStreamSlack) +
+           Arena::need(sizeof(double) * std::max<long>(nnz, 1) + kStreamSlack);
 }
 
 // ------------------------------------------------------------------ preconditioner
@@ -704,7 +716,7 @@ int Solver::create(int n_, const int *Ai, const int *Aj, const double *Av, const
         } else {
             // Deterministic shape: the same launch shape, hence the same reduction trees and
             // the same bits, in every process on the same GPU model.
-            M.staged = 0;
+            M.form = kFormRows;
             FIIM_TRY(set_tile(M, default_tile(M), stream));
         }
     }

@@ -206,11 +206,12 @@ class Solver:
     def device_bytes(self) -> int:
         return int(lib().fiim_solver_device_bytes(self._h))
 
-    def spmv_shape(self, which: int) -> int:
-        """Row-block size of matrix `which` (0 A, 1 G, 2 H); negative when bulk-copy staged."""
-        v = C.c_int(0)
-        _check(lib().fiim_solver_spmv_shape(self._h, C.c_int(which), C.byref(v)))
-        return v.value
+    def spmv_shape(self, which: int):
+        """(row-block size, form) of matrix `which` (0 A, 1 G, 2 H): form 0 streams through
+        registers, form 1 by bulk copies."""
+        t, f = C.c_int(0), C.c_int(0)
+        _check(lib().fiim_solver_spmv_shape(self._h, C.c_int(which), C.byref(t), C.byref(f)))
+        return t.value, f.value
 
     def apply(self, x, y, op="A"):
         """y = A x (op 'A') or y = M x (op 'M', the preconditioner) with the solver's kernels."""

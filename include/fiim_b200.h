@@ -130,9 +130,10 @@ int fiim_solver_solve(fiim_solver_t s, const double *b, double *x, double tol, i
 /* Bytes of device memory the solver holds. */
 int64_t fiim_solver_device_bytes(fiim_solver_t s);
 
-/* Row-block size (entries) of the CSR-stream SpMV for matrix `which` (0 A, 1 G, 2 H, 3 L,
-   4 U): positive for the register-staged form, negative for the bulk-copy-staged form. */
-int fiim_solver_spmv_shape(fiim_solver_t s, int which, int *shape);
+/* Row-block size (entries) and form of the CSR-stream SpMV for matrix `which` (0 A, 1 G,
+   2 H, 3 L, 4 U). Forms: 0 streams through registers, pipelined by one block; 1 bulk copies
+   into two shared-memory buffers. Both forms give the same bits. */
+int fiim_solver_spmv_shape(fiim_solver_t s, int which, int *tile, int *form);
 
 /* y = A x (op 0) or y = M x, the preconditioner application (op 1), with the solver's
  * own kernels; x, y in opt->memory space. Each row of every product is summed in
