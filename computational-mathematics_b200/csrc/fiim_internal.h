@@ -5,6 +5,7 @@
 #include <cuda_bf16.h>
 
 #include <cstdarg>
+#include <cstdlib>
 #include <algorithm>
 #include <cstddef>
 #include <map>
@@ -91,6 +92,33 @@ int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, con
 int set_tile(DevCsr &M, int tile, cudaStream_t s);
 void expand_sym_upper(int n, const int *rp, const int *ci, const double *v, HostCsr &out);
 void transpose_upper(int n, const int *rp, const int *ci, const double *v, HostCsr &out);
+
+// Launch a 256-thread kernel with programmatic stream serialization (programmatic
+// dependent launch: the kernel's CTAs may be scheduled while the previous kernel in the
+// stream finishes; the kernels wait for it with griddepcontrol.wait before touching its
+// results). FIIM_PDL=0 launches without the attribute.
+inline bool pdl_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("FIIM_PDL");
+        return !(e && e[0] == '0' && e[1] == 0);
+    }();
+    return on;
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_k(void (*kern)(KArgs...), int grid, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
 
 // Resident blocks per SM of a kernel launched with 256 threads, cached by kernel address.
 template <typename K>

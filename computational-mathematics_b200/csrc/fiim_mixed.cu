@@ -38,8 +38,8 @@ cudaError_t rows_f(cudaStream_t s, const DevCsr &M, const V *vals, const float *
                    DState *st, double *partials) {
     auto kern = mx::k_spmv_rows_f<TILE, V, Epi>;
     const int g = grid_for(kern, 1, M.nblk);
-    kern<<<g, kThreads, 0, s>>>(CsrView<V>{M.rp, M.ci, vals, (int)M.n}, M.rb, M.nblk, x, epi, st, partials);
-    return cudaGetLastError();
+    return launch_k(kern, g, 0, s, CsrView<V>{M.rp, M.ci, vals, (int)M.n}, M.rb, M.eb, M.nblk, x, epi, st,
+                    partials);
 }
 
 template <typename V, typename Epi>
@@ -108,16 +108,14 @@ struct MixedSolver : SolverBase {
         FIIM_CUDA(spmv_gh(H, false, p, mx::EpiScaleF{tm, D32}));
         FIIM_CUDA(spmv_gh(G, true, tm, mx::EpiNormF{pc}));
         FIIM_CUDA(spmv_f(A, A32, stream, pc, mx::EpiAlphaF{v, r0}, st, partials));
-        mx::k_update_s_f<<<sgrid(mx::k_update_s_f, nn), kThreads, 0, stream>>>(nn, r, v, e, s, st, partials);
-        FIIM_CUDA(cudaGetLastError());
+        FIIM_CUDA(launch_k(mx::k_update_s_f, sgrid(mx::k_update_s_f, nn), 0, stream, nn, r, v, e, s, st, partials));
         FIIM_CUDA(spmv_gh(H, false, s, mx::EpiScaleF{tm, D32}));
         FIIM_CUDA(spmv_gh(G, true, tm, mx::EpiStoreF{sc}));
         FIIM_CUDA(spmv_f(A, A32, stream, sc, mx::EpiOmegaF{t, s}, st, partials));
-        mx::k_update_xr_f<<<sgrid(mx::k_update_xr_f, nn), kThreads, 0, stream>>>(nn, pc, sc, s, t, r0, e, r, st,
-                                                                                   partials);
-        FIIM_CUDA(cudaGetLastError());
-        mx::k_update_p_f<<<sgrid(mx::k_update_p_f, nn), kThreads, 0, stream>>>(nn, r, v, p, st, h, cond ? 1 : 0);
-        FIIM_CUDA(cudaGetLastError());
+        FIIM_CUDA(launch_k(mx::k_update_xr_f, sgrid(mx::k_update_xr_f, nn), 0, stream, nn, pc, sc, s, t, r0, e, r,
+                           st, partials));
+        FIIM_CUDA(launch_k(mx::k_update_p_f, sgrid(mx::k_update_p_f, nn), 0, stream, nn, r, v, p, st, h,
+                           cond ? 1 : 0));
         return FIIM_OK;
     }
 

@@ -30,7 +30,10 @@ struct EpiScaleF {                 // y = d o (M x)
     FIIM_EPI(1, false, true);
     float *y;
     const float *__restrict__ d;
-    __device__ void emit(long i, float s, double (&)[NR]) const { y[i] = __ldg(d + i) * s; }
+    __device__ const float *pre_ptr() const { return d; }
+    __device__ float pre(long i) const { return __ldg(d + i); }
+    __device__ void emit_pre(long i, float s, float di, double (&)[NR]) const { y[i] = di * s; }
+    __device__ void emit(long i, float s, double (&r)[NR]) const { emit_pre(i, s, pre(i), r); }
     __device__ void finish(DState *, const double *) const {}
 };
 struct EpiNormF {                  // y = M x, ||y||^2 -> st->pc2
@@ -46,68 +49,126 @@ struct EpiAlphaF {                 // v = A pc, alpha = m1 / (r0 . v)
     FIIM_EPI(1, true, true);
     float *y;
     const float *__restrict__ r0;
-    __device__ void emit(long i, float s, double (&r)[NR]) const {
+    __device__ const float *pre_ptr() const { return r0; }
+    __device__ float pre(long i) const { return __ldg(r0 + i); }
+    __device__ void emit_pre(long i, float s, float r0i, double (&r)[NR]) const {
         y[i] = s;
-        r[0] += (double)__ldg(r0 + i) * (double)s;
+        r[0] += (double)r0i * (double)s;
     }
+    __device__ void emit(long i, float s, double (&r)[NR]) const { emit_pre(i, s, pre(i), r); }
     __device__ void finish(DState *st, const double *t) const { EpiAlpha{nullptr, nullptr}.finish(st, t); }
 };
 struct EpiOmegaF {                 // t = A sc, omega = (t . s) / (t . t)
     FIIM_EPI(2, true, true);
     float *y;
     const float *__restrict__ sv;
-    __device__ void emit(long i, float s, double (&r)[NR]) const {
+    __device__ const float *pre_ptr() const { return sv; }
+    __device__ float pre(long i) const { return __ldg(sv + i); }
+    __device__ void emit_pre(long i, float s, float si, double (&r)[NR]) const {
         y[i] = s;
-        r[0] += (double)s * (double)__ldg(sv + i);
+        r[0] += (double)s * (double)si;
         r[1] += (double)s * (double)s;
     }
+    __device__ void emit(long i, float s, double (&r)[NR]) const { emit_pre(i, s, pre(i), r); }
     __device__ void finish(DState *st, const double *t) const { EpiOmega{nullptr, nullptr}.finish(st, t); }
 };
 
 __device__ __forceinline__ float ldv(const float *p) { return __ldcs(p); }
 __device__ __forceinline__ float ldv(const __nv_bfloat16 *p) { return ldm(p); }
+__device__ __forceinline__ float2 ldv2(const float *p) { return __ldcs(reinterpret_cast<const float2 *>(p)); }
+__device__ __forceinline__ float2 ldv2(const __nv_bfloat16 *p) {
+    return __bfloat1622float2(__ldcs(reinterpret_cast<const __nv_bfloat162 *>(p)));
+}
 
-// CSR-stream SpMV on FP32 / BF16 values and an FP32 vector (same row blocks as the FP64
-// kernel; products staged in shared memory, each row summed in storage order).
+// CSR-stream SpMV on FP32 / BF16 values and an FP32 vector, with the FP64 kernel's row
+// blocks (at most TILE - 1 entries, bounds rb / eb) and structure: entries read in aligned
+// pairs, the next block's bounds, row offsets, entry streams and epilogue operands loaded
+// into registers before the barrier, products staged in shared memory, each row summed in
+// storage order.
 template <int TILE, typename V, typename Epi>
 static __global__ void __launch_bounds__(kThreads)
-k_spmv_rows_f(CsrView<V> M, const int *__restrict__ rb, int nblk, const float *__restrict__ x,
-              Epi epi, DState *st, double *__restrict__ partials) {
+k_spmv_rows_f(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, int nblk,
+              const float *__restrict__ x, Epi epi, DState *st, double *__restrict__ partials) {
+    pdl_enter();
     if (Epi::GATED && st != nullptr && st->done) return;
     __shared__ float prod[TILE];
+    constexpr int PER = TILE / kThreads;
+    const int tid = (int)threadIdx.x;
     double red[Epi::NR];
 #pragma unroll
     for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
+    int r0 = 0, r1 = 0, e0 = 0, e1 = 0, rbeg = 0, rend = 0;
+    float opnd = 0.f;
+    int c[PER];
+    float a[PER];
+    auto fetch = [&](int blk) {
+        r0 = __ldg(rb + blk);
+        r1 = __ldg(rb + blk + 1);
+        e0 = __ldg(eb + blk);
+        e1 = __ldg(eb + blk + 1);
+        rbeg = rend = 0;
+        if (r0 + tid < r1) {
+            rbeg = __ldg(M.rp + r0 + tid);
+            rend = __ldg(M.rp + r0 + tid + 1);
+            if constexpr (HasPre<Epi>::value) opnd = epi.pre(r0 + tid);
+        }
+        if (e1 - e0 < TILE) {
+            const int a0 = e0 & ~1;
+#pragma unroll
+            for (int u = 0; u < PER / 2; ++u) {
+                const int e = a0 + 2 * (tid + u * kThreads);
+                c[2 * u] = c[2 * u + 1] = 0;
+                a[2 * u] = a[2 * u + 1] = 0.f;
+                if (e + 1 < e1) {
+                    const int2 cc = ldi2(M.ci + e);
+                    const float2 aa = ldv2(M.v + e);
+                    c[2 * u] = cc.x;
+                    c[2 * u + 1] = cc.y;
+                    a[2 * u] = aa.x;
+                    a[2 * u + 1] = aa.y;
+                } else if (e < e1) {
+                    c[2 * u] = ldi(M.ci + e);
+                    a[2 * u] = ldv(M.v + e);
+                }
+            }
+        }
+    };
+    if ((int)blockIdx.x < nblk) fetch(blockIdx.x);
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
-        const int r0 = __ldg(rb + blk), r1 = __ldg(rb + blk + 1);
-        const int e0 = __ldg(M.rp + r0), e1 = __ldg(M.rp + r1);
-        if (e1 - e0 <= TILE) {
-#pragma unroll 4
-            for (int e = e0 + (int)threadIdx.x; e < e1; e += kThreads)
-                prod[e - e0] = ldv(M.v + e) * ldx(x + ldi(M.ci + e));
+        const int nxt = blk + (int)gridDim.x;
+        const int cr0 = r0, cr1 = r1, ce0 = e0, ce1 = e1, cb = rbeg - e0, ce = rend - e0;
+        const float copnd = opnd;
+        if (ce1 - ce0 < TILE) {
+            const int a0 = ce0 & ~1;
+#pragma unroll
+            for (int u = 0; u < PER; ++u) {
+                const int e = a0 + 2 * (tid + (u >> 1) * kThreads) + (u & 1);
+                if (e >= ce0 && e < ce1) prod[e - ce0] = a[u] * ldx(x + c[u]);
+            }
+            if (nxt < nblk) fetch(nxt);
             __syncthreads();
-            const int r = r0 + (int)threadIdx.x;
-            if (r < r1) {
-                const int b = __ldg(M.rp + r) - e0, e = __ldg(M.rp + r + 1) - e0;
+            if (cr0 + tid < cr1) {
                 float s = 0.f;
-                for (int k = b; k < e; ++k) s += prod[k];
-                epi.emit(r, s, red);
+                for (int k = cb; k < ce; ++k) s += prod[k];
+                if constexpr (HasPre<Epi>::value) epi.emit_pre(cr0 + tid, s, copnd, red);
+                else epi.emit(cr0 + tid, s, red);
             }
             __syncthreads();
         } else {
             float s = 0.f;
-            for (int c0 = e0; c0 < e1; c0 += TILE) {
-                const int c1 = min(c0 + TILE, e1);
-                for (int e = c0 + (int)threadIdx.x; e < c1; e += kThreads)
-                    prod[e - c0] = ldv(M.v + e) * ldx(x + ldi(M.ci + e));
+            for (int c0 = ce0; c0 < ce1; c0 += TILE) {
+                const int c1 = min(c0 + TILE, ce1);
+                for (int e = c0 + tid; e < c1; e += kThreads) prod[e - c0] = ldv(M.v + e) * ldx(x + ldi(M.ci + e));
                 __syncthreads();
-                if (threadIdx.x == 0)
+                if (tid == 0)
                     for (int k = 0; k < c1 - c0; ++k) s += prod[k];
                 __syncthreads();
             }
-            if (threadIdx.x == 0) epi.emit(r0, s, red);
+            if (tid == 0) epi.emit(cr0, s, red);
+            if (nxt < nblk) fetch(nxt);
         }
     }
+    pdl_release();
     if constexpr (Epi::REDUCES) grid_reduce<Epi::NR>(red, partials, st, epi);
 }
 
@@ -118,6 +179,7 @@ static __global__ void __launch_bounds__(kThreads)
 k_inner_init(long n, const double *__restrict__ r64, const DState *sto, float *__restrict__ r,
              float *__restrict__ r0, float *__restrict__ p, float *__restrict__ e, DState *st,
              double *__restrict__ partials) {
+    pdl_enter();
     const double inv = 1.0 / sqrt(sto->ts);
     double red[1] = {0.0};
     FIIM_FOR_ROWS(i, n) {
@@ -128,6 +190,7 @@ k_inner_init(long n, const double *__restrict__ r64, const DState *sto, float *_
         e[i] = 0.f;
         red[0] += (double)ri * (double)ri;
     }
+    pdl_release();
     grid_reduce<1>(red, partials, st, FinInit{});
 }
 
@@ -135,6 +198,7 @@ static __global__ void __launch_bounds__(kThreads)
 k_update_s_f(long n, const float *__restrict__ r, const float *__restrict__ v,
              const float *__restrict__ e, float *__restrict__ s, DState *st,
              double *__restrict__ partials) {
+    pdl_enter();
     if (st->done) return;
     const float na = (float)(-st->alpha);
     double red[2] = {0.0, 0.0};
@@ -144,6 +208,7 @@ k_update_s_f(long n, const float *__restrict__ r, const float *__restrict__ v,
         red[0] += (double)ri * (double)ri;
         red[1] += (double)ei * (double)ei;
     }
+    pdl_release();
     grid_reduce<2>(red, partials, st, FinS{});
 }
 
@@ -152,6 +217,7 @@ k_update_xr_f(long n, const float *__restrict__ pc, const float *__restrict__ sc
               const float *__restrict__ s, const float *__restrict__ t,
               const float *__restrict__ r0, float *__restrict__ e, float *__restrict__ r,
               DState *st, double *__restrict__ partials) {
+    pdl_enter();
     if (st->done) return;
     const float a = (float)st->alpha, om = (float)st->omega;
     double red[1] = {0.0};
@@ -161,12 +227,14 @@ k_update_xr_f(long n, const float *__restrict__ pc, const float *__restrict__ sc
         r[i] = ri;
         red[0] += (double)r0[i] * (double)ri;
     }
+    pdl_release();
     grid_reduce<1>(red, partials, st, FinControl{});
 }
 
 static __global__ void __launch_bounds__(kThreads)
 k_update_p_f(long n, const float *__restrict__ r, const float *__restrict__ v,
              float *__restrict__ p, DState *st, cudaGraphConditionalHandle h, int cond) {
+    pdl_enter();
     if (cond && blockIdx.x == 0 && threadIdx.x == 0) {
         const int loops = ++st->loops;
         if (!st->done && loops > st->nmax + 2) {
@@ -183,6 +251,7 @@ k_update_p_f(long n, const float *__restrict__ r, const float *__restrict__ v,
 // x += ||r64|| e (FP64): the refinement step.
 static __global__ void __launch_bounds__(kThreads)
 k_promote(long n, const float *__restrict__ e, double *__restrict__ x, const DState *sto) {
+    pdl_enter();
     const double scale = sqrt(sto->ts);
     FIIM_FOR_ROWS(i, n) { x[i] += scale * (double)e[i]; }
 }

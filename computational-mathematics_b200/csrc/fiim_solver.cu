@@ -105,30 +105,6 @@ void Arena::release() {
 size_t Arena::need(size_t bytes) { return (bytes + 255) & ~size_t(255); }
 
 // ------------------------------------------------------------------ launch shapes
-// Launch with programmatic stream serialization (PDL) unless FIIM_PDL=0.
-static bool pdl_enabled() {
-    static const bool on = [] {
-        const char *e = std::getenv("FIIM_PDL");
-        return !(e && std::strcmp(e, "0") == 0);
-    }();
-    return on;
-}
-
-template <typename... KArgs, typename... Args>
-static cudaError_t launch_k(void (*kern)(KArgs...), int grid, size_t smem, cudaStream_t s, Args... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(kThreads);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = pdl_enabled() ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
-}
-
 template <int VEC, int FILL, typename Epi>
 static cudaError_t spmv_vec(cudaStream_t s, const CsrView<double> &M, const double *x, const Epi &epi,
                             DState *st, double *partials) {
