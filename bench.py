@@ -29,6 +29,7 @@ import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 import numpy as np
@@ -78,24 +79,41 @@ class Clocks:
         self.p = None
 
     def __enter__(self):
+        # The sampler is started, and its first sample awaited, before the timed region: the
+        # start-up of nvidia-smi slows kernel launches for a moment.
+        self.lines = []
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "200"],
                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.p = None
+            return self
+        self.reader = threading.Thread(target=self._read, daemon=True)
+        self.reader.start()
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 5.0 and self.p.poll() is None:
+            time.sleep(0.02)
+        time.sleep(0.3)
+        self.skip = len(self.lines)
         return self
 
+    def _read(self):
+        for line in self.p.stdout:
+            if line.strip():
+                self.lines.append(line)
+
     def __exit__(self, *a):
-        self.lines = []
         if self.p:
             self.p.terminate()
             try:
-                out, _ = self.p.communicate(timeout=5)
+                self.p.wait(timeout=5)
             except Exception:
                 self.p.kill()
-                out = ""
-            self.lines = [l for l in out.splitlines() if l.strip()]
+            self.reader.join(timeout=5)
+            # keep the samples taken during the timed region (the warm-up ones, too, if
+            # the region was shorter than one sampling period)
+            self.lines = self.lines[self.skip:] or self.lines
 
     def summary(self):
         sm, mx, reasons = [], None, set()
@@ -528,10 +546,10 @@ def main():
     ap.add_argument("--ref-sample-its", type=int, default=10)
     ap.add_argument("--ref-iters", type=int, default=99,
                     help="iterations of the full 128^3 solve (the reference's own count, for scaling samples)")
-    # DRAM bytes per launch of the dominant kernel (H's SpMV) from the ncu capture summarised
-    # in profiles/spmv_rows_convdiff96_ncu_full.md (0.983 x algorithmic at 96^3), scaled to
-    # the 128^3 launch by units processed.
-    ap.add_argument("--ncu-traffic", type=float, default=325.6e6,
+    # DRAM bytes per launch of the dominant kernel (H's SpMV) from an ncu capture of the
+    # 96^3 case (read + write = 0.979 x its algorithmic bytes), scaled to the 128^3 launch by
+    # the units processed (entries and rows, which the traffic is proportional to).
+    ap.add_argument("--ncu-traffic", type=float, default=324.2e6,
                     help="dram bytes per launch of the dominant kernel from an ncu capture")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
