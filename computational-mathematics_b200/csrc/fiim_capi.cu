@@ -4,10 +4,14 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 #include <string>
 #include <vector>
+
+#include <algorithm>
 
 #include "fiim_b200.h"
 #include "fiim_internal.h"
@@ -16,11 +20,68 @@
 namespace {
 
 // Reference-facing calls reuse one solver per host thread while the problem shape is
-// unchanged, so repeated solves skip allocation, tuning and graph capture; the data
-// is uploaded again on every call, as the reference reads its arrays on every call.
+// unchanged, so repeated solves skip allocation, tuning and graph capture. The device
+// copies of the matrices and D^{-1} are also kept: each call stamps every input array
+// (address, size, 64-bit content hash) and uploads the arrays again only if a stamp
+// differs, so repeated solves with the same system upload only b and x0. The hash is
+// recomputed on every call, so arrays changed in place are seen. fiim_dropin_cache(0),
+// or FIIM_DROPIN_CACHE=0, uploads everything on every call instead.
+struct Stamp {
+    const void *p;
+    size_t bytes;
+    uint64_t h;
+    bool operator==(const Stamp &o) const { return p == o.p && bytes == o.bytes && h == o.h; }
+};
+
+// The splitmix64 finalizer (Steele, Lea and Flood, "Fast splittable pseudorandom number
+// generators", OOPSLA 2014), used as a mixing function.
+inline uint64_t mix64(uint64_t z) {
+    z ^= z >> 30;
+    z *= 0xbf58476d1ce4e5b9ULL;
+    z ^= z >> 27;
+    z *= 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+// Sum over 8-byte words of mix(word ^ position key): a change of any word, or a swap of
+// two, changes the sum by a pseudo-random 64-bit amount. Summed in parallel.
+uint64_t content_hash(const void *p, size_t bytes) {
+    const unsigned char *c = static_cast<const unsigned char *>(p);
+    const long nw = (long)(bytes / 8);
+    uint64_t acc = 0;
+#pragma omp parallel for reduction(+ : acc) schedule(static) if (nw > (1L << 16))
+    for (long i = 0; i < nw; ++i) {
+        uint64_t w;
+        std::memcpy(&w, c + 8 * i, 8);
+        acc += mix64(w ^ (0x9e3779b97f4a7c15ULL * (uint64_t)(i + 1)));
+    }
+    uint64_t tail = 0;
+    std::memcpy(&tail, c + 8 * nw, bytes - 8 * (size_t)nw);
+    return acc + mix64(tail ^ 0xd1b54a32d192ed03ULL) + mix64((uint64_t)bytes);
+}
+
+Stamp stamp(const void *p, size_t bytes) { return Stamp{p, bytes, p ? content_hash(p, bytes) : 0}; }
+
+void stamp_csr(std::vector<Stamp> &out, int n, const int *rp, const int *ci, const double *v) {
+    if (!rp) {
+        out.push_back(Stamp{nullptr, 0, 0});
+        return;
+    }
+    const size_t nnz = (size_t)std::max(rp[n], 0);
+    out.push_back(stamp(rp, sizeof(int) * (n + 1)));
+    out.push_back(stamp(ci, sizeof(int) * nnz));
+    out.push_back(stamp(v, sizeof(double) * nnz));
+}
+
+thread_local int g_cache = [] {
+    const char *e = std::getenv("FIIM_DROPIN_CACHE");
+    return (e && e[0] == '0' && e[1] == 0) ? 0 : 1;
+}();
+
 struct OneShot {
     fiim::Solver *s = nullptr;
     std::vector<long> key;
+    std::vector<Stamp> stamps;   // of the arrays now on the device (empty: unknown)
     ~OneShot() {
         if (s) {
             s->destroy();
@@ -49,11 +110,25 @@ int oneshot(int variant, int issym, char mode, int nr, int n, const double *Av, 
     std::vector<long> key = {variant, issym, (long)mode, combined ? nr : 1, n, Ai[n], Gi[n],
                              (!issym && Hi) ? Hi[n] : -1, (combined && Li) ? Li[n] : -1,
                              (combined && Ui) ? Ui[n] : -1};
-    int rc;
-    if (g_one.s && g_one.key == key && !issym) {
+    int rc = FIIM_OK;
+    std::vector<Stamp> st;
+    if (g_cache) {
+        stamp_csr(st, n, Ai, Aj, Av);
+        stamp_csr(st, n, Gi, Gj, Gv);
+        stamp_csr(st, n, Hi, Hj, Hv);
+        stamp_csr(st, n, combined ? Li : nullptr, Lj, Lv);
+        stamp_csr(st, n, combined ? Ui : nullptr, Uj, Uv);
+        st.push_back(stamp(IDv, sizeof(double) * n));
+    }
+    if (g_one.s && g_one.key == key && g_cache && !g_one.stamps.empty() && st == g_one.stamps) {
+        g_one.s->opt.verbose = verbose;   // the device copies are current
+    } else if (g_one.s && g_one.key == key && !issym) {
+        g_one.stamps.clear();
         g_one.s->opt.verbose = verbose;
         rc = g_one.s->reload(Ai, Aj, Av, Gi, Gj, Gv, IDv, Hi, Hj, Hv, Li, Lj, Lv, Ui, Uj, Uv);
+        if (rc == FIIM_OK) g_one.stamps = st;
     } else {
+        g_one.stamps.clear();
         if (g_one.s) {
             g_one.s->destroy();
             delete g_one.s;
@@ -68,6 +143,7 @@ int oneshot(int variant, int issym, char mode, int nr, int n, const double *Av, 
         }
         g_one.s = s;
         g_one.key = key;
+        g_one.stamps = st;
     }
     if (rc != FIIM_OK) return rc;
     fiim_result r{};
@@ -88,6 +164,13 @@ void throw_on(int rc) {
 extern "C" {
 
 const char *fiim_last_error(void) { return fiim::last_error(); }
+
+int fiim_dropin_cache(int enable) {
+    const int prev = g_cache;
+    g_cache = enable ? 1 : 0;
+    if (!g_cache) g_one.stamps.clear();
+    return prev;
+}
 
 void fiim_options_default(fiim_options *o) {
     if (!o) return;

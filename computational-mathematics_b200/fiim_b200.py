@@ -35,7 +35,7 @@ _PRECISIONS = {"fp64": FP64, "fp32": MIXED_FP32, "bf16": MIXED_BF16}
 
 # Every extern "C" symbol include/fiim_b200.h declares.
 EXPORTS = (
-    "fiim_last_error", "fiim_options_default", "fiim_EPBiCGSTAB_afiim", "fiim_EPBiCGSTAB_pdfiim",
+    "fiim_last_error", "fiim_dropin_cache", "fiim_options_default", "fiim_EPBiCGSTAB_afiim", "fiim_EPBiCGSTAB_pdfiim",
     "fiim_PBiCGSTAB_acifim", "fiim_solver_create", "fiim_solver_solve", "fiim_solver_device_bytes",
     "fiim_solver_spmv_shape", "fiim_solver_apply", "fiim_solver_kernel_times", "fiim_solver_iteration_bytes",
     "fiim_solver_destroy", "fiim_batch_create", "fiim_batch_solve", "fiim_batch_destroy",
@@ -109,6 +109,12 @@ def _ptr(a):
 
 
 # ----------------------------------------------------------------------------- drop-ins
+def dropin_cache(enable: bool) -> bool:
+    """Device-copy reuse of the drop-ins for this thread (on by default); returns the
+    previous setting."""
+    return bool(lib().fiim_dropin_cache(C.c_int(1 if enable else 0)))
+
+
 def EPBiCGSTAB(n, Av, Aj, Ai, b, tol, NMAX, Gv, Gj, Gi, IDv, Hv, Hj, Hi, x, verbose=0):
     """AFIIM EPBiCGSTAB on the GPU. x (float64, C-contiguous) is updated in place."""
     assert x.dtype == np.float64 and x.flags.c_contiguous

@@ -12,7 +12,10 @@
  *
  * Pointer spaces: the fiim_EPBiCGSTAB_* / fiim_PBiCGSTAB_* drop-ins take HOST arrays
  * and do the host->device upload, solve and download inside the call, as the
- * reference's blocking call does. The handle API (fiim_solver_*) takes host or
+ * reference's blocking call does. Each host thread keeps the device copies of its last
+ * system: a call stamps every matrix array and D^{-1} (address, size, 64-bit content
+ * hash, recomputed on every call) and uploads them again only when a stamp differs;
+ * b and x0 are uploaded on every call (see fiim_dropin_cache). The handle API (fiim_solver_*) takes host or
  * device arrays according to fiim_options.memory. The kernel-level entry points
  * (fiim_spmv, fiim_prec_apply) take DEVICE arrays and a cudaStream_t (as void*).
  */
@@ -48,6 +51,12 @@ extern "C" {
 
 /* Last error message of the calling thread (static storage, never NULL). */
 const char *fiim_last_error(void);
+
+/* Device-copy reuse of the drop-ins for the calling thread: enable != 0 (the default,
+ * unless FIIM_DROPIN_CACHE=0 is set) skips the upload of matrix arrays whose address,
+ * size and content hash are those of the previous call; 0 uploads every array on every
+ * call. Returns the previous setting. No counterpart in the reference. */
+int fiim_dropin_cache(int enable);
 
 /* ===========================================================================
  * Reference-facing drop-ins (host arrays).

@@ -228,6 +228,37 @@ def _forms_cache():
     return os.path.join(tempfile.gettempdir(), f"fiim_forms_{os.getpid()}.npy")
 
 
+def test_dropin_cache_follows_array_contents():
+    """Repeated drop-in calls reuse the device copies only while every matrix array keeps
+    its address, size and contents: a value changed in place is uploaded again, and the
+    result equals a call that uploads everything."""
+    A = FB.gen_convdiff3d(16, 0.5)
+    n = len(A[0]) - 1
+    b = FB.rand_normal(n, 7)
+    F = FB.pdfiim_build(A, 0.05, 2, 2, 1, -1, "I", "B")
+    G, H = (F["Gi"], F["Gj"], F["Gv"]), (F["Hi"], F["Hj"], F["Hv"])
+
+    def run():
+        x = np.zeros(n)
+        r = FB.EPBiCGSTAB_pdfiim(A, b, 1e-10, 500, G, F["IDv"], H, x)
+        return x, r
+
+    prev = FB.dropin_cache(True)
+    try:
+        x1, r1 = run()
+        x2, r2 = run()          # same arrays: no upload
+        assert np.array_equal(x1, x2) and r1 == r2
+        A[2][5] *= 1.5          # changed in place: same address and size
+        F["Hv"][7] *= 0.5
+        x3, r3 = run()
+        FB.dropin_cache(False)
+        x4, r4 = run()          # everything uploaded
+        assert np.array_equal(x3, x4) and r3 == r4
+        assert not np.array_equal(x3, x1)
+    finally:
+        FB.dropin_cache(prev)
+
+
 @pytest.mark.parametrize("memory", ["host", "device"])
 def test_handle_api_matches_dropin(golden, cuda, memory):
     import torch
