@@ -92,7 +92,7 @@ struct BatchSolver : SolverBase {
     cudaError_t spmv(const BMat &B, const V *vals, const double *xx, const Epi &epi) {
         auto kern = bt::k_bspmv<kTile, V, Epi>;
         const int g = sgrid(kern, B.M.nblk);
-        kern<<<g, kThreads, 0, stream>>>(CsrView<V>{B.M.rp, B.M.ci, vals, (int)B.M.n}, B.M.rb, B.blk_sys,
+        kern<<<g, kThreads, 0, stream>>>(CsrView<V>{B.M.rp, B.M.ci, vals, (int)B.M.n}, B.M.rb, B.M.eb, B.blk_sys,
                                          B.sys_blk, B.M.nblk, xx, epi, bs, partials);
         return cudaGetLastError();
     }
@@ -125,10 +125,13 @@ struct BatchSolver : SolverBase {
 
     int set_blocks(BMat &B) {
         std::vector<int> rb, bsys, sblk;
-        segment_blocks(B.M.hrp, sys_rows, kTile, kThreads, rb, bsys, sblk);
+        segment_blocks(B.M.hrp, sys_rows, kTile - 1, kThreads, rb, bsys, sblk);   // pairs: <= TILE - 1
         B.M.tile = kTile;
         B.M.nblk = (int)bsys.size();
+        std::vector<int> eb(rb.size());
+        for (size_t q = 0; q < rb.size(); ++q) eb[q] = B.M.hrp[rb[q]];
         FIIM_CUDA(cudaMemcpyAsync(B.M.rb, rb.data(), sizeof(int) * rb.size(), cudaMemcpyHostToDevice, stream));
+        FIIM_CUDA(cudaMemcpyAsync(B.M.eb, eb.data(), sizeof(int) * eb.size(), cudaMemcpyHostToDevice, stream));
         if (!bsys.empty())
             FIIM_CUDA(cudaMemcpyAsync(B.blk_sys, bsys.data(), sizeof(int) * bsys.size(), cudaMemcpyHostToDevice,
                                       stream));

@@ -2,7 +2,7 @@
 // block-diagonal CSR, each running the reference's BiCGSTAB (AFIIM/src/bicgstab.cpp:168-275
 // or ACIFIM/src/bicgstab.cpp:197-304) with its own scalars and termination.
 //
-// Row blocks (<= 256 rows, <= TILE entries) never straddle two systems. Every kernel walks
+// Row blocks (<= 256 rows, <= TILE - 1 entries) never straddle two systems. Every kernel walks
 // row blocks; a block of a system that has finished is skipped. Reductions are per system:
 // each row block reduces to one partial, and the last block of a system to finish (a
 // per-system ticket) adds that system's partials in block order and applies the system's
@@ -78,7 +78,9 @@ struct BEpiScale {
     FIIM_EPI(1, false, true);
     double *y;
     const double *__restrict__ d;
-    __device__ void emit(long i, double s, double (&)[NR]) const { y[i] = __dmul_rn(__ldg(d + i), s); }
+    __device__ double pre(long i) const { return __ldg(d + i); }
+    __device__ void emit_pre(long i, double s, double di, double (&)[NR]) const { y[i] = __dmul_rn(di, s); }
+    __device__ void emit(long i, double s, double (&r)[NR]) const { emit_pre(i, s, pre(i), r); }
     __device__ void finish(BState &, int, const double *) const {}
 };
 struct BEpiStore {
@@ -97,10 +99,12 @@ struct BEpiAlpha {
     FIIM_EPI(1, true, true);
     double *y;
     const double *__restrict__ r0;
-    __device__ void emit(long i, double s, double (&r)[NR]) const {
+    __device__ double pre(long i) const { return __ldg(r0 + i); }
+    __device__ void emit_pre(long i, double s, double r0i, double (&r)[NR]) const {
         y[i] = s;
-        r[0] += __ldg(r0 + i) * s;
+        r[0] += r0i * s;
     }
+    __device__ void emit(long i, double s, double (&r)[NR]) const { emit_pre(i, s, pre(i), r); }
     __device__ void finish(BState &bs, int k, const double *t) const {
         bs.alpha[k] = bs.m1[k] / t[0];
         if (bs.g->alpha_guard && !isfinite(bs.alpha[k])) {   // ACIFIM/src/bicgstab.cpp:208-213
@@ -113,11 +117,13 @@ struct BEpiOmega {
     FIIM_EPI(2, true, true);
     double *y;
     const double *__restrict__ sv;
-    __device__ void emit(long i, double s, double (&r)[NR]) const {
+    __device__ double pre(long i) const { return __ldg(sv + i); }
+    __device__ void emit_pre(long i, double s, double si, double (&r)[NR]) const {
         y[i] = s;
-        r[0] += s * __ldg(sv + i);
+        r[0] += s * si;
         r[1] += s * s;
     }
+    __device__ void emit(long i, double s, double (&r)[NR]) const { emit_pre(i, s, pre(i), r); }
     __device__ void finish(BState &bs, int k, const double *t) const { bs.omega[k] = t[0] / t[1]; }
 };
 struct BEpiInit {
@@ -213,48 +219,113 @@ __device__ __forceinline__ void block_to_system(double (&v)[NR], int blk, int k,
 __device__ __forceinline__ double widen(double v) { return v; }
 __device__ __forceinline__ double widen(float v) { return (double)v; }
 
+// Aligned pairs of matrix values: FP64 pairs as they are, FP32 and BF16 pairs as FP32 (held
+// in 4-byte registers until the product widens them).
+__device__ __forceinline__ double2 ldw2(const double *p) { return ldm2(p); }
+__device__ __forceinline__ float2 ldw2(const float *p) { return __ldcs(reinterpret_cast<const float2 *>(p)); }
+__device__ __forceinline__ float2 ldw2(const __nv_bfloat16 *p) {
+    return __bfloat1622float2(__ldcs(reinterpret_cast<const __nv_bfloat162 *>(p)));
+}
+
 // ---------------------------------------------------------------- batched CSR-stream SpMV
+// The single-system kernel's structure (k_spmv_rows): row blocks of at most TILE - 1
+// entries (first rows rb, first entries eb), entries read in aligned pairs, and the loop
+// pipelined by one block. The next block's system, bounds, row offsets, entry streams and
+// epilogue operand are loaded into registers before the barrier. A block whose system has
+// finished loads nothing and is skipped: a system's done flag changes only after all of its
+// blocks in the launch have been reduced, so the value read at prefetch is the one at use.
 template <int TILE, typename V, typename Epi>
-static __global__ void __launch_bounds__(kThreads)
-k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ blk_sys,
+static __global__ void __launch_bounds__(kThreads, 4)
+k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, const int *__restrict__ blk_sys,
         const int *__restrict__ sys_blk, int nblk, const double *__restrict__ x, Epi epi, BState bs,
         double *__restrict__ partials) {
     __shared__ double prod[TILE];
+    constexpr int PER = TILE / kThreads;
+    const int tid = (int)threadIdx.x;
+    int k = 0, r0 = 0, r1 = 0, e0 = 0, e1 = 0, rbeg = 0, rend = 0;
+    bool skip = false;
+    double opnd = 0.0;
+    using AV = typename std::conditional<std::is_same<V, double>::value, double, float>::type;
+    int c[PER];
+    AV a[PER];
+    auto fetch = [&](int blk) {
+        k = __ldg(blk_sys + blk);
+        r0 = __ldg(rb + blk);
+        r1 = __ldg(rb + blk + 1);
+        e0 = __ldg(eb + blk);
+        e1 = __ldg(eb + blk + 1);
+        skip = Epi::GATED && bs.done[k];
+        if (skip) return;
+        rbeg = rend = 0;
+        if (r0 + tid < r1) {
+            rbeg = __ldg(M.rp + r0 + tid);
+            rend = __ldg(M.rp + r0 + tid + 1);
+            if constexpr (HasPre<Epi>::value) opnd = epi.pre(r0 + tid);
+        }
+        if (e1 - e0 < TILE) {
+            const int a0 = e0 & ~1;
+#pragma unroll
+            for (int u = 0; u < PER / 2; ++u) {
+                const int e = a0 + 2 * (tid + u * kThreads);
+                c[2 * u] = c[2 * u + 1] = 0;
+                a[2 * u] = a[2 * u + 1] = AV(0);
+                if (e + 1 < e1) {
+                    const int2 cc = ldi2(M.ci + e);
+                    const auto aa = ldw2(M.v + e);
+                    c[2 * u] = cc.x;
+                    c[2 * u + 1] = cc.y;
+                    a[2 * u] = aa.x;
+                    a[2 * u + 1] = aa.y;
+                } else if (e < e1) {
+                    c[2 * u] = ldi(M.ci + e);
+                    a[2 * u] = ldm(M.v + e);
+                }
+            }
+        }
+    };
+    if ((int)blockIdx.x < nblk) fetch(blockIdx.x);
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
-        const int k = __ldg(blk_sys + blk);
-        if (Epi::GATED && bs.done[k]) continue;           // uniform in the CTA
+        const int nxt = blk + (int)gridDim.x;
+        const int ck = k, cr0 = r0, cr1 = r1, ce0 = e0, ce1 = e1, cb = rbeg - e0, ce = rend - e0;
+        const double copnd = opnd;
+        if (skip) {                                         // uniform in the CTA
+            if (nxt < nblk) fetch(nxt);
+            continue;
+        }
         double red[Epi::NR];
 #pragma unroll
         for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
-        const int r0 = __ldg(rb + blk), r1 = __ldg(rb + blk + 1);
-        const int e0 = __ldg(M.rp + r0), e1 = __ldg(M.rp + r1);
-        if (e1 - e0 <= TILE) {
-#pragma unroll 4
-            for (int e = e0 + (int)threadIdx.x; e < e1; e += kThreads)
-                prod[e - e0] = __dmul_rn(widen(ldm(M.v + e)), ldx(x + ldi(M.ci + e)));
+        if (ce1 - ce0 < TILE) {
+            const int a0 = ce0 & ~1;
+#pragma unroll
+            for (int u = 0; u < PER; ++u) {
+                const int e = a0 + 2 * (tid + (u >> 1) * kThreads) + (u & 1);
+                if (e >= ce0 && e < ce1) prod[e - ce0] = __dmul_rn(widen(a[u]), ldx(x + c[u]));
+            }
+            if (nxt < nblk) fetch(nxt);
             __syncthreads();
-            const int r = r0 + (int)threadIdx.x;
-            if (r < r1) {
-                const int b = __ldg(M.rp + r) - e0, e = __ldg(M.rp + r + 1) - e0;
+            if (cr0 + tid < cr1) {
                 double s = 0.0;
-                for (int q = b; q < e; ++q) s = __dadd_rn(s, prod[q]);
-                epi.emit(r, s, red);
+                for (int q = cb; q < ce; ++q) s = __dadd_rn(s, prod[q]);
+                if constexpr (HasPre<Epi>::value) epi.emit_pre(cr0 + tid, s, copnd, red);
+                else epi.emit(cr0 + tid, s, red);
             }
             __syncthreads();
         } else {
             double s = 0.0;
-            for (int c0 = e0; c0 < e1; c0 += TILE) {
-                const int c1 = min(c0 + TILE, e1);
-                for (int e = c0 + (int)threadIdx.x; e < c1; e += kThreads)
+            for (int c0 = ce0; c0 < ce1; c0 += TILE) {
+                const int c1 = min(c0 + TILE, ce1);
+                for (int e = c0 + tid; e < c1; e += kThreads)
                     prod[e - c0] = __dmul_rn(widen(ldm(M.v + e)), ldx(x + ldi(M.ci + e)));
                 __syncthreads();
-                if (threadIdx.x == 0)
+                if (tid == 0)
                     for (int q = 0; q < c1 - c0; ++q) s = __dadd_rn(s, prod[q]);
                 __syncthreads();
             }
-            if (threadIdx.x == 0) epi.emit(r0, s, red);
+            if (tid == 0) epi.emit(cr0, s, red);
+            if (nxt < nblk) fetch(nxt);
         }
-        if constexpr (Epi::REDUCES) block_to_system<Epi::NR>(red, blk, k, sys_blk, partials, bs, epi);
+        if constexpr (Epi::REDUCES) block_to_system<Epi::NR>(red, blk, ck, sys_blk, partials, bs, epi);
     }
 }
 
