@@ -5,7 +5,8 @@
 // Each system runs the reference's loop with its own scalars, divergence window
 // (min(max(n_k,500)/50,20), or min(max(n_k,2000)/50,40) for ACIFIM) and termination; a
 // finished system's row blocks are skipped. One CUDA graph with a WHILE node runs the
-// nine batched kernels until no system is active.
+// batched loop body (nine passes plus five per-system finish kernels) until no system is
+// active.
 //
 // Layout: CSR per matrix + row blocks aligned to systems (blk_sys, sys_blk); factor values
 // FP64, FP32 or BF16 (fiim_options.precision); A, D^-1 and all vectors FP64; per-system
@@ -16,6 +17,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -86,6 +88,7 @@ struct BatchSolver : SolverBase {
     unsigned long long *d_count = nullptr, *h_count = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    bool host_loop = false;          // FIIM_GRAPH=host: the host relaunches a one-iteration graph
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
     template <typename V, typename Epi>
@@ -103,20 +106,33 @@ struct BatchSolver : SolverBase {
         return spmv(B, B.M.v, xx, epi);
     }
 
+    // Second phase of a per-system reduction over matrix B's row blocks (bt::k_bfinish).
+    template <int NR, bool GATED = true, class Fin>
+    cudaError_t finish(const BMat &B, const Fin &fin) {
+        const int g = (int)std::min<long>(((long)nsys * 32 + kThreads - 1) / kThreads, 8L * num_sms());
+        bt::k_bfinish<NR, GATED, Fin><<<g, kThreads, 0, stream>>>(B.sys_blk, nsys, partials, bs, fin);
+        return cudaGetLastError();
+    }
+
     int enqueue_iteration(bool cond, cudaGraphConditionalHandle h) {
         const int nb = A.M.nblk;
         FIIM_CUDA(spmv_f(H, p, bt::BEpiScale{tm, IDv}));
         FIIM_CUDA(spmv_f(G, tm, bt::BEpiNorm{pc}));
+        FIIM_CUDA(finish<1>(G, bt::BEpiNorm{pc}));
         FIIM_CUDA(spmv(A, A.M.v, pc, bt::BEpiAlpha{v, r0}));
+        FIIM_CUDA(finish<1>(A, bt::BEpiAlpha{v, r0}));
         bt::k_bupdate_s<<<sgrid(bt::k_bupdate_s, nb), kThreads, 0, stream>>>(A.M.rb, A.blk_sys, A.sys_blk, nb, r, v,
                                                                              x, sv, bs, partials);
         FIIM_CUDA(cudaGetLastError());
+        FIIM_CUDA(finish<2>(A, bt::BFinS{}));
         FIIM_CUDA(spmv_f(H, sv, bt::BEpiScale{tm, IDv}));
         FIIM_CUDA(spmv_f(G, tm, bt::BEpiStore{sc}));
         FIIM_CUDA(spmv(A, A.M.v, sc, bt::BEpiOmega{t, sv}));
+        FIIM_CUDA(finish<2>(A, bt::BEpiOmega{t, sv}));
         bt::k_bupdate_xr<<<sgrid(bt::k_bupdate_xr, nb), kThreads, 0, stream>>>(A.M.rb, A.blk_sys, A.sys_blk, nb, pc,
                                                                                sc, sv, t, r0, x, r, bs, partials);
         FIIM_CUDA(cudaGetLastError());
+        FIIM_CUDA(finish<1>(A, bt::BFinControl{}));
         bt::k_bupdate_p<<<sgrid(bt::k_bupdate_p, nb), kThreads, 0, stream>>>(A.M.rb, A.blk_sys, nb, r, v, p, bs, h,
                                                                              cond ? 1 : 0);
         FIIM_CUDA(cudaGetLastError());
@@ -185,7 +201,6 @@ struct BatchSolver : SolverBase {
         bytes += 3 * 2 * Arena::need(sizeof(int) * (N + nsys + 1));        // blk_sys, sys_blk
         if (f32 || f16) bytes += Arena::need(vsz * std::max<long>(nG, 1)) + Arena::need(vsz * std::max<long>(nH, 1));
         bytes += 12 * Arena::need(sizeof(double) * N);
-        bytes += Arena::need(sizeof(double) * 2 * (N + nsys + 8));          // partials: <= 2 per block
         bytes += 12 * Arena::need(sizeof(double) * nsys) + 7 * Arena::need(sizeof(int) * nsys);
         bytes += Arena::need(sizeof(bt::BGlobal)) + 4096;
         FIIM_TRY(arena.reserve(bytes));
@@ -206,7 +221,6 @@ struct BatchSolver : SolverBase {
         double **vecs[] = {&IDv, &x, &b, &r, &r0, &p, &v, &sv, &t, &pc, &sc, &tm};
         for (auto pp : vecs)
             if (!(*pp = static_cast<double *>(arena.take(sizeof(double) * N)))) return set_error(FIIM_ENOMEM, "arena");
-        partials = static_cast<double *>(arena.take(sizeof(double) * 2 * (N + nsys + 8)));
         double **ds[] = {&bs.ro, &bs.rc, &bs.m1, &bs.m2, &bs.alpha, &bs.omega, &bs.beta, &bs.pc2, &bs.x2, &bs.r2,
                          &bs.ts, &bs.tt};
         for (auto pp : ds)
@@ -214,10 +228,9 @@ struct BatchSolver : SolverBase {
         int **is[] = {&bs.iter, &bs.stag, &bs.msteps, &bs.maxmsteps, &bs.info, &bs.done};
         for (auto pp : is)
             if (!(*pp = static_cast<int *>(arena.take(sizeof(int) * nsys)))) return set_error(FIIM_ENOMEM, "arena");
-        bs.ticket = static_cast<unsigned int *>(arena.take(sizeof(unsigned int) * nsys));
         bs.g = static_cast<bt::BGlobal *>(arena.take(sizeof(bt::BGlobal)));
         d_count = static_cast<unsigned long long *>(arena.take(sizeof(unsigned long long)));
-        if (!partials || !bs.ticket || !bs.g || !d_count) return set_error(FIIM_ENOMEM, "arena exhausted");
+        if (!bs.g || !d_count) return set_error(FIIM_ENOMEM, "arena exhausted");
         FIIM_CUDA(cudaHostAlloc(&hg, sizeof(bt::BGlobal) + 64, cudaHostAllocDefault));
         h_count = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(hg) + sizeof(bt::BGlobal) + 32);
 
@@ -235,6 +248,9 @@ struct BatchSolver : SolverBase {
             FIIM_CUDA(cudaGetLastError());
         }
         for (int m = 0; m < 3; ++m) FIIM_TRY(set_blocks(*mats[m]));
+        // Per-warp partials of the largest block count (two values each).
+        const long maxblk = std::max({(long)A.M.nblk, (long)G.M.nblk, (long)H.M.nblk, 1L});
+        FIIM_CUDA(cudaMalloc(&partials, sizeof(double) * 2 * kWarps * maxblk));
         // per-system divergence windows (AFIIM/src/bicgstab.cpp:114, ACIFIM/src/bicgstab.cpp:132)
         std::vector<int> mm(nsys);
         for (int k = 0; k < nsys; ++k) {
@@ -243,7 +259,6 @@ struct BatchSolver : SolverBase {
                                                  : std::min(std::max(nk, 500) / 50, 20);
         }
         FIIM_CUDA(cudaMemcpyAsync(bs.maxmsteps, mm.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, stream));
-        FIIM_CUDA(cudaMemsetAsync(bs.ticket, 0, sizeof(unsigned int) * nsys, stream));
         FIIM_CUDA(cudaStreamSynchronize(stream));
         return build_graph();
     }
@@ -262,7 +277,6 @@ struct BatchSolver : SolverBase {
         FIIM_CUDA(cudaMemcpyAsync(bs.g, hg, sizeof(bt::BGlobal), cudaMemcpyHostToDevice, stream));
         FIIM_CUDA(cudaMemsetAsync(bs.done, 0, sizeof(int) * nsys, stream));
         FIIM_CUDA(cudaMemsetAsync(bs.info, 0xff, sizeof(int) * nsys, stream));   // -1
-        FIIM_CUDA(cudaMemsetAsync(bs.ticket, 0, sizeof(unsigned int) * nsys, stream));
         return FIIM_OK;
     }
 
@@ -273,6 +287,21 @@ struct BatchSolver : SolverBase {
         FIIM_CUDA(cudaMemcpyAsync(bs.done, ones.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, stream));
         FIIM_TRY(enqueue_iteration(false, cudaGraphConditionalHandle{}));
         FIIM_CUDA(cudaStreamSynchronize(stream));
+        // FIIM_GRAPH=host: a graph of one loop iteration, relaunched by the host (the same
+        // kernels and shapes; for profilers that replay graph kernel nodes one by one).
+        const char *mode_env = std::getenv("FIIM_GRAPH");
+        if (mode_env && std::strcmp(mode_env, "host") == 0) {
+            FIIM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            const int rc = enqueue_iteration(false, cudaGraphConditionalHandle{});
+            cudaGraph_t g1 = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(stream, &g1);
+            if (rc != FIIM_OK) return rc;
+            FIIM_CUDA(ec);
+            FIIM_CUDA(cudaGraphInstantiate(&exec, g1, 0));
+            graph = g1;
+            host_loop = true;
+            return FIIM_OK;
+        }
         cudaGraph_t g = nullptr;
         FIIM_CUDA(cudaGraphCreate(&g, 0));
         cudaGraphConditionalHandle h;
@@ -306,8 +335,26 @@ struct BatchSolver : SolverBase {
         FIIM_CUDA(cudaMemcpyAsync(x, x_io, sizeof(double) * N, kin, stream));
         FIIM_TRY(reset_state(tol, nmax));
         FIIM_CUDA(spmv(A, A.M.v, x, bt::BEpiInit{b, p, r0, r}));
-        FIIM_CUDA(cudaGraphLaunch(exec, stream));
+        FIIM_CUDA(finish<1>(A, bt::BEpiInit{b, p, r0, r}));
+        if (!host_loop) {
+            FIIM_CUDA(cudaGraphLaunch(exec, stream));
+        } else {
+            int launched = 0, chunk = 1;
+            for (;;) {
+                for (int q = 0; q < chunk; ++q) FIIM_CUDA(cudaGraphLaunch(exec, stream));
+                launched += chunk;
+                FIIM_CUDA(cudaMemcpyAsync(hg, bs.g, sizeof(bt::BGlobal), cudaMemcpyDeviceToHost, stream));
+                FIIM_CUDA(cudaStreamSynchronize(stream));
+                if (hg->active <= 0) break;
+                if (launched > std::max(nmax, 0) + 2)
+                    return set_error(FIIM_ETIMEOUT, "batch not finished after %d iterations", launched);
+                chunk = std::min(chunk * 2, 16);
+            }
+            hg->loops = launched;
+            FIIM_CUDA(cudaMemcpyAsync(&bs.g->loops, &hg->loops, sizeof(int), cudaMemcpyHostToDevice, stream));
+        }
         FIIM_CUDA(spmv(A, A.M.v, x, bt::BEpiResid{b}));
+        FIIM_CUDA((finish<2, false>(A, bt::BEpiResid{b})));
         FIIM_CUDA(cudaMemcpyAsync(x_io, x, sizeof(double) * N, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                                   stream));
         FIIM_CUDA(cudaEventRecord(ev1, stream));
@@ -343,7 +390,7 @@ struct BatchSolver : SolverBase {
             summary->true_relres = worst_rel;
             summary->refine_steps = 0;
             summary->device_ms = ms;
-            summary->launches = 2 + hg->loops * 9;
+            summary->launches = 4 + hg->loops * 14;
         }
         return FIIM_OK;
     }
@@ -356,6 +403,8 @@ struct BatchSolver : SolverBase {
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
         if (hg) cudaFreeHost(hg);
+        if (partials) cudaFree(partials);
+        partials = nullptr;
         exec = nullptr;
         graph = nullptr;
         ev0 = ev1 = nullptr;

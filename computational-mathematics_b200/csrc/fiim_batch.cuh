@@ -4,10 +4,10 @@
 //
 // Row blocks (<= 256 rows, <= TILE - 1 entries) never straddle two systems. Every kernel walks
 // row blocks; a block of a system that has finished is skipped. Reductions are per system:
-// each row block reduces to one partial, and the last block of a system to finish (a
-// per-system ticket) adds that system's partials in block order and applies the system's
-// scalar step. Vectors are FP64; factor values may be FP64, FP32 or BF16 (widened to FP64
-// before the rounded product), so every vector operation is the reference's, bit for bit,
+// each warp of each row block stores one partial, and a finish kernel (one warp per system)
+// adds a system's partials in a fixed order and applies the system's scalar step. Vectors
+// are FP64; factor values may be FP64, FP32 or BF16 (widened to FP64 before the rounded
+// product), so every vector operation is the reference's, bit for bit,
 // on the factors as stored.
 #pragma once
 
@@ -25,7 +25,7 @@ struct BGlobal {
 struct BState {
     double *ro, *rc, *m1, *m2, *alpha, *omega, *beta, *pc2, *x2, *r2, *ts, *tt;
     int *iter, *stag, *msteps, *maxmsteps, *info, *done;
-    unsigned int *ticket;
+    unsigned int *ticket;   // per-system tickets (the block solver's last-CTA reductions)
     BGlobal *g;
 };
 
@@ -154,66 +154,40 @@ struct BEpiResid {
 };
 
 // ---------------------------------------------------------------- per-system reduction
-// Called by every thread of the CTA once per row block (uniformly). Reduces `v` over the
-// CTA, stores the block's partial, and, in the last block of system k, adds the system's
-// partials in block order and runs fin.finish(bs, k, totals).
-template <int NR, class Fin>
-__device__ __forceinline__ void block_to_system(double (&v)[NR], int blk, int k,
-                                                const int *__restrict__ sys_blk,
-                                                double *__restrict__ partials, BState &bs,
-                                                const Fin &fin) {
-    __shared__ double sm[kWarps][NR];
-    __shared__ int last;
+// Two phases. In a reducing kernel every warp of every row block stores its partial (lane 0,
+// after the warp's shuffle tree): no CTA barrier, fence or atomic per block. A finish kernel
+// then gives each system one warp, which adds the system's partials (blocks in order,
+// lane-strided, then the shuffle tree: a fixed order) and applies the system's scalar step.
+// Partials: (block * kWarps + warp) * NR + j.
+template <int NR>
+__device__ __forceinline__ void warp_partials(double (&v)[NR], int blk, double *__restrict__ partials) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
     for (int j = 0; j < NR; ++j) v[j] = warp_sum(v[j]);
     if (lane == 0)
 #pragma unroll
-        for (int j = 0; j < NR; ++j) sm[w][j] = v[j];
-    __syncthreads();
-    const int b0 = __ldg(sys_blk + k), b1 = __ldg(sys_blk + k + 1);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int j = 0; j < NR; ++j) {
-            double s = 0.0;
-#pragma unroll
-            for (int q = 0; q < kWarps; ++q) s += sm[q][j];
-            partials[(size_t)blk * NR + j] = s;
-        }
-        __threadfence();
-        const unsigned t = atomicAdd(&bs.ticket[k], 1u);
-        last = (t == (unsigned)(b1 - b0 - 1));
-    }
-    __syncthreads();
-    if (last) {
-        __threadfence();
+        for (int j = 0; j < NR; ++j) partials[((size_t)blk * kWarps + w) * NR + j] = v[j];
+}
+
+// One warp per system: systems whose loop has ended are left alone when GATED.
+template <int NR, bool GATED, class Fin>
+static __global__ void __launch_bounds__(kThreads)
+k_bfinish(const int *__restrict__ sys_blk, int nsys, const double *__restrict__ partials, BState bs, Fin fin) {
+    const int lane = threadIdx.x & 31;
+    const int nw = (int)(gridDim.x * blockDim.x) >> 5;
+    for (int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < nsys; k += nw) {
+        if (GATED && bs.done[k]) continue;             // uniform in the warp
+        const int q0 = __ldg(sys_blk + k) * kWarps, q1 = __ldg(sys_blk + k + 1) * kWarps;
         double acc[NR];
 #pragma unroll
         for (int j = 0; j < NR; ++j) acc[j] = 0.0;
-        for (int q = b0 + (int)threadIdx.x; q < b1; q += kThreads)
+        for (int q = q0 + lane; q < q1; q += 32)
 #pragma unroll
-            for (int j = 0; j < NR; ++j) acc[j] += __ldcg(partials + (size_t)q * NR + j);
+            for (int j = 0; j < NR; ++j) acc[j] += partials[(size_t)q * NR + j];
 #pragma unroll
         for (int j = 0; j < NR; ++j) acc[j] = warp_sum(acc[j]);
-        __syncthreads();
-        if (lane == 0)
-#pragma unroll
-            for (int j = 0; j < NR; ++j) sm[w][j] = acc[j];
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double tot[NR];
-#pragma unroll
-            for (int j = 0; j < NR; ++j) {
-                double s = 0.0;
-#pragma unroll
-                for (int q = 0; q < kWarps; ++q) s += sm[q][j];
-                tot[j] = s;
-            }
-            bs.ticket[k] = 0u;
-            fin.finish(bs, k, tot);
-        }
+        if (lane == 0) fin.finish(bs, k, acc);
     }
-    __syncthreads();
 }
 
 __device__ __forceinline__ double widen(double v) { return v; }
@@ -325,7 +299,7 @@ k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, co
             if (tid == 0) epi.emit(cr0, s, red);
             if (nxt < nblk) fetch(nxt);
         }
-        if constexpr (Epi::REDUCES) block_to_system<Epi::NR>(red, blk, ck, sys_blk, partials, bs, epi);
+        if constexpr (Epi::REDUCES) warp_partials<Epi::NR>(red, blk, partials);
     }
 }
 
@@ -346,7 +320,7 @@ k_bupdate_s(const int *__restrict__ rb, const int *__restrict__ blk_sys, const i
             red[0] = ri * ri;
             red[1] = xi * xi;
         }
-        block_to_system<2>(red, blk, k, sys_blk, partials, bs, BFinS{});
+        warp_partials<2>(red, blk, partials);
     }
 }
 
@@ -370,7 +344,7 @@ k_bupdate_xr(const int *__restrict__ rb, const int *__restrict__ blk_sys, const 
             r[row] = ri;
             red[0] = r0[row] * ri;
         }
-        block_to_system<1>(red, blk, k, sys_blk, partials, bs, BFinControl{});
+        warp_partials<1>(red, blk, partials);
     }
 }
 
