@@ -95,9 +95,8 @@ struct BatchSolver : SolverBase {
     cudaError_t spmv(const BMat &B, const V *vals, const double *xx, const Epi &epi) {
         auto kern = bt::k_bspmv<kTile, V, Epi>;
         const int g = sgrid(kern, B.M.nblk);
-        kern<<<g, kThreads, 0, stream>>>(CsrView<V>{B.M.rp, B.M.ci, vals, (int)B.M.n}, B.M.rb, B.M.eb, B.blk_sys,
-                                         B.sys_blk, B.M.nblk, xx, epi, bs, partials);
-        return cudaGetLastError();
+        return launch_k(kern, g, 0, stream, CsrView<V>{B.M.rp, B.M.ci, vals, (int)B.M.n}, B.M.rb, B.M.eb, B.blk_sys,
+                        B.sys_blk, B.M.nblk, xx, epi, bs, partials);
     }
     template <typename Epi>
     cudaError_t spmv_f(const BMat &B, const double *xx, const Epi &epi) {   // factors: stored precision
@@ -110,8 +109,7 @@ struct BatchSolver : SolverBase {
     template <int NR, bool GATED = true, class Fin>
     cudaError_t finish(const BMat &B, const Fin &fin) {
         const int g = (int)std::min<long>(((long)nsys * 32 + kThreads - 1) / kThreads, 8L * num_sms());
-        bt::k_bfinish<NR, GATED, Fin><<<g, kThreads, 0, stream>>>(B.sys_blk, nsys, partials, bs, fin);
-        return cudaGetLastError();
+        return launch_k(bt::k_bfinish<NR, GATED, Fin>, g, 0, stream, B.sys_blk, nsys, partials, bs, fin);
     }
 
     int enqueue_iteration(bool cond, cudaGraphConditionalHandle h) {
@@ -121,21 +119,18 @@ struct BatchSolver : SolverBase {
         FIIM_CUDA(finish<1>(G, bt::BEpiNorm{pc}));
         FIIM_CUDA(spmv(A, A.M.v, pc, bt::BEpiAlpha{v, r0}));
         FIIM_CUDA(finish<1>(A, bt::BEpiAlpha{v, r0}));
-        bt::k_bupdate_s<<<sgrid(bt::k_bupdate_s, nb), kThreads, 0, stream>>>(A.M.rb, A.blk_sys, A.sys_blk, nb, r, v,
-                                                                             x, sv, bs, partials);
-        FIIM_CUDA(cudaGetLastError());
+        FIIM_CUDA(launch_k(bt::k_bupdate_s, sgrid(bt::k_bupdate_s, nb), 0, stream, A.M.rb, A.blk_sys, A.sys_blk,
+                           nb, r, v, x, sv, bs, partials));
         FIIM_CUDA(finish<2>(A, bt::BFinS{}));
         FIIM_CUDA(spmv_f(H, sv, bt::BEpiScale{tm, IDv}));
         FIIM_CUDA(spmv_f(G, tm, bt::BEpiStore{sc}));
         FIIM_CUDA(spmv(A, A.M.v, sc, bt::BEpiOmega{t, sv}));
         FIIM_CUDA(finish<2>(A, bt::BEpiOmega{t, sv}));
-        bt::k_bupdate_xr<<<sgrid(bt::k_bupdate_xr, nb), kThreads, 0, stream>>>(A.M.rb, A.blk_sys, A.sys_blk, nb, pc,
-                                                                               sc, sv, t, r0, x, r, bs, partials);
-        FIIM_CUDA(cudaGetLastError());
+        FIIM_CUDA(launch_k(bt::k_bupdate_xr, sgrid(bt::k_bupdate_xr, nb), 0, stream, A.M.rb, A.blk_sys, A.sys_blk,
+                           nb, pc, sc, sv, t, r0, x, r, bs, partials));
         FIIM_CUDA(finish<1>(A, bt::BFinControl{}));
-        bt::k_bupdate_p<<<sgrid(bt::k_bupdate_p, nb), kThreads, 0, stream>>>(A.M.rb, A.blk_sys, nb, r, v, p, bs, h,
-                                                                             cond ? 1 : 0);
-        FIIM_CUDA(cudaGetLastError());
+        FIIM_CUDA(launch_k(bt::k_bupdate_p, sgrid(bt::k_bupdate_p, nb), 0, stream, A.M.rb, A.blk_sys, nb, r, v, p,
+                           bs, h, cond ? 1 : 0));
         return FIIM_OK;
     }
 

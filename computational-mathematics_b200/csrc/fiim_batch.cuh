@@ -173,6 +173,7 @@ __device__ __forceinline__ void warp_partials(double (&v)[NR], int blk, double *
 template <int NR, bool GATED, class Fin>
 static __global__ void __launch_bounds__(kThreads)
 k_bfinish(const int *__restrict__ sys_blk, int nsys, const double *__restrict__ partials, BState bs, Fin fin) {
+    pdl_enter();
     const int lane = threadIdx.x & 31;
     const int nw = (int)(gridDim.x * blockDim.x) >> 5;
     for (int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < nsys; k += nw) {
@@ -213,6 +214,7 @@ static __global__ void __launch_bounds__(kThreads, 4)
 k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, const int *__restrict__ blk_sys,
         const int *__restrict__ sys_blk, int nblk, const double *__restrict__ x, Epi epi, BState bs,
         double *__restrict__ partials) {
+    pdl_enter();
     __shared__ double prod[TILE];
     constexpr int PER = TILE / kThreads;
     const int tid = (int)threadIdx.x;
@@ -301,6 +303,7 @@ k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, co
         }
         if constexpr (Epi::REDUCES) warp_partials<Epi::NR>(red, blk, partials);
     }
+    pdl_release();
 }
 
 // ---------------------------------------------------------------- batched vector updates
@@ -309,6 +312,7 @@ static __global__ void __launch_bounds__(kThreads)
 k_bupdate_s(const int *__restrict__ rb, const int *__restrict__ blk_sys, const int *__restrict__ sys_blk,
             int nblk, const double *__restrict__ r, const double *__restrict__ v,
             const double *__restrict__ x, double *__restrict__ s, BState bs, double *__restrict__ partials) {
+    pdl_enter();
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
         const int k = __ldg(blk_sys + blk);
         if (bs.done[k]) continue;                         // uniform in the CTA
@@ -322,6 +326,7 @@ k_bupdate_s(const int *__restrict__ rb, const int *__restrict__ blk_sys, const i
         }
         warp_partials<2>(red, blk, partials);
     }
+    pdl_release();
 }
 
 static __global__ void __launch_bounds__(kThreads)
@@ -329,6 +334,7 @@ k_bupdate_xr(const int *__restrict__ rb, const int *__restrict__ blk_sys, const 
              int nblk, const double *__restrict__ pc, const double *__restrict__ sc,
              const double *__restrict__ s, const double *__restrict__ t, const double *__restrict__ r0,
              double *__restrict__ x, double *__restrict__ r, BState bs, double *__restrict__ partials) {
+    pdl_enter();
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
         const int k = __ldg(blk_sys + blk);
         if (bs.done[k]) continue;
@@ -346,6 +352,7 @@ k_bupdate_xr(const int *__restrict__ rb, const int *__restrict__ blk_sys, const 
         }
         warp_partials<1>(red, blk, partials);
     }
+    pdl_release();
 }
 
 // Last kernel of the loop body: block 0 counts the body, stops the loop should it ever run
@@ -355,6 +362,7 @@ static __global__ void __launch_bounds__(kThreads)
 k_bupdate_p(const int *__restrict__ rb, const int *__restrict__ blk_sys, int nblk,
             const double *__restrict__ r, const double *__restrict__ v, double *__restrict__ p, BState bs,
             cudaGraphConditionalHandle h, int cond) {
+    pdl_enter();
     if (cond && blockIdx.x == 0 && threadIdx.x == 0) {
         const int loops = ++bs.g->loops;
         if (bs.g->active > 0 && loops > bs.g->nmax + 2) bs.g->active = -1;
@@ -368,6 +376,7 @@ k_bupdate_p(const int *__restrict__ rb, const int *__restrict__ blk_sys, int nbl
         const double pi = __dadd_rn(__dmul_rn(c, v[row]), __dmul_rn(b, p[row]));
         p[row] = __dadd_rn(pi, r[row]);
     }
+    pdl_release();
 }
 
 // Factor values to FP32 / BF16 (round to nearest) for the reduced-precision factor forms.

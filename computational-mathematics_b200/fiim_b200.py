@@ -288,7 +288,9 @@ class BatchSolver:
     """Many independent systems in one device-driven loop (fiim_batch_*).
 
     systems: list of (A, F) with A = (Ai, Aj, Av) and F = {Gi, Gj, Gv, IDv, Hi, Hj, Hv}.
-    precision: 'fp64' | 'fp32' | 'bf16' storage of G and H."""
+    precision: 'fp64' | 'fp32' | 'bf16' storage of G and H.
+    memory: 'host' (numpy b, x) or 'device' (the concatenated arrays are uploaded here; b, x
+    are torch CUDA tensors)."""
 
     def __init__(self, systems, variant="acifim", precision="fp64", memory="host"):
         A, sys_rows = block_diag([s[0] for s in systems])
@@ -296,14 +298,18 @@ class BatchSolver:
         H, _ = block_diag([(s[1]["Hi"], s[1]["Hj"], s[1]["Hv"]) for s in systems])
         D = np.concatenate([np.asarray(s[1]["IDv"], np.float64) for s in systems])
         self.sys_rows, self.nsys, self.N = sys_rows, len(systems), int(sys_rows[-1])
+        self.memory = memory
         o = Options()
         lib().fiim_options_default(C.byref(o))
         o.variant = _VARIANTS[variant]
         o.precision = _PRECISIONS[precision]
-        o.memory = MEM_HOST
+        o.memory = MEM_DEVICE if memory == "device" else MEM_HOST
         self._h = C.c_void_p(0)
-        arrs = [A[0], A[1], A[2], G[0], G[1], G[2], D, H[0], H[1], H[2]]
-        _check(lib().fiim_batch_create(C.byref(self._h), C.c_int(self.nsys), _ptr(sys_rows),
+        arrs = [_i(A[0]), _i(A[1]), _d(A[2]), _i(G[0]), _i(G[1]), _d(G[2]), _d(D), _i(H[0]), _i(H[1]), _d(H[2])]
+        if memory == "device":
+            import torch
+            arrs = [torch.from_numpy(a).cuda() for a in arrs]
+        _check(lib().fiim_batch_create(C.byref(self._h), C.c_int(self.nsys), _ptr(_i(sys_rows)),
                                        *[_ptr(a) for a in arrs], C.byref(o)))
 
     def solve(self, b, x, tol=1e-8, nmax=2000):
@@ -312,8 +318,9 @@ class BatchSolver:
         it, info = np.zeros(k, np.int32), np.zeros(k, np.int32)
         rv, tr = np.zeros(k), np.zeros(k)
         r = Result()
-        b = _d(b)
-        assert x.dtype == np.float64 and x.flags.c_contiguous and len(x) == self.N
+        if self.memory != "device":
+            b = _d(b)
+            assert x.dtype == np.float64 and x.flags.c_contiguous and len(x) == self.N
         _check(lib().fiim_batch_solve(self._h, _ptr(b), _ptr(x), C.c_double(tol), C.c_int(nmax), _ptr(it),
                                       _ptr(info), _ptr(rv), _ptr(tr), C.byref(r)))
         return {"iter": it, "info": info, "resval": rv, "true_relres": tr, "summary": r.as_dict()}

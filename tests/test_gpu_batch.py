@@ -111,3 +111,20 @@ def test_batch_matches_single_system_solver():
         r = S.solve(b, x, tol=1e-8, nmax=2000)
         S.close()
         assert abs(r["iter"] - int(res["iter"][k])) <= 2 and r["info"] == res["info"][k]
+
+
+def test_batch_device_memory_equals_host_memory():
+    """The same batch created from device arrays and solved on device vectors gives the same
+    bits as the host-array form (the same kernels; only the copies differ)."""
+    systems = convdiff_systems(5, 23, "pdfiim")
+    b = np.concatenate([s[2] for s in systems])
+    Sh = FB.BatchSolver([(A, F) for A, F, _ in systems], variant="pdfiim", precision="fp32")
+    xh = np.zeros_like(b)
+    rh = Sh.solve(b, xh, tol=1e-8, nmax=2000)
+    Sh.close()
+    Sd = FB.BatchSolver([(A, F) for A, F, _ in systems], variant="pdfiim", precision="fp32", memory="device")
+    tx = torch.zeros(len(b), dtype=torch.float64, device="cuda")
+    rd = Sd.solve(torch.from_numpy(b).cuda(), tx, tol=1e-8, nmax=2000)
+    Sd.close()
+    assert np.array_equal(tx.cpu().numpy(), xh)
+    assert np.array_equal(rd["iter"], rh["iter"]) and np.array_equal(rd["info"], rh["info"])
