@@ -194,14 +194,6 @@ k_bfinish(const int *__restrict__ sys_blk, int nsys, const double *__restrict__ 
 __device__ __forceinline__ double widen(double v) { return v; }
 __device__ __forceinline__ double widen(float v) { return (double)v; }
 
-// Aligned pairs of matrix values: FP64 pairs as they are, FP32 and BF16 pairs as FP32 (held
-// in 4-byte registers until the product widens them).
-__device__ __forceinline__ double2 ldw2(const double *p) { return ldm2(p); }
-__device__ __forceinline__ float2 ldw2(const float *p) { return __ldcs(reinterpret_cast<const float2 *>(p)); }
-__device__ __forceinline__ float2 ldw2(const __nv_bfloat16 *p) {
-    return __bfloat1622float2(__ldcs(reinterpret_cast<const __nv_bfloat162 *>(p)));
-}
-
 // ---------------------------------------------------------------- batched CSR-stream SpMV
 // The single-system kernel's structure (k_spmv_rows): row blocks of at most TILE - 1
 // entries (first rows rb, first entries eb), entries read in aligned pairs, and the loop
@@ -221,9 +213,9 @@ k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, co
     int k = 0, r0 = 0, r1 = 0, e0 = 0, e1 = 0, rbeg = 0, rend = 0;
     bool skip = false;
     double opnd = 0.0;
-    using AV = typename std::conditional<std::is_same<V, double>::value, double, float>::type;
+    using VP = ValPair<V>;
     int c[PER];
-    AV a[PER];
+    typename VP::T a[PER / 2];
     auto fetch = [&](int blk) {
         k = __ldg(blk_sys + blk);
         r0 = __ldg(rb + blk);
@@ -244,17 +236,15 @@ k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, co
             for (int u = 0; u < PER / 2; ++u) {
                 const int e = a0 + 2 * (tid + u * kThreads);
                 c[2 * u] = c[2 * u + 1] = 0;
-                a[2 * u] = a[2 * u + 1] = AV(0);
+                a[u] = VP::zero();
                 if (e + 1 < e1) {
                     const int2 cc = ldi2(M.ci + e);
-                    const auto aa = ldw2(M.v + e);
                     c[2 * u] = cc.x;
                     c[2 * u + 1] = cc.y;
-                    a[2 * u] = aa.x;
-                    a[2 * u + 1] = aa.y;
+                    a[u] = VP::load2(M.v + e);
                 } else if (e < e1) {
                     c[2 * u] = ldi(M.ci + e);
-                    a[2 * u] = ldm(M.v + e);
+                    a[u] = VP::load1(M.v + e);
                 }
             }
         }
@@ -276,7 +266,7 @@ k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, co
 #pragma unroll
             for (int u = 0; u < PER; ++u) {
                 const int e = a0 + 2 * (tid + (u >> 1) * kThreads) + (u & 1);
-                if (e >= ce0 && e < ce1) prod[e - ce0] = __dmul_rn(widen(a[u]), ldx(x + c[u]));
+                if (e >= ce0 && e < ce1) prod[e - ce0] = __dmul_rn(widen(VP::get(a[u >> 1], u & 1)), ldx(x + c[u]));
             }
             if (nxt < nblk) fetch(nxt);
             __syncthreads();

@@ -71,13 +71,46 @@ __device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.lau
 // Matrix streams are read once per pass: evict-first so the vectors stay in L2.
 __device__ __forceinline__ double ldm(const double *p) { return __ldcs(p); }
 __device__ __forceinline__ float ldm(const float *p) { return __ldcs(p); }
+// A BF16 value is the upper half of the FP32 value it stands for: widening is a shift.
 __device__ __forceinline__ float ldm(const __nv_bfloat16 *p) {
     const unsigned short u = __ldcs(reinterpret_cast<const unsigned short *>(p));
-    return __bfloat162float(__ushort_as_bfloat16(u));
+    return __uint_as_float((unsigned)u << 16);
 }
 __device__ __forceinline__ int ldi(const int *p) { return __ldcs(p); }
 __device__ __forceinline__ int2 ldi2(const int *p) { return __ldcs(reinterpret_cast<const int2 *>(p)); }
 __device__ __forceinline__ double2 ldm2(const double *p) { return __ldcs(reinterpret_cast<const double2 *>(p)); }
+// Matrix values prefetched into registers stay in the form they were loaded in until they
+// are used: an FP64 or FP32 pair as two values, a BF16 pair as one 32-bit word. Widening a
+// BF16 value at load time would make the prefetching thread wait for the load there.
+template <typename V>
+struct ValPair;
+template <>
+struct ValPair<double> {
+    using T = double2;
+    __device__ static T load2(const double *p) { return __ldcs(reinterpret_cast<const double2 *>(p)); }
+    __device__ static T load1(const double *p) { return make_double2(__ldcs(p), 0.0); }
+    __device__ static T zero() { return make_double2(0.0, 0.0); }
+    __device__ static double get(const T &t, int h) { return h ? t.y : t.x; }
+};
+template <>
+struct ValPair<float> {
+    using T = float2;
+    __device__ static T load2(const float *p) { return __ldcs(reinterpret_cast<const float2 *>(p)); }
+    __device__ static T load1(const float *p) { return make_float2(__ldcs(p), 0.f); }
+    __device__ static T zero() { return make_float2(0.f, 0.f); }
+    __device__ static float get(const T &t, int h) { return h ? t.y : t.x; }
+};
+template <>
+struct ValPair<__nv_bfloat16> {   // the first value in the low half (little-endian)
+    using T = unsigned;
+    __device__ static T load2(const __nv_bfloat16 *p) { return __ldcs(reinterpret_cast<const unsigned *>(p)); }
+    __device__ static T load1(const __nv_bfloat16 *p) {
+        return (unsigned)__ldcs(reinterpret_cast<const unsigned short *>(p));
+    }
+    __device__ static T zero() { return 0u; }
+    __device__ static float get(const T &t, int h) { return __uint_as_float(h ? (t & 0xffff0000u) : (t << 16)); }
+};
+
 // Gathered vector entries: read-only path, cached.
 template <typename X>
 __device__ __forceinline__ X ldx(const X *p) { return __ldg(p); }

@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <iostream>
 #include <vector>
@@ -95,6 +96,7 @@ struct MixedSolver : SolverBase {
     unsigned long long *d_count = nullptr, *h_count = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    bool host_loop = false;   // FIIM_GRAPH=host: the host relaunches a one-iteration inner graph
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
     template <typename Epi>
@@ -127,6 +129,21 @@ struct MixedSolver : SolverBase {
         FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
         FIIM_TRY(enqueue_inner(false, cudaGraphConditionalHandle{}));
         FIIM_CUDA(cudaStreamSynchronize(stream));
+        // FIIM_GRAPH=host: a graph of one inner iteration, relaunched by the host (the same
+        // kernels and shapes; for profilers that replay graph kernel nodes one by one).
+        const char *mode_env = std::getenv("FIIM_GRAPH");
+        if (mode_env && std::strcmp(mode_env, "host") == 0) {
+            FIIM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            const int rc = enqueue_inner(false, cudaGraphConditionalHandle{});
+            cudaGraph_t g1 = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(stream, &g1);
+            if (rc != FIIM_OK) return rc;
+            FIIM_CUDA(ec);
+            FIIM_CUDA(cudaGraphInstantiate(&exec, g1, 0));
+            graph = g1;
+            host_loop = true;
+            return FIIM_OK;
+        }
         cudaGraph_t g = nullptr;
         FIIM_CUDA(cudaGraphCreate(&g, 0));
         cudaGraphConditionalHandle h;
@@ -317,7 +334,20 @@ struct MixedSolver : SolverBase {
             FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
             mx::k_inner_init<<<sgrid(mx::k_inner_init, n), kThreads, 0, stream>>>(n, r64, sto, r, r0, p, e, st, partials);
             FIIM_CUDA(cudaGetLastError());
-            FIIM_CUDA(cudaGraphLaunch(exec, stream));
+            if (!host_loop) {
+                FIIM_CUDA(cudaGraphLaunch(exec, stream));
+            } else {
+                int launched = 0, chunk = 1;
+                for (;;) {
+                    for (int q = 0; q < chunk; ++q) FIIM_CUDA(cudaGraphLaunch(exec, stream));
+                    launched += chunk;
+                    FIIM_CUDA(cudaMemcpyAsync(&hst->done, &st->done, sizeof(int), cudaMemcpyDeviceToHost, stream));
+                    FIIM_CUDA(cudaStreamSynchronize(stream));
+                    if (hst->done) break;
+                    if (launched > hst->nmax + 2) return set_error(FIIM_ETIMEOUT, "inner solve did not finish");
+                    chunk = std::min(chunk * 2, 16);
+                }
+            }
             mx::k_promote<<<sgrid(mx::k_promote, n), kThreads, 0, stream>>>(n, e, x, sto);
             FIIM_CUDA(cudaGetLastError());
             FIIM_CUDA(cudaMemcpyAsync(hst, st, sizeof(DState), cudaMemcpyDeviceToHost, stream));

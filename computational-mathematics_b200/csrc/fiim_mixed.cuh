@@ -75,10 +75,6 @@ struct EpiOmegaF {                 // t = A sc, omega = (t . s) / (t . t)
 
 __device__ __forceinline__ float ldv(const float *p) { return __ldcs(p); }
 __device__ __forceinline__ float ldv(const __nv_bfloat16 *p) { return ldm(p); }
-__device__ __forceinline__ float2 ldv2(const float *p) { return __ldcs(reinterpret_cast<const float2 *>(p)); }
-__device__ __forceinline__ float2 ldv2(const __nv_bfloat16 *p) {
-    return __bfloat1622float2(__ldcs(reinterpret_cast<const __nv_bfloat162 *>(p)));
-}
 
 // CSR-stream SpMV on FP32 / BF16 values and an FP32 vector, with the FP64 kernel's row
 // blocks (at most TILE - 1 entries, bounds rb / eb) and structure: entries read in aligned
@@ -99,8 +95,9 @@ k_spmv_rows_f(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ 
     for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
     int r0 = 0, r1 = 0, e0 = 0, e1 = 0, rbeg = 0, rend = 0;
     float opnd = 0.f;
+    using VP = ValPair<V>;
     int c[PER];
-    float a[PER];
+    typename VP::T a[PER / 2];
     auto fetch = [&](int blk) {
         r0 = __ldg(rb + blk);
         r1 = __ldg(rb + blk + 1);
@@ -118,17 +115,15 @@ k_spmv_rows_f(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ 
             for (int u = 0; u < PER / 2; ++u) {
                 const int e = a0 + 2 * (tid + u * kThreads);
                 c[2 * u] = c[2 * u + 1] = 0;
-                a[2 * u] = a[2 * u + 1] = 0.f;
+                a[u] = VP::zero();
                 if (e + 1 < e1) {
                     const int2 cc = ldi2(M.ci + e);
-                    const float2 aa = ldv2(M.v + e);
                     c[2 * u] = cc.x;
                     c[2 * u + 1] = cc.y;
-                    a[2 * u] = aa.x;
-                    a[2 * u + 1] = aa.y;
+                    a[u] = VP::load2(M.v + e);
                 } else if (e < e1) {
                     c[2 * u] = ldi(M.ci + e);
-                    a[2 * u] = ldv(M.v + e);
+                    a[u] = VP::load1(M.v + e);
                 }
             }
         }
@@ -143,7 +138,7 @@ k_spmv_rows_f(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ 
 #pragma unroll
             for (int u = 0; u < PER; ++u) {
                 const int e = a0 + 2 * (tid + (u >> 1) * kThreads) + (u & 1);
-                if (e >= ce0 && e < ce1) prod[e - ce0] = a[u] * ldx(x + c[u]);
+                if (e >= ce0 && e < ce1) prod[e - ce0] = VP::get(a[u >> 1], u & 1) * ldx(x + c[u]);
             }
             if (nxt < nblk) fetch(nxt);
             __syncthreads();
