@@ -35,6 +35,7 @@ constexpr int kTile = 2048;
 struct BMat {
     DevCsr M;
     int *blk_sys = nullptr, *sys_blk = nullptr;   // device
+    int *flag = nullptr;                           // device: finished-system flag per row block
     float *v32 = nullptr;
     __nv_bfloat16 *v16 = nullptr;
 };
@@ -95,8 +96,8 @@ struct BatchSolver : SolverBase {
     cudaError_t spmv(const BMat &B, const V *vals, const double *xx, const Epi &epi) {
         auto kern = bt::k_bspmv<kTile, V, Epi>;
         const int g = sgrid(kern, B.M.nblk);
-        return launch_k(kern, g, 0, stream, CsrView<V>{B.M.rp, B.M.ci, vals, (int)B.M.n}, B.M.rb, B.M.eb, B.blk_sys,
-                        B.sys_blk, B.M.nblk, xx, epi, bs, partials);
+        return launch_k(kern, g, 0, stream, CsrView<V>{B.M.rp, B.M.ci, vals, (int)B.M.n}, B.M.rb, B.M.eb, B.flag,
+                        B.M.nblk, xx, epi, bs, partials);
     }
     template <typename Epi>
     cudaError_t spmv_f(const BMat &B, const double *xx, const Epi &epi) {   // factors: stored precision
@@ -193,7 +194,7 @@ struct BatchSolver : SolverBase {
         const bool f32 = (opt.precision == FIIM_MIXED_FP32), f16 = (opt.precision == FIIM_MIXED_BF16);
         const size_t vsz = f16 ? 2 : 4;
         size_t bytes = csr_bytes(N, nA) + csr_bytes(N, nG) + csr_bytes(N, nH);
-        bytes += 3 * 2 * Arena::need(sizeof(int) * (N + nsys + 1));        // blk_sys, sys_blk
+        bytes += 3 * 3 * Arena::need(sizeof(int) * (N + nsys + 1));        // blk_sys, sys_blk, flag
         if (f32 || f16) bytes += Arena::need(vsz * std::max<long>(nG, 1)) + Arena::need(vsz * std::max<long>(nH, 1));
         bytes += 12 * Arena::need(sizeof(double) * N);
         bytes += 12 * Arena::need(sizeof(double) * nsys) + 7 * Arena::need(sizeof(int) * nsys);
@@ -205,7 +206,10 @@ struct BatchSolver : SolverBase {
             FIIM_TRY(carve_csr(arena, mats[m]->M, N, nz[m]));
             mats[m]->blk_sys = static_cast<int *>(arena.take(sizeof(int) * (N + nsys + 1)));
             mats[m]->sys_blk = static_cast<int *>(arena.take(sizeof(int) * (N + nsys + 1)));
-            if (!mats[m]->blk_sys || !mats[m]->sys_blk) return set_error(FIIM_ENOMEM, "arena exhausted");
+            mats[m]->flag = static_cast<int *>(arena.take(sizeof(int) * (N + nsys + 1)));
+            if (!mats[m]->blk_sys || !mats[m]->sys_blk || !mats[m]->flag)
+                return set_error(FIIM_ENOMEM, "arena exhausted");
+            bs.bf[m] = bt::BlockFlags{mats[m]->flag, mats[m]->sys_blk};
         }
         for (int m = 1; m < 3 && (f32 || f16); ++m) {
             void *pv = arena.take(vsz * std::max<long>(nz[m], 1));
@@ -272,6 +276,8 @@ struct BatchSolver : SolverBase {
         FIIM_CUDA(cudaMemcpyAsync(bs.g, hg, sizeof(bt::BGlobal), cudaMemcpyHostToDevice, stream));
         FIIM_CUDA(cudaMemsetAsync(bs.done, 0, sizeof(int) * nsys, stream));
         FIIM_CUDA(cudaMemsetAsync(bs.info, 0xff, sizeof(int) * nsys, stream));   // -1
+        for (const BMat *B : {&A, &G, &H})
+            FIIM_CUDA(cudaMemsetAsync(B->flag, 0, sizeof(int) * std::max(B->M.nblk, 1), stream));
         return FIIM_OK;
     }
 
@@ -280,6 +286,8 @@ struct BatchSolver : SolverBase {
         FIIM_TRY(reset_state(0.0, 0));
         std::vector<int> ones(nsys, 1);
         FIIM_CUDA(cudaMemcpyAsync(bs.done, ones.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, stream));
+        for (const BMat *B : {&A, &G, &H})   // nonzero: finished
+            FIIM_CUDA(cudaMemsetAsync(B->flag, 1, sizeof(int) * std::max(B->M.nblk, 1), stream));
         FIIM_TRY(enqueue_iteration(false, cudaGraphConditionalHandle{}));
         FIIM_CUDA(cudaStreamSynchronize(stream));
         // FIIM_GRAPH=host: a graph of one loop iteration, relaunched by the host (the same

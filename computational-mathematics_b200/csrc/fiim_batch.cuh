@@ -21,18 +21,30 @@ struct BGlobal {
     int nmax, alpha_guard, active, loops;
 };
 
+// Finished-system flags per row block of one matrix (batched solve; NULL elsewhere):
+// flag[b] != 0 once the system of block b has left the loop, so a kernel can skip a block
+// with one load that needs no other.
+struct BlockFlags {
+    int *flag;
+    const int *sys_blk;   // nsys + 1 block offsets per system
+};
+
 // Per-system state, structure of arrays (nsys entries each).
 struct BState {
     double *ro, *rc, *m1, *m2, *alpha, *omega, *beta, *pc2, *x2, *r2, *ts, *tt;
     int *iter, *stag, *msteps, *maxmsteps, *info, *done;
     unsigned int *ticket;   // per-system tickets (the block solver's last-CTA reductions)
     BGlobal *g;
+    BlockFlags bf[3];       // A, G, H row blocks (batched solve)
 };
 
 __device__ __forceinline__ void retire(BState &bs, int k, int info) {
     bs.info[k] = info;
     bs.done[k] = 1;
     atomicSub(&bs.g->active, 1);
+    for (int m = 0; m < 3; ++m)
+        if (bs.bf[m].flag)
+            for (int b = bs.bf[m].sys_blk[k]; b < bs.bf[m].sys_blk[k + 1]; ++b) bs.bf[m].flag[b] = 1;
 }
 
 // ---------------------------------------------------------------- per-system scalar steps
@@ -203,26 +215,24 @@ __device__ __forceinline__ double widen(float v) { return (double)v; }
 // blocks in the launch have been reduced, so the value read at prefetch is the one at use.
 template <int TILE, typename V, typename Epi>
 static __global__ void __launch_bounds__(kThreads, 4)
-k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, const int *__restrict__ blk_sys,
-        const int *__restrict__ sys_blk, int nblk, const double *__restrict__ x, Epi epi, BState bs,
-        double *__restrict__ partials) {
+k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, const int *__restrict__ bflag,
+        int nblk, const double *__restrict__ x, Epi epi, BState bs, double *__restrict__ partials) {
     pdl_enter();
     __shared__ double prod[TILE];
     constexpr int PER = TILE / kThreads;
     const int tid = (int)threadIdx.x;
-    int k = 0, r0 = 0, r1 = 0, e0 = 0, e1 = 0, rbeg = 0, rend = 0;
+    int r0 = 0, r1 = 0, e0 = 0, e1 = 0, rbeg = 0, rend = 0;
     bool skip = false;
     double opnd = 0.0;
     using VP = ValPair<V>;
     int c[PER];
     typename VP::T a[PER / 2];
     auto fetch = [&](int blk) {
-        k = __ldg(blk_sys + blk);
         r0 = __ldg(rb + blk);
         r1 = __ldg(rb + blk + 1);
         e0 = __ldg(eb + blk);
         e1 = __ldg(eb + blk + 1);
-        skip = Epi::GATED && bs.done[k];
+        skip = Epi::GATED && bflag[blk];   // flags change only in the finish kernels
         if (skip) return;
         rbeg = rend = 0;
         if (r0 + tid < r1) {
@@ -252,7 +262,7 @@ k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, co
     if ((int)blockIdx.x < nblk) fetch(blockIdx.x);
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
         const int nxt = blk + (int)gridDim.x;
-        const int ck = k, cr0 = r0, cr1 = r1, ce0 = e0, ce1 = e1, cb = rbeg - e0, ce = rend - e0;
+        const int cr0 = r0, cr1 = r1, ce0 = e0, ce1 = e1, cb = rbeg - e0, ce = rend - e0;
         const double copnd = opnd;
         if (skip) {                                         // uniform in the CTA
             if (nxt < nblk) fetch(nxt);
@@ -304,8 +314,8 @@ k_bupdate_s(const int *__restrict__ rb, const int *__restrict__ blk_sys, const i
             const double *__restrict__ x, double *__restrict__ s, BState bs, double *__restrict__ partials) {
     pdl_enter();
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        if (bs.bf[0].flag[blk]) continue;                 // uniform in the CTA
         const int k = __ldg(blk_sys + blk);
-        if (bs.done[k]) continue;                         // uniform in the CTA
         const int row = __ldg(rb + blk) + (int)threadIdx.x;
         double red[2] = {0.0, 0.0};
         if (row < __ldg(rb + blk + 1)) {
@@ -326,8 +336,8 @@ k_bupdate_xr(const int *__restrict__ rb, const int *__restrict__ blk_sys, const 
              double *__restrict__ x, double *__restrict__ r, BState bs, double *__restrict__ partials) {
     pdl_enter();
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        if (bs.bf[0].flag[blk]) continue;
         const int k = __ldg(blk_sys + blk);
-        if (bs.done[k]) continue;
         const int row = __ldg(rb + blk) + (int)threadIdx.x;
         double red[1] = {0.0};
         if (row < __ldg(rb + blk + 1)) {
@@ -359,9 +369,10 @@ k_bupdate_p(const int *__restrict__ rb, const int *__restrict__ blk_sys, int nbl
         cudaGraphSetConditional(h, bs.g->active > 0 ? 1u : 0u);
     }
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        if (bs.bf[0].flag[blk]) continue;
         const int k = __ldg(blk_sys + blk);
         const int row = __ldg(rb + blk) + (int)threadIdx.x;
-        if (bs.done[k] || row >= __ldg(rb + blk + 1)) continue;
+        if (row >= __ldg(rb + blk + 1)) continue;
         const double b = bs.beta[k], c = __dmul_rn(-bs.beta[k], bs.omega[k]);
         const double pi = __dadd_rn(__dmul_rn(c, v[row]), __dmul_rn(b, p[row]));
         p[row] = __dadd_rn(pi, r[row]);
