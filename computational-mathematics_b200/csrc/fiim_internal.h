@@ -67,6 +67,7 @@ struct DevCsr {
     int *eb = nullptr;           // row-block first entries (device), nblk + 1 entries
     int nblk = 0;
     std::vector<int> hrp;        // row offsets on the host (row blocks, tuning key)
+    bool rows_same = false;      // the last upload_csr found the same row offsets as before
     std::vector<long> sig;       // tuning-cache key: n, nnz, sampled row offsets
 };
 

@@ -367,14 +367,21 @@ void signature(DevCsr &M, const int *host_rp) {
 int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, const double *v,
                       int fill, bool device_src, cudaStream_t s, unsigned long long *d_count,
                       unsigned long long *h_count) {
-    M.n = n;
     std::vector<int> &hrp = M.hrp;
-    hrp.resize(n + 1);
+    const bool had = (M.n == n && (long)hrp.size() == (long)n + 1);
+    M.n = n;
     if (device_src) {
-        FIIM_CUDA(cudaMemcpyAsync(hrp.data(), rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
+        std::vector<int> nrp(n + 1);
+        FIIM_CUDA(cudaMemcpyAsync(nrp.data(), rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
         FIIM_CUDA(cudaStreamSynchronize(s));
+        M.rows_same = had && nrp == hrp;
+        hrp.swap(nrp);
     } else {
-        std::memcpy(hrp.data(), rp, sizeof(int) * (n + 1));
+        M.rows_same = had && std::memcmp(hrp.data(), rp, sizeof(int) * (n + 1)) == 0;
+        if (!M.rows_same) {
+            hrp.resize(n + 1);
+            std::memcpy(hrp.data(), rp, sizeof(int) * (n + 1));
+        }
     }
     const long nnz = hrp[n];
     if (nnz > nnz_cap) return set_error(FIIM_EARG, "matrix has %ld entries, capacity %ld", nnz, nnz_cap);
@@ -420,6 +427,7 @@ int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, con
         FIIM_CUDA(cudaMemcpy(M.v, cv.data(), sizeof(double) * c, cudaMemcpyHostToDevice));
     }
     hrp.swap(nrp);
+    M.rows_same = false;   // the stored offsets are the filtered ones
     signature(M, hrp.data());
     return FIIM_OK;
 }
@@ -723,10 +731,12 @@ int Solver::reload(const int *Ai, const int *Aj, const double *Av, const int *Gi
     }
     FIIM_CUDA(cudaMemcpyAsync(IDv, IDv_, sizeof(double) * n,
                               dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
-    // Row blocks follow the new row offsets; the graph bakes in each block count.
+    // Row blocks follow the new row offsets (rebuilt only where they changed); the graph
+    // bakes in each block count.
     bool regraph = false;
     DevCsr *mats[] = {&A, &G, &H, &L, &U};
     for (int k = 0; k < (combined ? 5 : 3); ++k) {
+        if (mats[k]->rows_same && mats[k]->nblk > 0) continue;
         const int old = mats[k]->nblk;
         FIIM_TRY(set_tile(*mats[k], mats[k]->tile, stream));
         regraph |= (mats[k]->nblk != old);

@@ -228,6 +228,34 @@ def _forms_cache():
     return os.path.join(tempfile.gettempdir(), f"fiim_forms_{os.getpid()}.npy")
 
 
+def test_dropin_reload_follows_row_structure():
+    """A drop-in call with a system of the same size and entry count but other row offsets
+    rebuilds the row blocks: its result equals a fresh solver's bit for bit."""
+    A = FB.gen_convdiff3d(12, 0.5)
+    n = len(A[0]) - 1
+    M = sp.csr_matrix((A[2], A[1], A[0]), shape=(n, n))
+    P = sp.eye(n, format="csr")[np.random.default_rng(5).permutation(n)]
+    M2 = (P @ M @ P.T).tocsr()
+    M2.sort_indices()
+    A2 = (M2.indptr.astype(np.int32), M2.indices.astype(np.int32), M2.data.copy())
+    assert len(A2[1]) == len(A[1]) and not np.array_equal(A2[0], A[0])
+    F = identity_factors(n)
+    G, H = (F["Gi"], F["Gj"], F["Gv"]), (F["Hi"], F["Hj"], F["Hv"])
+    b = FB.rand_normal(n, 3)
+    prev = FB.dropin_cache(False)
+    try:
+        for AA in (A, A2):
+            x = np.zeros(n)
+            r = FB.EPBiCGSTAB_pdfiim(AA, b, 1e-10, 500, G, F["IDv"], H, x)
+            S = FB.Solver(AA, F, variant="pdfiim")
+            y = np.zeros(n)
+            r1 = S.solve(b, y, tol=1e-10, nmax=500)
+            S.close()
+            assert np.array_equal(x, y) and r[1] == r1["iter"]
+    finally:
+        FB.dropin_cache(prev)
+
+
 def test_dropin_cache_follows_array_contents():
     """Repeated drop-in calls reuse the device copies only while every matrix array keeps
     its address, size and contents: a value changed in place is uploaded again, and the
