@@ -178,7 +178,8 @@ k_spmm(CsrView<V> M, Shape sh, const double *__restrict__ X, Epi epi, BState bs,
             beg = __ldg(M.rp + row);
             len = __ldg(M.rp + row + 1) - beg;
         }
-        // every group of the warp walks the longest row of the warp (uniform shuffles)
+        // every group of the warp walks the longest row of the warp (uniform shuffles), and
+        // within a trip only as many entries as the longest remaining row part holds
         const int trips = __reduce_max_sync(0xffffffffu, (len + KP - 1) / KP);
         double s = 0.0;
         for (int t = 0; t < trips; ++t) {
@@ -189,8 +190,9 @@ k_spmm(CsrView<V> M, Shape sh, const double *__restrict__ X, Epi epi, BState bs,
                 c = ldi(M.ci + beg + q);
                 a = wide(ldm(M.v + beg + q));
             }
-#pragma unroll 8
-            for (int e = 0; e < KP; ++e) {
+            const int ne = (int)__reduce_max_sync(0xffffffffu, (unsigned)max(0, min(KP, len - t * KP)));
+#pragma unroll 4
+            for (int e = 0; e < ne; ++e) {
                 const int ce = __shfl_sync(0xffffffffu, c, grp_ * KP + e);
                 const double ae = __shfl_sync(0xffffffffu, a, grp_ * KP + e);
                 if (t * KP + e < len && j_ < sh.k)
