@@ -109,7 +109,7 @@ struct BatchSolver : SolverBase {
     // Second phase of a per-system reduction over matrix B's row blocks (bt::k_bfinish).
     template <int NR, bool GATED = true, class Fin>
     cudaError_t finish(const BMat &B, const Fin &fin) {
-        const int g = (int)std::min<long>(((long)nsys * 32 + kThreads - 1) / kThreads, 8L * num_sms());
+        const int g = (int)std::min<long>(nsys, 8L * num_sms());
         return launch_k(bt::k_bfinish<NR, GATED, Fin>, g, 0, stream, B.sys_blk, nsys, partials, bs, fin);
     }
 

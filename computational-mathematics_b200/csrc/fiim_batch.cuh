@@ -4,7 +4,7 @@
 //
 // Row blocks (<= 256 rows, <= TILE - 1 entries) never straddle two systems. Every kernel walks
 // row blocks; a block of a system that has finished is skipped. Reductions are per system:
-// each warp of each row block stores one partial, and a finish kernel (one warp per system)
+// each warp of each row block stores one partial, and a finish kernel (one CTA per system)
 // adds a system's partials in a fixed order and applies the system's scalar step. Vectors
 // are FP64; factor values may be FP64, FP32 or BF16 (widened to FP64 before the rounded
 // product), so every vector operation is the reference's, bit for bit,
@@ -170,7 +170,7 @@ struct BEpiResid {
 // after the warp's shuffle tree): no CTA barrier, fence or atomic per block. A finish kernel
 // then gives each system one warp, which adds the system's partials (blocks in order,
 // lane-strided, then the shuffle tree: a fixed order) and applies the system's scalar step.
-// Partials: (block * kWarps + warp) * NR + j.
+// Partials: (block * kWarps + warp) * NR + j. The finish kernel gives each system one CTA.
 template <int NR>
 __device__ __forceinline__ void warp_partials(double (&v)[NR], int blk, double *__restrict__ partials) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -181,25 +181,42 @@ __device__ __forceinline__ void warp_partials(double (&v)[NR], int blk, double *
         for (int j = 0; j < NR; ++j) partials[((size_t)blk * kWarps + w) * NR + j] = v[j];
 }
 
-// One warp per system: systems whose loop has ended are left alone when GATED.
+// One CTA per system (grid-stride over systems): thread t adds partials t, t + 256, ...
+// of the system, then the CTA's warp trees and the warp totals in warp order (a fixed
+// order). Systems whose loop has ended are left alone when GATED.
 template <int NR, bool GATED, class Fin>
 static __global__ void __launch_bounds__(kThreads)
 k_bfinish(const int *__restrict__ sys_blk, int nsys, const double *__restrict__ partials, BState bs, Fin fin) {
     pdl_enter();
-    const int lane = threadIdx.x & 31;
-    const int nw = (int)(gridDim.x * blockDim.x) >> 5;
-    for (int k = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); k < nsys; k += nw) {
-        if (GATED && bs.done[k]) continue;             // uniform in the warp
+    __shared__ double sm[kWarps][NR];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int k = blockIdx.x; k < nsys; k += gridDim.x) {
+        if (GATED && bs.done[k]) continue;             // uniform in the CTA
         const int q0 = __ldg(sys_blk + k) * kWarps, q1 = __ldg(sys_blk + k + 1) * kWarps;
         double acc[NR];
 #pragma unroll
         for (int j = 0; j < NR; ++j) acc[j] = 0.0;
-        for (int q = q0 + lane; q < q1; q += 32)
+        for (int q = q0 + (int)threadIdx.x; q < q1; q += kThreads)
 #pragma unroll
             for (int j = 0; j < NR; ++j) acc[j] += partials[(size_t)q * NR + j];
 #pragma unroll
         for (int j = 0; j < NR; ++j) acc[j] = warp_sum(acc[j]);
-        if (lane == 0) fin.finish(bs, k, acc);
+        if (lane == 0)
+#pragma unroll
+            for (int j = 0; j < NR; ++j) sm[w][j] = acc[j];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot[NR];
+#pragma unroll
+            for (int j = 0; j < NR; ++j) {
+                double t = 0.0;
+#pragma unroll
+                for (int q = 0; q < kWarps; ++q) t += sm[q][j];
+                tot[j] = t;
+            }
+            fin.finish(bs, k, tot);
+        }
+        __syncthreads();
     }
 }
 
