@@ -571,9 +571,10 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=99,
                     help="iterations of the full 128^3 solve (the reference's own count, for scaling samples)")
     # DRAM bytes per launch of the dominant kernel (H's SpMV) from an ncu capture of the
-    # 96^3 case (read + write = 0.979 x its algorithmic bytes), scaled to the 128^3 launch by
-    # the units processed (entries and rows, which the traffic is proportional to).
-    ap.add_argument("--ncu-traffic", type=float, default=324.2e6,
+    # 96^3 case (read + write = 0.842 x its algorithmic bytes: the column stream is stored as
+    # 16-bit offsets), scaled to the 128^3 launch by the units processed (entries and rows,
+    # which the traffic is proportional to).
+    ap.add_argument("--ncu-traffic", type=float, default=278.8e6,
                     help="dram bytes per launch of the dominant kernel from an ncu capture")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

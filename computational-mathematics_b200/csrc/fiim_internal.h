@@ -65,6 +65,10 @@ struct DevCsr {
     int form = 0;                // CSR-stream SpMV form, one of the kForm* constants
     int *rb = nullptr;           // row-block first rows (device), nblk + 1 entries
     int *eb = nullptr;           // row-block first entries (device), nblk + 1 entries
+    int *cb = nullptr;           // row-block base columns of the narrow column stream
+    short *cd = nullptr;         // narrow column stream: column - block base (device)
+    int *wide = nullptr;         // device flag written by the narrow-stream builder
+    int narrow = 0;              // 1: the CSR-stream SpMV reads cd / cb instead of ci
     int nblk = 0;
     std::vector<int> hrp;        // row offsets on the host (row blocks, tuning key)
     bool rows_same = false;      // the last upload_csr found the same row offsets as before

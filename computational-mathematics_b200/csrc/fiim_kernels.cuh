@@ -353,10 +353,50 @@ struct EpiAccumNorm {              // y = (M x) + y, ||y||^2 -> st->pc2
 // The loop is software-pipelined by one block: the next block's bounds, this thread's
 // row offsets in it and its share of the column/value stream are loaded into registers
 // before the barrier, so they are in flight while the current block's rows are summed.
-template <int TILE, typename Epi>
+// Narrow column stream (NARROW): 16-bit offsets from a per-row-block base column, built by
+// k_narrow_cols when every block's columns span at most 65,536; 10 bytes per entry instead of
+// 12. A thread keeps each prefetched pair of offsets as the 32-bit word it was loaded as and
+// forms the columns only at the product, so no instruction waits on the prefetch.
+struct NarrowCols {
+    const short *__restrict__ d = nullptr;     // column - base of the entry's block
+    const int *__restrict__ base = nullptr;    // per row block
+};
+
+template <bool NARROW, int PER>
+struct ColRegs;
+template <int PER>
+struct ColRegs<false, PER> {
+    int c[PER];
+    __device__ void zero(int u) { c[2 * u] = c[2 * u + 1] = 0; }
+    __device__ void load2(const int *ci, const NarrowCols &, int e, int u) {
+        const int2 cc = ldi2(ci + e);
+        c[2 * u] = cc.x;
+        c[2 * u + 1] = cc.y;
+    }
+    __device__ void load1(const int *ci, const NarrowCols &, int e, int u) { c[2 * u] = ldi(ci + e); }
+    __device__ int get(int u, int) const { return c[u]; }
+};
+template <int PER>
+struct ColRegs<true, PER> {
+    unsigned w[PER / 2];
+    __device__ void zero(int u) { w[u] = 0u; }
+    __device__ void load2(const int *, const NarrowCols &nc, int e, int u) {
+        w[u] = __ldcs(reinterpret_cast<const unsigned *>(nc.d + e));
+    }
+    __device__ void load1(const int *, const NarrowCols &nc, int e, int u) {
+        w[u] = (unsigned)__ldcs(reinterpret_cast<const unsigned short *>(nc.d + e));
+    }
+    __device__ int get(int u, int base) const {
+        const unsigned v = w[u >> 1];
+        return base + (int)(short)(unsigned short)((u & 1) ? (v >> 16) : (v & 0xffffu));
+    }
+};
+
+template <int TILE, typename Epi, bool NARROW = false>
 static __global__ void __launch_bounds__(kThreads)
 k_spmv_rows(CsrView<double> M, const int *__restrict__ rb, const int *__restrict__ eb, int nblk,
-            const double *__restrict__ x, Epi epi, DState *st, double *__restrict__ partials) {
+            const double *__restrict__ x, Epi epi, DState *st, double *__restrict__ partials,
+            NarrowCols nc = NarrowCols{}) {
     pdl_enter();
     if (Epi::GATED && st != nullptr && st->done) return;
     __shared__ double prod[TILE];
@@ -365,19 +405,20 @@ k_spmv_rows(CsrView<double> M, const int *__restrict__ rb, const int *__restrict
     double red[Epi::NR];
 #pragma unroll
     for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
-    int r0 = 0, r1 = 0, e0 = 0, e1 = 0, rbeg = 0, rend = 0;
+    int r0 = 0, r1 = 0, e0 = 0, e1 = 0, rbeg = 0, rend = 0, cbase = 0;
     double opnd = 0.0;   // the epilogue's operand for this thread's row (HasPre)
     // Entries are read in aligned pairs: thread tid holds entries a0 + 2 (tid + u kThreads)
     // + h of the window [a0, a0 + TILE), a0 = e0 rounded down to even. Row blocks have at
     // most TILE - 1 entries, so the window covers [e0, e1); a block that does not fit is a
     // single long row.
-    int c[PER];
+    ColRegs<NARROW, PER> c;
     double a[PER];
     auto fetch = [&](int blk) {
         r0 = __ldg(rb + blk);
         r1 = __ldg(rb + blk + 1);
         e0 = __ldg(eb + blk);
         e1 = __ldg(eb + blk + 1);
+        if constexpr (NARROW) cbase = __ldg(nc.base + blk);
         rbeg = rend = 0;
         if (r0 + tid < r1) {
             rbeg = __ldg(M.rp + r0 + tid);
@@ -389,17 +430,15 @@ k_spmv_rows(CsrView<double> M, const int *__restrict__ rb, const int *__restrict
 #pragma unroll
             for (int u = 0; u < PER / 2; ++u) {
                 const int e = a0 + 2 * (tid + u * kThreads);
-                c[2 * u] = c[2 * u + 1] = 0;
+                c.zero(u);
                 a[2 * u] = a[2 * u + 1] = 0.0;
                 if (e + 1 < e1) {
-                    const int2 cc = ldi2(M.ci + e);
+                    c.load2(M.ci, nc, e, u);
                     const double2 aa = ldm2(M.v + e);
-                    c[2 * u] = cc.x;
-                    c[2 * u + 1] = cc.y;
                     a[2 * u] = aa.x;
                     a[2 * u + 1] = aa.y;
                 } else if (e < e1) {
-                    c[2 * u] = ldi(M.ci + e);
+                    c.load1(M.ci, nc, e, u);
                     a[2 * u] = ldm(M.v + e);
                 }
             }
@@ -408,14 +447,14 @@ k_spmv_rows(CsrView<double> M, const int *__restrict__ rb, const int *__restrict
     if ((int)blockIdx.x < nblk) fetch(blockIdx.x);
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
         const int nxt = blk + (int)gridDim.x;
-        const int cr0 = r0, cr1 = r1, ce0 = e0, ce1 = e1, cb = rbeg - e0, ce = rend - e0;
+        const int cr0 = r0, cr1 = r1, ce0 = e0, ce1 = e1, cb = rbeg - e0, ce = rend - e0, cbs = cbase;
         const double copnd = opnd;
         if (ce1 - ce0 < TILE) {
             const int a0 = ce0 & ~1;
 #pragma unroll
             for (int u = 0; u < PER; ++u) {
                 const int e = a0 + 2 * (tid + (u >> 1) * kThreads) + (u & 1);
-                if (e >= ce0 && e < ce1) prod[e - ce0] = __dmul_rn(a[u], ldx(x + c[u]));
+                if (e >= ce0 && e < ce1) prod[e - ce0] = __dmul_rn(a[u], ldx(x + c.get(u, cbs)));
             }
             if (nxt < nblk) fetch(nxt);
             __syncthreads();
@@ -430,8 +469,10 @@ k_spmv_rows(CsrView<double> M, const int *__restrict__ rb, const int *__restrict
             double s = 0.0;
             for (int c0 = ce0; c0 < ce1; c0 += TILE) {
                 const int c1 = min(c0 + TILE, ce1);
-                for (int e = c0 + tid; e < c1; e += kThreads)
-                    prod[e - c0] = __dmul_rn(ldm(M.v + e), ldx(x + ldi(M.ci + e)));
+                for (int e = c0 + tid; e < c1; e += kThreads) {
+                    const int j = NARROW ? cbs + (int)__ldcs(nc.d + e) : ldi(M.ci + e);
+                    prod[e - c0] = __dmul_rn(ldm(M.v + e), ldx(x + j));
+                }
                 __syncthreads();
                 if (tid == 0)
                     for (int k = 0; k < c1 - c0; ++k) s = __dadd_rn(s, prod[k]);
@@ -443,6 +484,47 @@ k_spmv_rows(CsrView<double> M, const int *__restrict__ rb, const int *__restrict
     }
     pdl_release();
     if constexpr (Epi::REDUCES) grid_reduce<Epi::NR>(red, partials, st, epi);
+}
+
+// Narrow column stream for k_spmv_rows: per row block, base = smallest column + 32768 and
+// d[e] = column - base, when the block's columns span at most 65,536; otherwise *wide is set
+// and the matrix keeps its 32-bit columns. One CTA per block, grid-stride.
+static __global__ void __launch_bounds__(kThreads)
+k_narrow_cols(const int *__restrict__ ci, const int *__restrict__ eb, int nblk, short *__restrict__ d,
+              int *__restrict__ base, int *wide) {
+    __shared__ int smin[kWarps], smax[kWarps];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        const int e0 = eb[blk], e1 = eb[blk + 1];
+        int lo = 0x7fffffff, hi = -0x7fffffff - 1;
+        for (int e = e0 + (int)threadIdx.x; e < e1; e += kThreads) {
+            lo = min(lo, ci[e]);
+            hi = max(hi, ci[e]);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if (lane == 0) {
+            smin[w] = lo;
+            smax[w] = hi;
+        }
+        __syncthreads();
+        lo = smin[0];
+        hi = smax[0];
+        for (int q = 1; q < kWarps; ++q) {
+            lo = min(lo, smin[q]);
+            hi = max(hi, smax[q]);
+        }
+        __syncthreads();
+        if (e1 > e0 && (long)hi - (long)lo > 65535) {
+            if (threadIdx.x == 0) atomicExch(wide, 1);
+            continue;
+        }
+        const int b = e1 > e0 ? lo + 32768 : 0;
+        if (threadIdx.x == 0) base[blk] = b;
+        for (int e = e0 + (int)threadIdx.x; e < e1; e += kThreads) d[e] = (short)(ci[e] - b);
+    }
 }
 
 // ---------------------------------------------------------------- CSR-vector SpMV

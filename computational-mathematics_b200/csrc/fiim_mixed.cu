@@ -56,9 +56,9 @@ cudaError_t spmv_f(const DevCsr &M, const V *vals, cudaStream_t s, const float *
 template <int TILE, typename Epi>
 cudaError_t rows_64(cudaStream_t s, const DevCsr &M, const double *x, const Epi &epi, DState *st,
                     double *partials) {
-    auto kern = k_spmv_rows<TILE, Epi>;
+    auto kern = k_spmv_rows<TILE, Epi, false>;
     const int g = grid_for(kern, 1, M.nblk);
-    kern<<<g, kThreads, 0, s>>>(view64(M), M.rb, M.eb, M.nblk, x, epi, st, partials);
+    kern<<<g, kThreads, 0, s>>>(view64(M), M.rb, M.eb, M.nblk, x, epi, st, partials, NarrowCols{});
     return cudaGetLastError();
 }
 

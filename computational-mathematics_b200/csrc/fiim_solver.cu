@@ -132,9 +132,14 @@ static CsrView<double> view(const DevCsr &M) { return CsrView<double>{M.rp, M.ci
 template <int TILE, typename Epi>
 static cudaError_t spmv_rows(cudaStream_t s, const DevCsr &M, const double *x, const Epi &epi,
                              DState *st, double *partials) {
-    auto kern = k_spmv_rows<TILE, Epi>;
+    if (M.narrow) {
+        auto kern = k_spmv_rows<TILE, Epi, true>;
+        const int g = grid_for(kern, 1, M.nblk);
+        return launch_k(kern, g, 0, s, view(M), M.rb, M.eb, M.nblk, x, epi, st, partials, NarrowCols{M.cd, M.cb});
+    }
+    auto kern = k_spmv_rows<TILE, Epi, false>;
     const int g = grid_for(kern, 1, M.nblk);
-    return launch_k(kern, g, 0, s, view(M), M.rb, M.eb, M.nblk, x, epi, st, partials);
+    return launch_k(kern, g, 0, s, view(M), M.rb, M.eb, M.nblk, x, epi, st, partials, NarrowCols{});
 }
 
 // Resident CTAs per SM of a kernel with `smem` bytes of dynamic shared memory, with the
@@ -226,6 +231,19 @@ int set_tile(DevCsr &M, int tile, cudaStream_t s) {
     for (size_t k = 0; k < rb.size(); ++k) eb[k] = M.hrp[rb[k]];
     FIIM_CUDA(cudaMemcpyAsync(M.rb, rb.data(), sizeof(int) * rb.size(), cudaMemcpyHostToDevice, s));
     FIIM_CUDA(cudaMemcpyAsync(M.eb, eb.data(), sizeof(int) * eb.size(), cudaMemcpyHostToDevice, s));
+    // Narrow column stream when every row block allows it (FIIM_COLS=wide keeps 32-bit columns).
+    M.narrow = 0;
+    const char *cols = std::getenv("FIIM_COLS");
+    if (M.nblk > 0 && M.nnz > 0 && M.cd && !(cols && std::strcmp(cols, "wide") == 0)) {
+        FIIM_CUDA(cudaMemsetAsync(M.wide, 0, sizeof(int), s));
+        const int g = (int)std::min<long>(M.nblk, 16L * num_sms());
+        k_narrow_cols<<<g, kThreads, 0, s>>>(M.ci, M.eb, M.nblk, M.cd, M.cb, M.wide);
+        FIIM_CUDA(cudaGetLastError());
+        int wide = 1;
+        FIIM_CUDA(cudaMemcpyAsync(&wide, M.wide, sizeof(int), cudaMemcpyDeviceToHost, s));
+        FIIM_CUDA(cudaStreamSynchronize(s));
+        M.narrow = wide ? 0 : 1;
+    }
     FIIM_CUDA(cudaStreamSynchronize(s));
     return FIIM_OK;
 }
@@ -440,14 +458,18 @@ int carve_csr(Arena &ar, DevCsr &M, long n, long nnz) {
     M.rp = static_cast<int *>(ar.take(sizeof(int) * (n + 1)));
     M.ci = static_cast<int *>(ar.take(sizeof(int) * std::max<long>(nnz, 1) + kStreamSlack));
     M.v = static_cast<double *>(ar.take(sizeof(double) * std::max<long>(nnz, 1) + kStreamSlack));
-    M.rb = static_cast<int *>(ar.take(sizeof(int) * 2 * (n + 1)));   // at most one block per row
-    if (!M.rp || !M.ci || !M.v || !M.rb) return set_error(FIIM_ENOMEM, "arena exhausted");
+    M.rb = static_cast<int *>(ar.take(sizeof(int) * (3 * (n + 1) + 1)));   // at most one block per row
+    M.cd = static_cast<short *>(ar.take(sizeof(short) * std::max<long>(nnz, 1) + kStreamSlack));
+    if (!M.rp || !M.ci || !M.v || !M.rb || !M.cd) return set_error(FIIM_ENOMEM, "arena exhausted");
     M.eb = M.rb + (n + 1);
+    M.cb = M.rb + 2 * (n + 1);
+    M.wide = M.rb + 3 * (n + 1);
     return FIIM_OK;
 }
 
 size_t csr_bytes(long n, long nnz) {
-    return Arena::need(sizeof(int) * (n + 1)) + Arena::need(sizeof(int) * 2 * (n + 1)) +
+    return Arena::need(sizeof(int) * (n + 1)) + Arena::need(sizeof(int) * (3 * (n + 1) + 1)) +
+           Arena::need(sizeof(short) * std::max<long>(nnz, 1) + kStreamSlack) +
            Arena::need(sizeof(int) * std::max<long>(nnz, 1) + kStreamSlack) +
            Arena::need(sizeof(double) * std::max<long>(nnz, 1) + kStreamSlack);
 }

@@ -70,11 +70,12 @@ def test_prec_apply_matches_oracle(golden, cuda, name, prefix):
     ("poisson128_afiim", "", "afiim", {}), ("convdiff16_pdfiim", "", "pdfiim", {}),
     ("convdiff2d48_acifim", "", "acifim", {"mode": "C", "nr": 2}), ("poisson32_sym_pdfiim", "", "pdfiim",
                                                                      {"issym": True})])
-@pytest.mark.parametrize("form", ["rows", "staged"])
-def test_solver_products_bit_identical(golden, monkeypatch, name, prefix, variant, kw, form):
-    """The solver's tuned CSR-stream kernels (streams through registers or bulk copies)
-    reproduce the oracle's A x and M x exactly."""
+@pytest.mark.parametrize("form,cols", [("rows", "narrow"), ("rows", "wide"), ("staged", "wide")])
+def test_solver_products_bit_identical(golden, monkeypatch, name, prefix, variant, kw, form, cols):
+    """The solver's tuned CSR-stream kernels (streams through registers, with 16-bit or 32-bit
+    column streams, or by bulk copies) reproduce the oracle's A x and M x exactly."""
     monkeypatch.setenv("FIIM_SPMV", form)
+    monkeypatch.setenv("FIIM_COLS", cols)
     g = golden(name)
     F = sub(g, prefix)
     S = FB.Solver((g["Ai"], g["Aj"], g["Av"]), F, variant=variant, autotune=True, **kw)
@@ -116,6 +117,26 @@ def test_solver_spmv_random_rows(monkeypatch, long_len, form):
     S = FB.Solver(A, identity_factors(n), autotune=form is not None)
     if form is None:
         assert S.spmv_shape(0) == (2048, 0)
+    y = S.apply(u, np.zeros(n), op="A")
+    S.close()
+    assert np.array_equal(y, O.csr_mv(*A, u))
+
+
+@pytest.mark.parametrize("spread", [60000, 70000, 400000])
+def test_solver_spmv_column_spans(spread):
+    """Row blocks whose columns span more than 65,536 keep 32-bit columns (the matrix falls
+    back as a whole); narrower spans use 16-bit offsets from a per-block base. Either way A x
+    equals the oracle's bit for bit."""
+    rng = np.random.default_rng(spread)
+    n = 200000
+    rows = np.repeat(np.arange(n), 6)
+    cols = np.clip(rows + rng.integers(-spread // 2, spread // 2 + 1, rows.size), 0, n - 1)
+    M = sp.csr_matrix((rng.uniform(-1, 1, rows.size), (rows, cols)), shape=(n, n)) + sp.eye(n) * 8
+    M.sum_duplicates()
+    M.sort_indices()
+    A = (M.indptr.astype(np.int32), M.indices.astype(np.int32), M.data)
+    u = rng.standard_normal(n)
+    S = FB.Solver(A, identity_factors(n))
     y = S.apply(u, np.zeros(n), op="A")
     S.close()
     assert np.array_equal(y, O.csr_mv(*A, u))
