@@ -94,10 +94,15 @@ struct BatchSolver : SolverBase {
 
     template <typename V, typename Epi>
     cudaError_t spmv(const BMat &B, const V *vals, const double *xx, const Epi &epi) {
-        auto kern = bt::k_bspmv<kTile, V, Epi>;
+        auto kern = bt::k_bspmv<kTile, V, Epi, false>;
         const int g = sgrid(kern, B.M.nblk);
+        if (B.M.narrow) {
+            auto kn = bt::k_bspmv<kTile, V, Epi, true>;
+            return launch_k(kn, sgrid(kn, B.M.nblk), 0, stream, CsrView<V>{B.M.rp, B.M.ci, vals, (int)B.M.n}, B.M.rb,
+                            B.M.eb, B.flag, B.M.nblk, xx, epi, bs, partials, NarrowCols{B.M.cd, B.M.cb});
+        }
         return launch_k(kern, g, 0, stream, CsrView<V>{B.M.rp, B.M.ci, vals, (int)B.M.n}, B.M.rb, B.M.eb, B.flag,
-                        B.M.nblk, xx, epi, bs, partials);
+                        B.M.nblk, xx, epi, bs, partials, NarrowCols{});
     }
     template <typename Epi>
     cudaError_t spmv_f(const BMat &B, const double *xx, const Epi &epi) {   // factors: stored precision
@@ -149,7 +154,7 @@ struct BatchSolver : SolverBase {
                                       stream));
         FIIM_CUDA(cudaMemcpyAsync(B.sys_blk, sblk.data(), sizeof(int) * sblk.size(), cudaMemcpyHostToDevice, stream));
         FIIM_CUDA(cudaStreamSynchronize(stream));
-        return FIIM_OK;
+        return build_narrow(B.M, stream);
     }
 
     int create(int nsys_, const int *sys_rows_, const int *Ai, const int *Aj, const double *Av, const int *Gi,

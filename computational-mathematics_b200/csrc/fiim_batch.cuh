@@ -230,19 +230,20 @@ __device__ __forceinline__ double widen(float v) { return (double)v; }
 // epilogue operand are loaded into registers before the barrier. A block whose system has
 // finished loads nothing and is skipped: a system's done flag changes only after all of its
 // blocks in the launch have been reduced, so the value read at prefetch is the one at use.
-template <int TILE, typename V, typename Epi>
+template <int TILE, typename V, typename Epi, bool NARROW = false>
 static __global__ void __launch_bounds__(kThreads, 4)
 k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, const int *__restrict__ bflag,
-        int nblk, const double *__restrict__ x, Epi epi, BState bs, double *__restrict__ partials) {
+        int nblk, const double *__restrict__ x, Epi epi, BState bs, double *__restrict__ partials,
+        NarrowCols nc = NarrowCols{}) {
     pdl_enter();
     __shared__ double prod[TILE];
     constexpr int PER = TILE / kThreads;
     const int tid = (int)threadIdx.x;
-    int r0 = 0, r1 = 0, e0 = 0, e1 = 0, rbeg = 0, rend = 0;
+    int r0 = 0, r1 = 0, e0 = 0, e1 = 0, rbeg = 0, rend = 0, cbase = 0;
     bool skip = false;
     double opnd = 0.0;
     using VP = ValPair<V>;
-    int c[PER];
+    ColRegs<NARROW, PER> c;
     typename VP::T a[PER / 2];
     auto fetch = [&](int blk) {
         r0 = __ldg(rb + blk);
@@ -251,6 +252,7 @@ k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, co
         e1 = __ldg(eb + blk + 1);
         skip = Epi::GATED && bflag[blk];   // flags change only in the finish kernels
         if (skip) return;
+        if constexpr (NARROW) cbase = __ldg(nc.base + blk);
         rbeg = rend = 0;
         if (r0 + tid < r1) {
             rbeg = __ldg(M.rp + r0 + tid);
@@ -262,15 +264,13 @@ k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, co
 #pragma unroll
             for (int u = 0; u < PER / 2; ++u) {
                 const int e = a0 + 2 * (tid + u * kThreads);
-                c[2 * u] = c[2 * u + 1] = 0;
+                c.zero(u);
                 a[u] = VP::zero();
                 if (e + 1 < e1) {
-                    const int2 cc = ldi2(M.ci + e);
-                    c[2 * u] = cc.x;
-                    c[2 * u + 1] = cc.y;
+                    c.load2(M.ci, nc, e, u);
                     a[u] = VP::load2(M.v + e);
                 } else if (e < e1) {
-                    c[2 * u] = ldi(M.ci + e);
+                    c.load1(M.ci, nc, e, u);
                     a[u] = VP::load1(M.v + e);
                 }
             }
@@ -279,7 +279,7 @@ k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, co
     if ((int)blockIdx.x < nblk) fetch(blockIdx.x);
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
         const int nxt = blk + (int)gridDim.x;
-        const int cr0 = r0, cr1 = r1, ce0 = e0, ce1 = e1, cb = rbeg - e0, ce = rend - e0;
+        const int cr0 = r0, cr1 = r1, ce0 = e0, ce1 = e1, cb = rbeg - e0, ce = rend - e0, cbs = cbase;
         const double copnd = opnd;
         if (skip) {                                         // uniform in the CTA
             if (nxt < nblk) fetch(nxt);
@@ -293,7 +293,8 @@ k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, co
 #pragma unroll
             for (int u = 0; u < PER; ++u) {
                 const int e = a0 + 2 * (tid + (u >> 1) * kThreads) + (u & 1);
-                if (e >= ce0 && e < ce1) prod[e - ce0] = __dmul_rn(widen(VP::get(a[u >> 1], u & 1)), ldx(x + c[u]));
+                if (e >= ce0 && e < ce1)
+                    prod[e - ce0] = __dmul_rn(widen(VP::get(a[u >> 1], u & 1)), ldx(x + c.get(u, cbs)));
             }
             if (nxt < nblk) fetch(nxt);
             __syncthreads();
@@ -308,8 +309,10 @@ k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, co
             double s = 0.0;
             for (int c0 = ce0; c0 < ce1; c0 += TILE) {
                 const int c1 = min(c0 + TILE, ce1);
-                for (int e = c0 + tid; e < c1; e += kThreads)
-                    prod[e - c0] = __dmul_rn(widen(ldm(M.v + e)), ldx(x + ldi(M.ci + e)));
+                for (int e = c0 + tid; e < c1; e += kThreads) {
+                    const int j = NARROW ? cbs + (int)__ldcs(nc.d + e) : ldi(M.ci + e);
+                    prod[e - c0] = __dmul_rn(widen(ldm(M.v + e)), ldx(x + j));
+                }
                 __syncthreads();
                 if (tid == 0)
                     for (int q = 0; q < c1 - c0; ++q) s = __dadd_rn(s, prod[q]);

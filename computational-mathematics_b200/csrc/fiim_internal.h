@@ -95,6 +95,8 @@ int carve_csr(Arena &ar, DevCsr &M, long n, long nnz);
 int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, const double *v, int fill,
                bool device_src, cudaStream_t s, unsigned long long *d_count, unsigned long long *h_count);
 int set_tile(DevCsr &M, int tile, cudaStream_t s);
+// Builds the narrow column stream (cd, cb) of M's row blocks (eb) when every block allows it.
+int build_narrow(DevCsr &M, cudaStream_t s);
 void expand_sym_upper(int n, const int *rp, const int *ci, const double *v, HostCsr &out);
 void transpose_upper(int n, const int *rp, const int *ci, const double *v, HostCsr &out);
 

@@ -37,10 +37,16 @@ CsrView<double> view64(const DevCsr &M) { return CsrView<double>{M.rp, M.ci, M.v
 template <int TILE, typename V, typename Epi>
 cudaError_t rows_f(cudaStream_t s, const DevCsr &M, const V *vals, const float *x, const Epi &epi,
                    DState *st, double *partials) {
-    auto kern = mx::k_spmv_rows_f<TILE, V, Epi>;
+    if (M.narrow) {
+        auto kern = mx::k_spmv_rows_f<TILE, V, Epi, true>;
+        const int g = grid_for(kern, 1, M.nblk);
+        return launch_k(kern, g, 0, s, CsrView<V>{M.rp, M.ci, vals, (int)M.n}, M.rb, M.eb, M.nblk, x, epi, st,
+                        partials, NarrowCols{M.cd, M.cb});
+    }
+    auto kern = mx::k_spmv_rows_f<TILE, V, Epi, false>;
     const int g = grid_for(kern, 1, M.nblk);
     return launch_k(kern, g, 0, s, CsrView<V>{M.rp, M.ci, vals, (int)M.n}, M.rb, M.eb, M.nblk, x, epi, st,
-                    partials);
+                    partials, NarrowCols{});
 }
 
 template <typename V, typename Epi>

@@ -77,14 +77,16 @@ __device__ __forceinline__ float ldv(const float *p) { return __ldcs(p); }
 __device__ __forceinline__ float ldv(const __nv_bfloat16 *p) { return ldm(p); }
 
 // CSR-stream SpMV on FP32 / BF16 values and an FP32 vector, with the FP64 kernel's row
-// blocks (at most TILE - 1 entries, bounds rb / eb) and structure: entries read in aligned
+// blocks (at most TILE - 1 entries, bounds rb / eb), column streams (32-bit or NARROW) and
+// structure: entries read in aligned
 // pairs, the next block's bounds, row offsets, entry streams and epilogue operands loaded
 // into registers before the barrier, products staged in shared memory, each row summed in
 // storage order.
-template <int TILE, typename V, typename Epi>
+template <int TILE, typename V, typename Epi, bool NARROW = false>
 static __global__ void __launch_bounds__(kThreads)
 k_spmv_rows_f(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, int nblk,
-              const float *__restrict__ x, Epi epi, DState *st, double *__restrict__ partials) {
+              const float *__restrict__ x, Epi epi, DState *st, double *__restrict__ partials,
+              NarrowCols nc = NarrowCols{}) {
     pdl_enter();
     if (Epi::GATED && st != nullptr && st->done) return;
     __shared__ float prod[TILE];
@@ -93,16 +95,17 @@ k_spmv_rows_f(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ 
     double red[Epi::NR];
 #pragma unroll
     for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
-    int r0 = 0, r1 = 0, e0 = 0, e1 = 0, rbeg = 0, rend = 0;
+    int r0 = 0, r1 = 0, e0 = 0, e1 = 0, rbeg = 0, rend = 0, cbase = 0;
     float opnd = 0.f;
     using VP = ValPair<V>;
-    int c[PER];
+    ColRegs<NARROW, PER> c;
     typename VP::T a[PER / 2];
     auto fetch = [&](int blk) {
         r0 = __ldg(rb + blk);
         r1 = __ldg(rb + blk + 1);
         e0 = __ldg(eb + blk);
         e1 = __ldg(eb + blk + 1);
+        if constexpr (NARROW) cbase = __ldg(nc.base + blk);
         rbeg = rend = 0;
         if (r0 + tid < r1) {
             rbeg = __ldg(M.rp + r0 + tid);
@@ -114,15 +117,13 @@ k_spmv_rows_f(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ 
 #pragma unroll
             for (int u = 0; u < PER / 2; ++u) {
                 const int e = a0 + 2 * (tid + u * kThreads);
-                c[2 * u] = c[2 * u + 1] = 0;
+                c.zero(u);
                 a[u] = VP::zero();
                 if (e + 1 < e1) {
-                    const int2 cc = ldi2(M.ci + e);
-                    c[2 * u] = cc.x;
-                    c[2 * u + 1] = cc.y;
+                    c.load2(M.ci, nc, e, u);
                     a[u] = VP::load2(M.v + e);
                 } else if (e < e1) {
-                    c[2 * u] = ldi(M.ci + e);
+                    c.load1(M.ci, nc, e, u);
                     a[u] = VP::load1(M.v + e);
                 }
             }
@@ -131,14 +132,14 @@ k_spmv_rows_f(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ 
     if ((int)blockIdx.x < nblk) fetch(blockIdx.x);
     for (int blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
         const int nxt = blk + (int)gridDim.x;
-        const int cr0 = r0, cr1 = r1, ce0 = e0, ce1 = e1, cb = rbeg - e0, ce = rend - e0;
+        const int cr0 = r0, cr1 = r1, ce0 = e0, ce1 = e1, cb = rbeg - e0, ce = rend - e0, cbs = cbase;
         const float copnd = opnd;
         if (ce1 - ce0 < TILE) {
             const int a0 = ce0 & ~1;
 #pragma unroll
             for (int u = 0; u < PER; ++u) {
                 const int e = a0 + 2 * (tid + (u >> 1) * kThreads) + (u & 1);
-                if (e >= ce0 && e < ce1) prod[e - ce0] = VP::get(a[u >> 1], u & 1) * ldx(x + c[u]);
+                if (e >= ce0 && e < ce1) prod[e - ce0] = VP::get(a[u >> 1], u & 1) * ldx(x + c.get(u, cbs));
             }
             if (nxt < nblk) fetch(nxt);
             __syncthreads();
@@ -153,7 +154,10 @@ k_spmv_rows_f(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ 
             float s = 0.f;
             for (int c0 = ce0; c0 < ce1; c0 += TILE) {
                 const int c1 = min(c0 + TILE, ce1);
-                for (int e = c0 + tid; e < c1; e += kThreads) prod[e - c0] = ldv(M.v + e) * ldx(x + ldi(M.ci + e));
+                for (int e = c0 + tid; e < c1; e += kThreads) {
+                    const int j = NARROW ? cbs + (int)__ldcs(nc.d + e) : ldi(M.ci + e);
+                    prod[e - c0] = ldv(M.v + e) * ldx(x + j);
+                }
                 __syncthreads();
                 if (tid == 0)
                     for (int k = 0; k < c1 - c0; ++k) s += prod[k];

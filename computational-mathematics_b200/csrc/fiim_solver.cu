@@ -222,15 +222,7 @@ void build_row_blocks(const std::vector<int> &rp, int tile, int max_rows, std::v
     }
 }
 
-int set_tile(DevCsr &M, int tile, cudaStream_t s) {
-    std::vector<int> rb;
-    build_row_blocks(M.hrp, tile - 1, kThreads, rb);   // k_spmv_rows reads aligned pairs
-    M.tile = tile;
-    M.nblk = (int)rb.size() - 1;
-    std::vector<int> eb(rb.size());
-    for (size_t k = 0; k < rb.size(); ++k) eb[k] = M.hrp[rb[k]];
-    FIIM_CUDA(cudaMemcpyAsync(M.rb, rb.data(), sizeof(int) * rb.size(), cudaMemcpyHostToDevice, s));
-    FIIM_CUDA(cudaMemcpyAsync(M.eb, eb.data(), sizeof(int) * eb.size(), cudaMemcpyHostToDevice, s));
+int build_narrow(DevCsr &M, cudaStream_t s) {
     // Narrow column stream when every row block allows it (FIIM_COLS=wide keeps 32-bit columns).
     M.narrow = 0;
     const char *cols = std::getenv("FIIM_COLS");
@@ -244,6 +236,19 @@ int set_tile(DevCsr &M, int tile, cudaStream_t s) {
         FIIM_CUDA(cudaStreamSynchronize(s));
         M.narrow = wide ? 0 : 1;
     }
+    return FIIM_OK;
+}
+
+int set_tile(DevCsr &M, int tile, cudaStream_t s) {
+    std::vector<int> rb;
+    build_row_blocks(M.hrp, tile - 1, kThreads, rb);   // k_spmv_rows reads aligned pairs
+    M.tile = tile;
+    M.nblk = (int)rb.size() - 1;
+    std::vector<int> eb(rb.size());
+    for (size_t k = 0; k < rb.size(); ++k) eb[k] = M.hrp[rb[k]];
+    FIIM_CUDA(cudaMemcpyAsync(M.rb, rb.data(), sizeof(int) * rb.size(), cudaMemcpyHostToDevice, s));
+    FIIM_CUDA(cudaMemcpyAsync(M.eb, eb.data(), sizeof(int) * eb.size(), cudaMemcpyHostToDevice, s));
+    FIIM_TRY(build_narrow(M, s));
     FIIM_CUDA(cudaStreamSynchronize(s));
     return FIIM_OK;
 }
