@@ -25,6 +25,15 @@ def test_shard_by_nnz_covers_every_unit_once():
     assert FB.shard_by_nnz([5], 2, 1) in ((1, 1), (0, 1))
 
 
+def test_rhs_shards_are_contiguous_and_even():
+    """The multi-RHS leg gives each rank a contiguous share of the 32 right-hand sides."""
+    for world in (1, 2, 4, 8):
+        shards = [FB.shard_by_nnz([1] * 32, world, r) for r in range(world)]
+        assert shards[0][0] == 0 and shards[-1][1] == 32
+        assert all(b == c for (_, b), (c, _) in zip(shards, shards[1:]))
+        assert {b - a for a, b in shards} == {32 // world}
+
+
 def _free_port():
     s = socket.socket()
     s.bind(("127.0.0.1", 0))
