@@ -43,6 +43,7 @@ EXPORTS = (
     "fiim_spmv", "fiim_prec_apply", "fiim_prec_apply_noalloc",
     "fiim_gen_poisson2d", "fiim_gen_convdiff3d", "fiim_gen_convdiff2d", "fiim_gen_batch_params",
     "fiim_gen_zipf", "fiim_gen_zipf_mean", "fiim_rand_normal", "fiim_model_rhs", "fiim_pdfiim_build",
+    "fiim_read_mtx", "fiim_read_rhs", "fiim_factors_save", "fiim_factors_load",
 )
 
 
@@ -496,6 +497,49 @@ def pdfiim_build(A, ftol, prefill=1, lfill=1, postfill=1, warpsize=-1, filttype=
          "Hi": np.zeros(n + 1, np.int32)}
     _check(L.fiim_pdfiim_build(*args, C.byref(ng), C.byref(nh), _ptr(F["Gv"]), _ptr(F["Gj"]), _ptr(F["Gi"]),
                                _ptr(F["IDv"]), _ptr(F["Hv"]), _ptr(F["Hj"]), _ptr(F["Hi"])))
+    return F
+
+
+def read_mtx(path, form="afiim"):
+    """Matrix Market matrix -> ((Ai, Aj, Av), issym), the same arrays as the reference's
+    reader: form 'afiim' (also ACIFIM) expands a symmetric file, 'pdfiim' keeps its upper
+    triangle and returns issym = True."""
+    n, z, sym = C.c_int(0), C.c_int(0), C.c_int(0)
+    f = 1 if form == "pdfiim" else 0
+    _check(lib().fiim_read_mtx(os.fsencode(path), C.c_int(f), C.byref(n), C.byref(z), C.byref(sym),
+                               None, None, None))
+    Ai, Aj, Av = np.zeros(n.value + 1, np.int32), np.zeros(z.value, np.int32), np.zeros(z.value)
+    _check(lib().fiim_read_mtx(None, C.c_int(f), C.byref(n), C.byref(z), C.byref(sym), _ptr(Ai), _ptr(Aj),
+                               _ptr(Av)))
+    return (Ai, Aj, Av), bool(sym.value)
+
+
+def read_rhs(path):
+    n = C.c_int(0)
+    _check(lib().fiim_read_rhs(os.fsencode(path), C.c_int(0), None, C.byref(n)))
+    b = np.zeros(n.value)
+    _check(lib().fiim_read_rhs(os.fsencode(path), C.c_int(n.value), _ptr(b), C.byref(n)))
+    return b
+
+
+def factors_save(path, F):
+    """Writes G, D^{-1}, H of a factor dict (Gi, Gj, Gv, IDv, Hi, Hj, Hv) to a binary file."""
+    Gi, Gj, Gv = _i(F["Gi"]), _i(F["Gj"]), _d(F["Gv"])
+    Hi, Hj, Hv = _i(F["Hi"]), _i(F["Hj"]), _d(F["Hv"])
+    _check(lib().fiim_factors_save(os.fsencode(path), C.c_int(len(Gi) - 1), _ptr(Gi), _ptr(Gj), _ptr(Gv),
+                                   _ptr(_d(F["IDv"])), _ptr(Hi), _ptr(Hj), _ptr(Hv)))
+
+
+def factors_load(path):
+    n, ng, nh = C.c_int(0), C.c_int(0), C.c_int(0)
+    L = lib()
+    _check(L.fiim_factors_load(os.fsencode(path), C.byref(n), C.byref(ng), C.byref(nh), None, None, None, None,
+                               None, None, None))
+    F = {"Gi": np.zeros(n.value + 1, np.int32), "Gj": np.zeros(ng.value, np.int32), "Gv": np.zeros(ng.value),
+         "IDv": np.zeros(n.value), "Hi": np.zeros(n.value + 1, np.int32), "Hj": np.zeros(nh.value, np.int32),
+         "Hv": np.zeros(nh.value)}
+    _check(L.fiim_factors_load(None, C.byref(n), C.byref(ng), C.byref(nh), *[_ptr(F[k]) for k in
+                               ("Gi", "Gj", "Gv", "IDv", "Hi", "Hj", "Hv")]))
     return F
 
 

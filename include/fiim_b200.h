@@ -273,6 +273,33 @@ int fiim_pdfiim_build(int n, const int *Ai, const int *Aj, const double *Av, int
                       char patt, int *nnzG, int *nnzH, double *Gv, int *Gj, int *Gi,
                       double *D, double *Hv, int *Hj, int *Hi);
 
+/* ===========================================================================
+ * Host input/output around the solve (no GPU needed).
+ * ======================================================================== */
+
+/* Reads a Matrix Market "coordinate real general|symmetric" square matrix into 0-based CSR
+ * with each row sorted by column, giving the same arrays as the reference's readers:
+ * form 0 as AFIIM/ACIFIM's read_coeff_matrix (AFIIM/src/rw_matrix.cpp:62-216: a symmetric
+ * file is expanded to general), form 1 as PDFIIM's (PDFIIM/src/rw_matrix.cpp:60-150: a
+ * symmetric file is kept as the upper triangle and *issym = 1). Two calls: first with
+ * Ai == NULL returns *n and *nnz and keeps the matrix in a buffer bound to the calling
+ * thread; the second (same *n, *nnz) copies it out. Unsupported types return FIIM_EARG. */
+int fiim_read_mtx(const char *path, int form, int *n, int *nnz, int *issym, int *Ai, int *Aj,
+                  double *Av);
+
+/* Reads a Matrix Market "array real general" n x 1 vector (AFIIM/src/rw_matrix.cpp:246-309).
+ * b == NULL: returns the length through *n; otherwise fills b[0..*n) (at most cap). */
+int fiim_read_rhs(const char *path, int cap, double *b, int *n);
+
+/* Binary factor file of G, D^{-1}, H (little-endian, checksummed), so that a factor
+ * construction can be stored and reused. No counterpart in the reference. Load is two
+ * calls: first with Gi == NULL returns *n, *nnzG, *nnzH (damaged or truncated files and
+ * checksum mismatches return FIIM_EARG); the second copies the factors out. */
+int fiim_factors_save(const char *path, int n, const int *Gi, const int *Gj, const double *Gv,
+                      const double *IDv, const int *Hi, const int *Hj, const double *Hv);
+int fiim_factors_load(const char *path, int *n, int *nnzG, int *nnzH, int *Gi, int *Gj, double *Gv,
+                      double *IDv, int *Hi, int *Hj, double *Hv);
+
 #ifdef __cplusplus
 }
 #endif
