@@ -42,7 +42,7 @@ EXPORTS = (
     "fiim_block_create", "fiim_block_solve", "fiim_block_destroy",
     "fiim_spmv", "fiim_prec_apply", "fiim_prec_apply_noalloc",
     "fiim_gen_poisson2d", "fiim_gen_convdiff3d", "fiim_gen_convdiff2d", "fiim_gen_batch_params",
-    "fiim_gen_zipf", "fiim_gen_zipf_mean", "fiim_rand_normal", "fiim_model_rhs", "fiim_pdfiim_build",
+    "fiim_gen_zipf", "fiim_gen_zipf_mean", "fiim_rand_normal", "fiim_model_rhs", "fiim_pdfiim_build", "fiim_pdfiim_build_gpu",
     "fiim_read_mtx", "fiim_read_rhs", "fiim_factors_save", "fiim_factors_load",
 )
 
@@ -481,21 +481,25 @@ def model_rhs(A):
     return b
 
 
-def pdfiim_build(A, ftol, prefill=1, lfill=1, postfill=1, warpsize=-1, filttype="I", patt="B"):
-    """Host PDFIIM construction (same factors as PDFIIM/src/parPrec.cpp:95-588). Returns a factor dict."""
+def pdfiim_build(A, ftol, prefill=1, lfill=1, postfill=1, warpsize=-1, filttype="I", patt="B", gpu=False):
+    """PDFIIM construction (same factors as PDFIIM/src/parPrec.cpp:95-588), on the host or,
+    with gpu=True, on the GPU (the same factors bit for bit). Returns a factor dict."""
     Ai, Aj, Av = _i(A[0]), _i(A[1]), _d(A[2])
     n = len(Ai) - 1
     ng, nh = C.c_int(0), C.c_int(0)
     L = lib()
+    fn = L.fiim_pdfiim_build_gpu if gpu else L.fiim_pdfiim_build
     args = (C.c_int(n), _ptr(Ai), _ptr(Aj), _ptr(Av), C.c_int(prefill), C.c_int(lfill), C.c_int(postfill),
             C.c_double(ftol), C.c_int(warpsize), C.c_char(filttype.encode()), C.c_char(patt.encode()))
-    rc = L.fiim_pdfiim_build(*args, C.byref(ng), C.byref(nh), None, None, None, None, None, None, None)
+    rc = fn(*args, C.byref(ng), C.byref(nh), None, None, None, None, None, None, None)
     if rc != FIIM_OK:
+        if gpu:
+            _check(rc)
         raise FiimError(rc, "pdfiim_build rejected its arguments")
     F = {"Gv": np.zeros(ng.value), "Gj": np.zeros(ng.value, np.int32), "Gi": np.zeros(n + 1, np.int32),
          "IDv": np.zeros(n), "Hv": np.zeros(nh.value), "Hj": np.zeros(nh.value, np.int32),
          "Hi": np.zeros(n + 1, np.int32)}
-    _check(L.fiim_pdfiim_build(*args, C.byref(ng), C.byref(nh), _ptr(F["Gv"]), _ptr(F["Gj"]), _ptr(F["Gi"]),
+    _check(fn(*args, C.byref(ng), C.byref(nh), _ptr(F["Gv"]), _ptr(F["Gj"]), _ptr(F["Gi"]),
                                _ptr(F["IDv"]), _ptr(F["Hv"]), _ptr(F["Hj"]), _ptr(F["Hi"])))
     return F
 
