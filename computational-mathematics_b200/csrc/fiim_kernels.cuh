@@ -590,11 +590,13 @@ struct FinS {
 
 // s = r + (-alpha) v (cblas_dcopy + cblas_daxpy, AFIIM/src/bicgstab.cpp:184-185);
 // ||r||^2 (the residual norm the reference tests, taken before r is updated, :216)
-// and ||x||^2 (stagnation test, :201).
+// and ||x||^2 (stagnation test, :201). Fin receives the two sums (FinS stores them in the
+// scalars; a row-partitioned solve exports its block's sums instead).
+template <class Fin>
 static __global__ void __launch_bounds__(kThreads)
 k_update_s(long n, const double *__restrict__ r, const double *__restrict__ v,
            const double *__restrict__ x, double *__restrict__ s, DState *st,
-           double *__restrict__ partials) {
+           double *__restrict__ partials, Fin fin) {
     pdl_enter();
     if (st->done) return;
     const double na = -st->alpha;
@@ -606,7 +608,7 @@ k_update_s(long n, const double *__restrict__ r, const double *__restrict__ v,
         red[1] += xi * xi;
     }
     pdl_release();
-    grid_reduce<2>(red, partials, st, FinS{});
+    grid_reduce<2>(red, partials, st, fin);
 }
 
 // Termination tests and the beta recurrence (AFIIM/src/bicgstab.cpp:201-274).
@@ -631,12 +633,13 @@ struct FinControl {
 };
 
 // x = x + alpha pc; x = x + omega sc; r = s + (-omega) t (AFIIM/src/bicgstab.cpp:207-259);
-// sum r0 . r; then the tests.
+// sum r0 . r; then the tests (Fin = FinControl; a row-partitioned solve exports the sum).
+template <class Fin>
 static __global__ void __launch_bounds__(kThreads)
 k_update_xr(long n, const double *__restrict__ pc, const double *__restrict__ sc,
             const double *__restrict__ s, const double *__restrict__ t,
             const double *__restrict__ r0, double *__restrict__ x, double *__restrict__ r,
-            DState *st, double *__restrict__ partials) {
+            DState *st, double *__restrict__ partials, Fin fin) {
     pdl_enter();
     if (st->done) return;
     const double a = st->alpha, om = st->omega, nom = -st->omega;
@@ -651,7 +654,7 @@ k_update_xr(long n, const double *__restrict__ pc, const double *__restrict__ sc
         red[0] += r0[i] * ri;
     }
     pdl_release();
-    grid_reduce<1>(red, partials, st, FinControl{});
+    grid_reduce<1>(red, partials, st, fin);
 }
 
 // p = (-beta omega) v + beta p; p = p + r (cblas_daxpby + cblas_daxpy,

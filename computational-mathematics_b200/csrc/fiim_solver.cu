@@ -524,11 +524,12 @@ int Solver::enqueue_iteration(bool cond, cudaGraphConditionalHandle h) {
     const long nn = n;
     FIIM_TRY(enqueue_prec(p, pc, true));                                             // K1-K2
     FIIM_CUDA(launch_spmv(A, s, pc, EpiAlpha{v, r0}, st, partials, fault));     // K3
-    FIIM_CUDA(launch_k(k_update_s, stream_grid(k_update_s, nn), 0, s, nn, r, v, x, sv, st, partials));  // K4
+    FIIM_CUDA(launch_k(k_update_s<FinS>, stream_grid(k_update_s<FinS>, nn), 0, s, nn, r, v, x, sv, st, partials,
+                       FinS{}));                                                        // K4
     FIIM_TRY(enqueue_prec(sv, sc, false));                                           // K5-K6
     FIIM_CUDA(launch_spmv(A, s, sc, EpiOmega{t, sv}, st, partials, fault));    // K7
-    FIIM_CUDA(launch_k(k_update_xr, stream_grid(k_update_xr, nn), 0, s, nn, pc, sc, sv, t, r0, x, r, st,
-                       partials));                                                      // K8
+    FIIM_CUDA(launch_k(k_update_xr<FinControl>, stream_grid(k_update_xr<FinControl>, nn), 0, s, nn, pc, sc, sv,
+                       t, r0, x, r, st, partials, FinControl{}));                       // K8
     FIIM_CUDA(launch_k(k_update_p, stream_grid(k_update_p, nn), 0, s, nn, r, v, p, st, h, cond ? 1 : 0));  // K9
     return FIIM_OK;
 }
@@ -914,10 +915,10 @@ int Solver::kernel_times(int reps, int max_k, double *ms, double *bytes, char *n
         {"H_spmv_scale", S(H) + 3 * nv, [&] { return launch_spmv(H, stream, p, EpiScale{tm, IDv}, st, partials, fault); }},
         {"G_spmv_norm", S(G) + 2 * nv, [&] { return launch_spmv(G, stream, tm, EpiNorm{pc}, st, partials, fault); }},
         {"A_spmv_alpha", S(A) + 3 * nv, [&] { return launch_spmv(A, stream, pc, EpiAlpha{v, r0}, st, partials, fault); }},
-        {"update_s", 4 * nv, [&] { k_update_s<<<stream_grid(k_update_s, nn), kThreads, 0, stream>>>(nn, r, v, x, sv, st, partials); return cudaGetLastError(); }},
+        {"update_s", 4 * nv, [&] { k_update_s<FinS><<<stream_grid(k_update_s<FinS>, nn), kThreads, 0, stream>>>(nn, r, v, x, sv, st, partials, FinS{}); return cudaGetLastError(); }},
         {"G_spmv", S(G) + 2 * nv, [&] { return launch_spmv(G, stream, tm, EpiStore{sc}, st, partials, fault); }},
         {"A_spmv_omega", S(A) + 3 * nv, [&] { return launch_spmv(A, stream, sc, EpiOmega{t, sv}, st, partials, fault); }},
-        {"update_xr", 8 * nv, [&] { k_update_xr<<<stream_grid(k_update_xr, nn), kThreads, 0, stream>>>(nn, pc, sc, sv, t, r0, x, r, st, partials); return cudaGetLastError(); }},
+        {"update_xr", 8 * nv, [&] { k_update_xr<FinControl><<<stream_grid(k_update_xr<FinControl>, nn), kThreads, 0, stream>>>(nn, pc, sc, sv, t, r0, x, r, st, partials, FinControl{}); return cudaGetLastError(); }},
         {"update_p", 4 * nv, [&] { k_update_p<<<stream_grid(k_update_p, nn), kThreads, 0, stream>>>(nn, r, v, p, st, cudaGraphConditionalHandle{}, 0); return cudaGetLastError(); }},
     };
     // Scalars that keep every kernel on its full path; the solver's vectors are

@@ -44,6 +44,8 @@ EXPORTS = (
     "fiim_gen_poisson2d", "fiim_gen_convdiff3d", "fiim_gen_convdiff2d", "fiim_gen_batch_params",
     "fiim_gen_zipf", "fiim_gen_zipf_mean", "fiim_rand_normal", "fiim_model_rhs", "fiim_pdfiim_build", "fiim_pdfiim_build_gpu",
     "fiim_read_mtx", "fiim_read_rhs", "fiim_factors_save", "fiim_factors_load",
+    "fiim_dist_unique_id", "fiim_dist_partition", "fiim_dist_plan", "fiim_dist_create", "fiim_dist_solve",
+    "fiim_dist_destroy", "fiim_dist_emulate",
 )
 
 
@@ -245,6 +247,120 @@ class Solver:
     def close(self):
         if self._h and self._h.value:
             lib().fiim_solver_destroy(self._h)
+            self._h = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ----------------------------------------------------------------------------- row-partitioned solve
+def _options(variant="afiim", memory="host", mode="E"):
+    o = Options()
+    lib().fiim_options_default(C.byref(o))
+    o.variant = _VARIANTS[variant]
+    o.memory = MEM_DEVICE if memory == "device" else MEM_HOST
+    o.mode = mode.encode()
+    return o
+
+
+def dist_partition(A, F, world):
+    """Contiguous row blocks balancing the rows' entries of A, G and H (row_starts, int64)."""
+    n = len(A[0]) - 1
+    rs = np.zeros(world + 1, np.int64)
+    Gi = None if F is None else _i(F["Gi"])
+    Hi = None if F is None else _i(F["Hi"])
+    _check(lib().fiim_dist_partition(C.c_int(n), _ptr(_i(A[0])), _ptr(Gi), _ptr(Hi), C.c_int(world), _ptr(rs)))
+    return rs
+
+
+def dist_rows(M, lo, hi):
+    """Rows [lo, hi) of a CSR matrix (rp, ci, v) with global columns, offsets from the block's
+    first entry: what rank r is given in a row-partitioned solve."""
+    rp, ci, v = M
+    e0, e1 = int(rp[lo]), int(rp[hi])
+    return _i(np.asarray(rp[lo:hi + 1]) - e0), _i(ci[e0:e1]), _d(v[e0:e1])
+
+
+def dist_local(A, F, row_starts, rank):
+    """Rank `rank`'s rows of A, G, D^{-1} and H."""
+    lo, hi = int(row_starts[rank]), int(row_starts[rank + 1])
+    Al = dist_rows(A, lo, hi)
+    Gl = dist_rows((F["Gi"], F["Gj"], F["Gv"]), lo, hi)
+    Hl = dist_rows((F["Hi"], F["Hj"], F["Hv"]), lo, hi)
+    Fl = {"Gi": Gl[0], "Gj": Gl[1], "Gv": Gl[2], "IDv": _d(F["IDv"][lo:hi]), "Hi": Hl[0], "Hj": Hl[1], "Hv": Hl[2]}
+    return Al, Fl
+
+
+def dist_plan(rank, world, row_starts, M, fill=0):
+    """One matrix's plan on one rank (host only): halo (below, then above), the kept row
+    offsets and the renumbered columns. M is the rank's rows (dist_rows)."""
+    rs = np.ascontiguousarray(row_starts, dtype=np.int64)
+    rp, ci = _i(M[0]), _i(M[1])
+    nb, na, nk = C.c_int(0), C.c_int(0), C.c_int(0)
+    L = lib()
+    _check(L.fiim_dist_plan(C.c_int(rank), C.c_int(world), _ptr(rs), _ptr(rp), _ptr(ci), C.c_int(fill),
+                            C.byref(nb), C.byref(na), C.byref(nk), None, None, None))
+    halo, krp, cols = np.zeros(nb.value + na.value, np.int32), np.zeros(len(rp), np.int32), np.zeros(nk.value, np.int32)
+    _check(L.fiim_dist_plan(C.c_int(rank), C.c_int(world), _ptr(rs), _ptr(rp), _ptr(ci), C.c_int(fill),
+                            C.byref(nb), C.byref(na), C.byref(nk), _ptr(halo), _ptr(krp), _ptr(cols)))
+    return {"nbelow": nb.value, "nabove": na.value, "halo": halo, "rp": krp, "cols": cols}
+
+
+def dist_emulate(A, F, b, x, world, tol=1e-8, nmax=1000, variant="afiim", row_starts=None):
+    """The row-partitioned solve of `world` row blocks in this process on one GPU (device
+    copies in place of NCCL; the same bits as a world-GPU run). x is updated in place."""
+    rs = dist_partition(A, F, world) if row_starts is None else np.ascontiguousarray(row_starts, dtype=np.int64)
+    n = len(A[0]) - 1
+    assert x.dtype == np.float64 and x.flags.c_contiguous
+    o = _options(variant)
+    r = Result()
+    _check(lib().fiim_dist_emulate(
+        C.c_int(world), _ptr(rs), C.c_int(n), _ptr(_i(A[0])), _ptr(_i(A[1])), _ptr(_d(A[2])),
+        _ptr(_i(F["Gi"])), _ptr(_i(F["Gj"])), _ptr(_d(F["Gv"])), _ptr(_d(F["IDv"])),
+        _ptr(_i(F["Hi"])), _ptr(_i(F["Hj"])), _ptr(_d(F["Hv"])), _ptr(_d(b)), _ptr(x),
+        C.c_double(tol), C.c_int(nmax), C.byref(o), C.byref(r)))
+    return r.as_dict()
+
+
+def dist_unique_id() -> bytes:
+    """NCCL unique id for a DistSolver communicator (make it on one rank, share it)."""
+    buf = (C.c_ubyte * 128)()
+    _check(lib().fiim_dist_unique_id(buf))
+    return bytes(buf)
+
+
+class DistSolver:
+    """One rank of a row-partitioned solve (one process per GPU). Collective: every rank
+    constructs it with the same uid, world and row_starts, and calls solve together.
+
+    A_local, F_local: this rank's rows (dist_local); b and x of solve: this rank's rows,
+    numpy (memory='host') or torch CUDA tensors (memory='device')."""
+
+    def __init__(self, rank, world, uid, row_starts, A_local, F_local, variant="afiim", memory="host", device=-1):
+        self._h = C.c_void_p(0)
+        self.memory = memory
+        o = _options(variant, memory)
+        rs = np.ascontiguousarray(row_starts, dtype=np.int64)
+        idb = (C.c_ubyte * 128).from_buffer_copy(uid)
+        keep = [_i(A_local[0]), _i(A_local[1]), _d(A_local[2]), _i(F_local["Gi"]), _i(F_local["Gj"]),
+                _d(F_local["Gv"]), _d(F_local["IDv"]), _i(F_local["Hi"]), _i(F_local["Hj"]), _d(F_local["Hv"])]
+        _check(lib().fiim_dist_create(C.byref(self._h), C.c_int(rank), C.c_int(world), idb, C.c_int(device),
+                                      _ptr(rs), *[_ptr(a) for a in keep], C.byref(o)))
+
+    def solve(self, b, x, tol=1e-8, nmax=1000) -> dict:
+        r = Result()
+        if self.memory != "device":
+            b = _d(b)
+            assert x.dtype == np.float64 and x.flags.c_contiguous
+        _check(lib().fiim_dist_solve(self._h, _ptr(b), _ptr(x), C.c_double(tol), C.c_int(nmax), C.byref(r)))
+        return r.as_dict()
+
+    def close(self):
+        if self._h and self._h.value:
+            lib().fiim_dist_destroy(self._h)
             self._h = C.c_void_p(0)
 
     def __del__(self):

@@ -284,6 +284,66 @@ int fiim_pdfiim_build_gpu(int n, const int *Ai, const int *Aj, const double *Av,
                           double *D, double *Hv, int *Hj, int *Hi);
 
 /* ===========================================================================
+ * Row-partitioned solve of one system over several GPUs (one process per GPU).
+ * No counterpart in the reference, whose solve runs on one node's cores.
+ *
+ * Rank r owns rows [row_starts[r], row_starts[r+1]) of A, G, D^{-1} and H and is given
+ * exactly those rows, with GLOBAL column indices (row offsets 0-based at the block's first
+ * row). Each iteration exchanges the halo entries each product needs (NCCL send/recv) and
+ * gathers the ranks' partial dot products (NCCL all-gather); the gathered partials are
+ * summed in rank order on every rank, so all ranks take the same termination decision.
+ * Every rank's rows of every vector are computed as the single-GPU solve computes them;
+ * the dot products differ from it in summation order only. Variants: AFIIM, PDFIIM with
+ * the full (expanded) A and H, ACIFIM mode 'E'; FP64.
+ * ======================================================================== */
+#define FIIM_DIST_ID_BYTES 128
+typedef struct fiim_dist_s *fiim_dist_t;
+
+/* NCCL unique id for a new communicator (call on one rank, pass to all).
+ * NCCL is loaded at run time: an already loaded libnccl.so.2 (PyTorch's) or the one named
+ * by FIIM_NCCL_LIB; FIIM_ENODEV if none loads. */
+int fiim_dist_unique_id(unsigned char *id);
+
+/* Contiguous row blocks balancing each rank's streamed entries (rows of A, G, H; G and H
+ * may be NULL): row_starts[0..world], each block at least one row. Host only. */
+int fiim_dist_partition(int n, const int *Ai, const int *Gi, const int *Hi, int world,
+                        int64_t *row_starts);
+
+/* Host-only view of one matrix's plan on one rank (for inspection and tests): the rows
+ * [row_starts[rank], +nloc) given by Mi (local offsets) and Mj (global columns); fill 1 keeps
+ * col >= row (G), 2 keeps col <= row (H). Returns the halo (nbelow columns below the block,
+ * then nabove above, ascending), the kept row offsets rp[nloc+1] and the renumbered columns
+ * cols[nkept] (extended layout: halo below, owned rows, halo above). halo, rp, cols may be
+ * NULL to query sizes. */
+int fiim_dist_plan(int rank, int world, const int64_t *row_starts, const int *Mi, const int *Mj,
+                   int fill, int *nbelow, int *nabove, int *nkept, int *halo, int *rp, int *cols);
+
+/* Collective over all ranks: every rank calls it with the same id, world and row_starts.
+ * device >= 0 selects the GPU (else the current one). Matrix arrays are host arrays, read
+ * during the call; opt->memory says where solve's b and x live. Set-up errors are agreed
+ * among the ranks, so that all of them return the same failure. */
+int fiim_dist_create(fiim_dist_t *out, int rank, int world, const unsigned char *id, int device,
+                     const int64_t *row_starts, const int *Ai, const int *Aj, const double *Av,
+                     const int *Gi, const int *Gj, const double *Gv, const double *IDv,
+                     const int *Hi, const int *Hj, const double *Hv, const fiim_options *opt);
+
+/* Collective: b and x are this rank's rows. res->device_ms is this rank's device time;
+ * every other field is the same on all ranks. */
+int fiim_dist_solve(fiim_dist_t h, const double *b, double *x, double tol, int NMAX,
+                    fiim_result *res);
+int fiim_dist_destroy(fiim_dist_t h);
+
+/* All `world` row blocks of one system in this process, on the current GPU: the same
+ * per-rank kernels, launch shapes and step order as fiim_dist_create/solve, with device
+ * copies in place of NCCL, so its results are those of a world-GPU run, bit for bit. Global
+ * host arrays; res->launches counts every block's kernels. */
+int fiim_dist_emulate(int world, const int64_t *row_starts, int n, const int *Ai, const int *Aj,
+                      const double *Av, const int *Gi, const int *Gj, const double *Gv,
+                      const double *IDv, const int *Hi, const int *Hj, const double *Hv,
+                      const double *b, double *x, double tol, int NMAX, const fiim_options *opt,
+                      fiim_result *res);
+
+/* ===========================================================================
  * Host input/output around the solve (no GPU needed).
  * ======================================================================== */
 

@@ -74,3 +74,161 @@ def test_two_rank_sharding_and_max_over_ranks():
     for rank, got, tmax in out:
         assert tmax == 11.0
         assert got[0][0] == 0 and got[0][1] == got[1][0] and got[1][1] == 256
+
+
+# ----------------------------------------------------------------------------- row-partitioned solve
+def _system(N=6):
+    A = FB.gen_convdiff3d(N, 0.5)
+    F = FB.pdfiim_build(A, 0.05, 2, 2, 1)
+    return A, F
+
+
+def _row_sums(rp, ci, v, x):
+    """CSR product, each row summed left to right with the product rounded first (the
+    solve's exact-order SpMV)."""
+    y = np.zeros(len(rp) - 1)
+    for i in range(len(rp) - 1):
+        s = 0.0
+        for k in range(rp[i], rp[i + 1]):
+            s = s + float(v[k]) * float(x[ci[k]])
+        y[i] = s
+    return y
+
+
+def _keep(M, fill):
+    """The triangle the solve applies to G (fill 1) and H (fill 2), as global CSR."""
+    rp, ci, v = M
+    orp, oci, ov = [0], [], []
+    for i in range(len(rp) - 1):
+        for k in range(rp[i], rp[i + 1]):
+            if (fill == 1 and ci[k] < i) or (fill == 2 and ci[k] > i):
+                continue
+            oci.append(ci[k])
+            ov.append(v[k])
+        orp.append(len(oci))
+    return np.array(orp), np.array(oci), np.array(ov)
+
+
+def test_dist_partition_covers_rows_and_balances():
+    A, F = _system(8)
+    n = len(A[0]) - 1
+    w = 1 + np.diff(A[0]) + np.diff(F["Gi"]) + np.diff(F["Hi"])
+    for world in (1, 2, 3, 4, 7, 8, n):
+        rs = FB.dist_partition(A, F, world)
+        assert rs[0] == 0 and rs[-1] == n and len(rs) == world + 1
+        assert (np.diff(rs) >= 1).all()
+        loads = np.add.reduceat(w, rs[:-1])
+        assert loads.max() <= w.sum() / world + w.max()
+    with pytest.raises(FB.FiimError):
+        FB.dist_partition(A, F, n + 1)
+
+
+@pytest.mark.parametrize("world", [2, 3, 5])
+def test_dist_plan_renumbers_monotonically(world):
+    """Every rank's renumbered columns map back to the kept global columns in stored order,
+    and the halo is exactly the referenced columns outside the rank's rows."""
+    A, F = _system(6)
+    rs = FB.dist_partition(A, F, world)
+    mats = [(A, 0), ((F["Gi"], F["Gj"], F["Gv"]), 1), ((F["Hi"], F["Hj"], F["Hv"]), 2)]
+    for M, fill in mats:
+        Kp, Kc, _ = _keep(M, fill)
+        for r in range(world):
+            lo, hi = int(rs[r]), int(rs[r + 1])
+            nloc = hi - lo
+            p = FB.dist_plan(r, world, rs, FB.dist_rows(M, lo, hi), fill)
+            nb, halo, cols = p["nbelow"], p["halo"], p["cols"]
+            ext_to_global = np.concatenate([halo[:nb], np.arange(lo, hi), halo[nb:]])
+            back = ext_to_global[cols]
+            assert len(ext_to_global) == nb + nloc + p["nabove"]
+            assert np.array_equal(p["rp"], Kp[lo:hi + 1] - Kp[lo])
+            assert np.array_equal(back, Kc[Kp[lo]:Kp[hi]])
+            ref = np.unique(Kc[Kp[lo]:Kp[hi]])
+            ref = ref[(ref < lo) | (ref >= hi)]
+            assert np.array_equal(halo, ref)
+            assert (halo[:nb] < lo).all() and (halo[nb:] >= hi).all()
+            if fill == 1:
+                assert nb == 0     # G (upper) reaches only rows above the block
+            if fill == 2:
+                assert p["nabove"] == 0
+
+
+def _dist_rank(rank, world, port, q):
+    """One rank: plan A, G, H; exchange the needs and the halo values over gloo as the
+    solve does over NCCL; multiply; gather a partial dot product in rank order."""
+    import torch
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    A, F = _system(6)
+    n = len(A[0]) - 1
+    rs = FB.dist_partition(A, F, world)
+    lo, hi = int(rs[rank]), int(rs[rank + 1])
+    x = FB.rand_normal(n, 11)                 # every rank knows only x[lo:hi] below
+    x_own = x[lo:hi].copy()
+    out = {}
+    for name, M, fill in (("A", A, 0), ("G", (F["Gi"], F["Gj"], F["Gv"]), 1), ("H", (F["Hi"], F["Hj"], F["Hv"]), 2)):
+        Ml = FB.dist_rows(M, lo, hi)
+        p = FB.dist_plan(rank, world, rs, Ml, fill)
+        halo = p["halo"]
+        owners = np.searchsorted(rs, halo, side="right") - 1
+        # needs: what this rank asks of each owner; the owners answer with their values
+        needs = [halo[owners == o].tolist() for o in range(world)]
+        asked = [None] * world
+        dist.all_gather_object(asked, needs)
+        replies = [x_own[np.array(asked[o][rank], dtype=np.int64) - lo].tolist() if asked[o][rank] else []
+                   for o in range(world)]
+        answers = [None] * world
+        dist.all_gather_object(answers, replies)
+        vals = np.zeros(len(halo))
+        for o in range(world):
+            if o != rank:
+                vals[owners == o] = answers[o][rank]
+        nb = p["nbelow"]
+        x_ext = np.concatenate([vals[:nb], x_own, vals[nb:]])
+        # the kept values in stored order
+        e0, e1 = int(M[0][lo]), int(M[0][hi])
+        keep = [(M[1][k] >= lo + i if fill == 1 else M[1][k] <= lo + i if fill == 2 else True)
+                for i in range(hi - lo) for k in range(int(M[0][lo + i]), int(M[0][lo + i + 1]))]
+        v = np.asarray(M[2][e0:e1])[np.array(keep, dtype=bool)]
+        y = _row_sums(p["rp"], p["cols"], v, x_ext)
+        part = 0.0
+        for yi in y:
+            part = part + yi * yi
+        parts = [None] * world
+        dist.all_gather_object(parts, part)
+        tot = parts[0]
+        for o in range(1, world):
+            tot = tot + parts[o]
+        out[name] = (lo, y, tot)
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, out))
+
+
+@pytest.mark.timeout(180)
+@pytest.mark.parametrize("world", [2, 3])
+def test_dist_halo_exchange_reproduces_global_products(world):
+    """Ranks exchanging halos by their plans compute every row of A x, G x and H x exactly as
+    the single-system product (bit for bit), and all ranks hold the same gathered sum."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_dist_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = dict(q.get(timeout=150) for _ in procs)
+    for p in procs:
+        p.join(timeout=30)
+        assert p.exitcode == 0
+    A, F = _system(6)
+    n = len(A[0]) - 1
+    x = FB.rand_normal(n, 11)
+    for name, M, fill in (("A", A, 0), ("G", (F["Gi"], F["Gj"], F["Gv"]), 1), ("H", (F["Hi"], F["Hj"], F["Hv"]), 2)):
+        ref = _row_sums(*_keep(M, fill), x)
+        got = np.zeros(n)
+        tots = set()
+        for r in range(world):
+            lo, y, tot = out[r][name]
+            got[lo:lo + len(y)] = y
+            tots.add(tot)
+        assert np.array_equal(got, ref), name
+        assert len(tots) == 1
