@@ -19,8 +19,11 @@ sources compiled against the project's MKL shim, OpenMP on all host cores) on th
 system with the reference's own pdfiim factors; each step is a bounded sample (a capped
 number of iterations), scaled to solves/s by the full solve's iteration count.
 
-Multi-GPU (torchrun): one full replica per rank (the 128^3 system is one unit; nothing
-is exchanged during a solve), value = total solves / max-over-ranks time.
+Multi-GPU (torchrun): by default one full replica per rank (nothing is exchanged during a
+solve), value = total solves / max-over-ranks time, weak scaling. --partition rows splits the
+one system into row blocks over the ranks instead (NCCL halo exchange and gathered partial
+sums each iteration), value = solves of the whole system / max-over-ranks time, strong
+scaling. At N = 1 the "partitioned" leg runs that path on one rank.
 """
 from __future__ import annotations
 
@@ -289,6 +292,63 @@ def run_e2e(args, A, F, b, n, ws, dist):
 
 
 
+def run_partitioned(args, A, F, b, rank, ws, dist, dev):
+    """The system split into ws contiguous row blocks, one per rank (fiim_dist_*: NCCL halo
+    exchange before each product, gathered partial sums for the scalars). Strong scaling:
+    one solve of the whole system per step, value = steps / max-over-ranks device time.
+    At ws = 1 it measures the partition machinery's own cost (NCCL at one rank, one-thread
+    scalar kernels, host-relaunched graph) against the single-GPU solve."""
+    import torch
+    import fiim_b200 as FB
+    rs = FB.dist_partition(A, F, ws)
+    uid = [FB.dist_unique_id() if rank == 0 else None]
+    if dist is not None:
+        dist.broadcast_object_list(uid, src=0)
+    lo, hi = int(rs[rank]), int(rs[rank + 1])
+    Al, Fl = FB.dist_local(A, F, rs, rank)
+    D = FB.DistSolver(rank, ws, uid[0], rs, Al, Fl, variant="pdfiim", memory="device", device=dev.index)
+    bl = torch.from_numpy(np.ascontiguousarray(b[lo:hi])).to(dev)
+    xl = torch.zeros(hi - lo, dtype=torch.float64, device=dev)
+    for _ in range(args.warmup):
+        xl.zero_()
+        D.solve(bl, xl, tol=1e-8, nmax=1200)
+    torch.cuda.synchronize()
+    barrier(dist)
+    rr = []
+    for _ in range(args.steps):
+        xl.zero_()
+        rr.append(D.solve(bl, xl, tol=1e-8, nmax=1200))
+    torch.cuda.synchronize()
+    dev_ms = max_over_ranks(dist, sum(q["device_ms"] for q in rr))
+    assert all(q["info"] == 0 for q in rr), rr[0]
+    # e2e: the same call with this rank's b and x in pinned host memory (copies inside).
+    hb = torch.from_numpy(np.ascontiguousarray(b[lo:hi])).pin_memory()
+    hx = torch.zeros(hi - lo, dtype=torch.float64).pin_memory()
+    D.close()
+    uid2 = [FB.dist_unique_id() if rank == 0 else None]
+    if dist is not None:
+        dist.broadcast_object_list(uid2, src=0)
+    Dh = FB.DistSolver(rank, ws, uid2[0], rs, Al, Fl, variant="pdfiim", memory="host", device=dev.index)
+    for _ in range(args.warmup):
+        hx.zero_()
+        Dh.solve(hb.numpy(), hx.numpy(), tol=1e-8, nmax=1200)
+    barrier(dist)
+    e_times = []
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        hx.zero_()
+        Dh.solve(hb.numpy(), hx.numpy(), tol=1e-8, nmax=1200)
+        e_times.append(time.perf_counter() - t1)
+    e_tot = max_over_ranks(dist, sum(e_times))
+    Dh.close()
+    return {"value": args.steps / (dev_ms / 1000.0), "unit": "solves/s", "ms_per_solve": dev_ms / args.steps,
+            "ranks": ws, "row_starts": [int(v) for v in rs], "iterations": rr[-1]["iter"],
+            "true_relres": rr[-1]["true_relres"], "launches_per_solve_per_rank": rr[-1]["launches"],
+            "e2e": {"value": args.steps / e_tot, "unit": "solves/s", "h2d_bytes_per_step": 16 * (hi - lo),
+                    "d2h_bytes_per_step": 8 * (hi - lo), "bytes": "of rank 0's rows",
+                    "timing": "host wall clock around the blocking call, max over ranks"}}
+
+
 def run_batched(args, rank=0, world=1, dist=None):
     """256 independent 2D convection-diffusion systems (side U{32..256}, diffusion log-U[0.1,10],
     random direction, cell Peclet <= 1), each with factors from the library's PDFIIM
@@ -532,6 +592,11 @@ def run_ours(args):
     if not args.no_mrhs:
         multi_rhs = run_multi_rhs(args, rank, ws, dist)
 
+    # ---- row-partitioned solve of the one system (headline with --partition rows)
+    part = None
+    if args.partition == "rows" or (ws == 1 and not args.no_dist):
+        part = run_partitioned(args, A, F, b, rank, ws, dist, dev)
+
     # ---- CPU baseline (rank 0, N = 1): bounded sample of the reference's solve
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -549,15 +614,23 @@ def run_ours(args):
                          f"scaled by the GPU solve's {its} iterations"}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": round(value, 4), "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": round(dev_ms_max / args.steps, 4), "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": config(args.size, nnz, {"iterations": iters[0], "parallelism": f"replicas x{ws}",
+        headline, scaling, par, ms_step = value, "weak", f"replicas x{ws}", dev_ms_max / args.steps
+        replicas = None
+        if args.partition == "rows":
+            replicas = {"value": round(value, 4), "unit": "solves/s", "e2e": e2e}
+            headline, scaling, par, ms_step = part["value"], "strong", f"rows x{ws}", part["ms_per_solve"]
+            e2e = part["e2e"]
+            launches = part["launches_per_solve_per_rank"] * args.steps
+        line = {"metric": METRIC, "value": round(headline, 4), "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True,
+                "scaling": scaling, "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": config(args.size, nnz, {"iterations": iters[0], "parallelism": par,
                                                   "setup_s": round(t_setup, 2)}),
                 "hbm_gbs": round(hbm_gbs, 1), "hbm_frac": round(hbm_gbs / peak, 4),
                 "iteration_bytes": it_bytes, "true_relres": results[-1]["true_relres"],
                 "resval": results[-1]["resval"], "wall_ms_per_step": round(1000 * wall / args.steps, 4),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed, "batched": batched, "multi_rhs": multi_rhs,
+                "partitioned": part, "replicas": replicas,
                 "gpu_launches": launches,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
@@ -580,6 +653,10 @@ def main():
     ap.add_argument("--batch", type=int, default=256, help="systems in the batched leg")
     ap.add_argument("--no-mrhs", action="store_true", help="skip the multi-RHS leg")
     ap.add_argument("--mrhs-n", type=int, default=4000000, help="rows of the multi-RHS system")
+    ap.add_argument("--partition", default="replicas", choices=["replicas", "rows"],
+                    help="N > 1: replicas of the system per rank (weak scaling, default) or one system in "
+                         "row blocks over the ranks (strong scaling)")
+    ap.add_argument("--no-dist", action="store_true", help="skip the row-partitioned leg at N = 1")
     ap.add_argument("--cpu-sample-its", type=int, default=12)
     ap.add_argument("--ref-sample-its", type=int, default=10)
     ap.add_argument("--ref-iters", type=int, default=99,
