@@ -254,7 +254,6 @@ def run_e2e(args, A, F, b, n, ws, dist):
     P = lambda t: C.c_void_p(t.data_ptr())
 
     def e2e_call(rhs):
-        hx.zero_()
         rc = L.fiim_EPBiCGSTAB_pdfiim(C.c_int(n), 0, P(hA[2]), P(hA[1]), P(hA[0]), P(rhs), C.c_double(1e-8), 1200,
                                       P(hG[2]), P(hG[1]), P(hG[0]), P(hD), P(hH[2]), P(hH[1]), P(hH[0]), P(hx),
                                       C.byref(resval), C.byref(it), 0, C.byref(info))
@@ -262,11 +261,13 @@ def run_e2e(args, A, F, b, n, ws, dist):
 
     def timed(rhs_list):
         for k in range(args.warmup):
+            hx.zero_()
             e2e_call(rhs_list[k % len(rhs_list)])
         barrier(dist)
         e_times = []
         for k in range(args.steps):
-            t1 = time.perf_counter()
+            hx.zero_()                      # the caller's initial guess, x0 = 0
+            t1 = time.perf_counter()        # timed: the C-ABI call alone
             e2e_call(rhs_list[k % len(rhs_list)])
             e_times.append(time.perf_counter() - t1)
         return max_over_ranks(dist, sum(e_times))
@@ -335,8 +336,8 @@ def run_partitioned(args, A, F, b, rank, ws, dist, dev):
     barrier(dist)
     e_times = []
     for _ in range(args.steps):
-        t1 = time.perf_counter()
         hx.zero_()
+        t1 = time.perf_counter()
         Dh.solve(hb.numpy(), hx.numpy(), tol=1e-8, nmax=1200)
         e_times.append(time.perf_counter() - t1)
     e_tot = max_over_ranks(dist, sum(e_times))

@@ -92,6 +92,10 @@ int heuristic_vec(long n, long nnz);
 void signature(DevCsr &M, const int *host_rp);
 size_t csr_bytes(long n, long nnz);
 int carve_csr(Arena &ar, DevCsr &M, long n, long nnz);
+int upload_csr_async(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, const double *v, bool device_src,
+                     cudaStream_t s);
+int check_fill_launch(DevCsr &M, int fill, cudaStream_t s, unsigned long long *d_count, unsigned long long *h_count);
+int check_fill_finish(DevCsr &M, int fill, unsigned long long outside);
 int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, const double *v, int fill,
                bool device_src, cudaStream_t s, unsigned long long *d_count, unsigned long long *h_count);
 int set_tile(DevCsr &M, int tile, cudaStream_t s);

@@ -581,6 +581,31 @@ k_spmv_vec(CsrView<double> M, const double *__restrict__ x, Epi epi, DState *st,
 #define FIIM_FOR_ROWS(i, n) \
     for (long i = (long)blockIdx.x * kThreads + threadIdx.x; i < (n); i += (long)gridDim.x * kThreads)
 
+// Grid-stride loop over [0, n), U elements per trip: the loads of all U elements (ld(i)
+// returns them as one value) are issued before any is used (op(i, loaded)), so a thread has
+// U times as many loads in flight. A thread still visits its elements in ascending order, so
+// its partial sums are those of the plain loop, bit for bit.
+template <int U, class Ld, class Op>
+__device__ __forceinline__ void stream_rows(long n, const Ld &ld, const Op &op) {
+    const long S = (long)gridDim.x * kThreads;
+    long i = (long)blockIdx.x * kThreads + threadIdx.x;
+    for (; i + (U - 1) * S < n; i += U * S) {
+        decltype(ld(0L)) q[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) q[u] = ld(i + u * S);
+#pragma unroll
+        for (int u = 0; u < U; ++u) op(i + u * S, q[u]);
+    }
+    for (; i < n; i += S) op(i, ld(i));
+}
+
+struct Ld3 {
+    double a, b, c;
+};
+struct Ld6 {
+    double a, b, c, d, e, f;
+};
+
 struct FinS {
     __device__ void finish(DState *st, const double *t) const {
         st->r2 = t[0];
@@ -601,12 +626,13 @@ k_update_s(long n, const double *__restrict__ r, const double *__restrict__ v,
     if (st->done) return;
     const double na = -st->alpha;
     double red[2] = {0.0, 0.0};
-    FIIM_FOR_ROWS(i, n) {
-        const double ri = r[i], xi = x[i];
-        s[i] = __dadd_rn(ri, __dmul_rn(na, v[i]));
-        red[0] += ri * ri;
-        red[1] += xi * xi;
-    }
+    stream_rows<1>(   // unrolling measured slower here (12.2 against 10.7 us at 128^3)
+        n, [&](long i) { return Ld3{r[i], v[i], x[i]}; },
+        [&](long i, const Ld3 &q) {
+            s[i] = __dadd_rn(q.a, __dmul_rn(na, q.b));
+            red[0] += q.a * q.a;
+            red[1] += q.c * q.c;
+        });
     pdl_release();
     grid_reduce<2>(red, partials, st, fin);
 }
@@ -644,15 +670,17 @@ k_update_xr(long n, const double *__restrict__ pc, const double *__restrict__ sc
     if (st->done) return;
     const double a = st->alpha, om = st->omega, nom = -st->omega;
     double red[1] = {0.0};
-    FIIM_FOR_ROWS(i, n) {
-        double xi = x[i];
-        xi = __dadd_rn(xi, __dmul_rn(a, pc[i]));
-        xi = __dadd_rn(xi, __dmul_rn(om, sc[i]));
-        x[i] = xi;
-        const double ri = __dadd_rn(s[i], __dmul_rn(nom, t[i]));
-        r[i] = ri;
-        red[0] += r0[i] * ri;
-    }
+    stream_rows<4>(   // 26.0 against 27.6 us at 128^3
+        n, [&](long i) { return Ld6{x[i], pc[i], sc[i], s[i], t[i], r0[i]}; },
+        [&](long i, const Ld6 &q) {
+            double xi = q.a;
+            xi = __dadd_rn(xi, __dmul_rn(a, q.b));
+            xi = __dadd_rn(xi, __dmul_rn(om, q.c));
+            x[i] = xi;
+            const double ri = __dadd_rn(q.d, __dmul_rn(nom, q.e));
+            r[i] = ri;
+            red[0] += q.f * ri;
+        });
     pdl_release();
     grid_reduce<1>(red, partials, st, fin);
 }
@@ -676,10 +704,9 @@ k_update_p(long n, const double *__restrict__ r, const double *__restrict__ v,
     }
     if (st->done) return;
     const double b = st->beta, c = __dmul_rn(-st->beta, st->omega);
-    FIIM_FOR_ROWS(i, n) {
-        const double pi = __dadd_rn(__dmul_rn(c, v[i]), __dmul_rn(b, p[i]));
-        p[i] = __dadd_rn(pi, r[i]);
-    }
+    stream_rows<4>(
+        n, [&](long i) { return Ld3{v[i], p[i], r[i]}; },
+        [&](long i, const Ld3 &q) { p[i] = __dadd_rn(__dadd_rn(__dmul_rn(c, q.a), __dmul_rn(b, q.b)), q.c); });
 }
 
 // Count entries of a CSR matrix outside the kept triangle (upper: col < row is outside;

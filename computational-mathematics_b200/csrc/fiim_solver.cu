@@ -383,48 +383,73 @@ void signature(DevCsr &M, const int *host_rp) {
     M.sig.push_back(host_rp[M.n]);
 }
 
-// Upload one CSR matrix into pre-carved buffers (capacity nnz_cap) and apply MKL's
-// TRIANGULAR fill semantics: fill 1 keeps col >= row, fill 2 keeps col <= row
-// (AFIIM/src/bicgstab.cpp:140-147). The check runs on the device; the rare matrix
-// with entries outside its triangle is compacted on the host.
-int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, const double *v,
-                      int fill, bool device_src, cudaStream_t s, unsigned long long *d_count,
-                      unsigned long long *h_count) {
+// Upload one CSR matrix into pre-carved buffers (capacity nnz_cap), in two halves:
+// upload_csr_async issues the copies (the column and value arrays first; a host-side row
+// offset array is compared with the previous upload's while they run, and copied only if it
+// differs), and check_fill_launch / check_fill_finish apply MKL's TRIANGULAR fill semantics:
+// fill 1 keeps col >= row, fill 2 keeps col <= row (AFIIM/src/bicgstab.cpp:140-147). The check
+// runs on the device; the rare matrix with entries outside its triangle is compacted on the
+// host. A caller uploading several matrices issues every copy and check before one sync.
+int upload_csr_async(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, const double *v, bool device_src,
+                     cudaStream_t s) {
     std::vector<int> &hrp = M.hrp;
     const bool had = (M.n == n && (long)hrp.size() == (long)n + 1);
     M.n = n;
+    const cudaMemcpyKind kind = device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     if (device_src) {
         std::vector<int> nrp(n + 1);
         FIIM_CUDA(cudaMemcpyAsync(nrp.data(), rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
         FIIM_CUDA(cudaStreamSynchronize(s));
         M.rows_same = had && nrp == hrp;
         hrp.swap(nrp);
+        const long nnz = hrp[n];
+        if (nnz > nnz_cap) return set_error(FIIM_EARG, "matrix has %ld entries, capacity %ld", nnz, nnz_cap);
+        if (nnz < 0) return set_error(FIIM_EARG, "negative row offset at n");
+        M.nnz = nnz;
+        FIIM_CUDA(cudaMemcpyAsync(M.rp, rp, sizeof(int) * (n + 1), kind, s));
+        if (nnz > 0) {
+            FIIM_CUDA(cudaMemcpyAsync(M.ci, ci, sizeof(int) * nnz, kind, s));
+            FIIM_CUDA(cudaMemcpyAsync(M.v, v, sizeof(double) * nnz, kind, s));
+        }
     } else {
+        const long nnz = rp[n];
+        if (nnz > nnz_cap) return set_error(FIIM_EARG, "matrix has %ld entries, capacity %ld", nnz, nnz_cap);
+        if (nnz < 0) return set_error(FIIM_EARG, "negative row offset at n");
+        M.nnz = nnz;
+        if (nnz > 0) {
+            FIIM_CUDA(cudaMemcpyAsync(M.ci, ci, sizeof(int) * nnz, kind, s));
+            FIIM_CUDA(cudaMemcpyAsync(M.v, v, sizeof(double) * nnz, kind, s));
+        }
+        // The device keeps the previous upload's offsets (hrp mirrors them): copy only on change.
         M.rows_same = had && std::memcmp(hrp.data(), rp, sizeof(int) * (n + 1)) == 0;
         if (!M.rows_same) {
             hrp.resize(n + 1);
             std::memcpy(hrp.data(), rp, sizeof(int) * (n + 1));
+            FIIM_CUDA(cudaMemcpyAsync(M.rp, rp, sizeof(int) * (n + 1), kind, s));
         }
     }
-    const long nnz = hrp[n];
-    if (nnz > nnz_cap) return set_error(FIIM_EARG, "matrix has %ld entries, capacity %ld", nnz, nnz_cap);
-    if (nnz < 0) return set_error(FIIM_EARG, "negative row offset at n");
-    M.nnz = nnz;
-    const cudaMemcpyKind kind = device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    FIIM_CUDA(cudaMemcpyAsync(M.rp, rp, sizeof(int) * (n + 1), kind, s));
-    if (nnz > 0) {
-        FIIM_CUDA(cudaMemcpyAsync(M.ci, ci, sizeof(int) * nnz, kind, s));
-        FIIM_CUDA(cudaMemcpyAsync(M.v, v, sizeof(double) * nnz, kind, s));
-    }
     signature(M, hrp.data());
-    if (fill == 0 || nnz == 0) return FIIM_OK;
+    return FIIM_OK;
+}
+
+int check_fill_launch(DevCsr &M, int fill, cudaStream_t s, unsigned long long *d_count, unsigned long long *h_count) {
+    *h_count = 0;
+    if (fill == 0 || M.nnz == 0) return FIIM_OK;
     FIIM_CUDA(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), s));
+    const int n = (int)M.n;
     const int g = std::min(num_sms() * 8, std::max(1, (n + kThreads - 1) / kThreads));
     k_count_outside<<<g, kThreads, 0, s>>>(n, M.rp, M.ci, fill == 1, d_count);
     FIIM_CUDA(cudaGetLastError());
     FIIM_CUDA(cudaMemcpyAsync(h_count, d_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    FIIM_CUDA(cudaStreamSynchronize(s));
-    if (*h_count == 0) return FIIM_OK;
+    return FIIM_OK;
+}
+
+// After the stream has synchronized: compact M to its triangle if the check found entries
+// outside it.
+int check_fill_finish(DevCsr &M, int fill, unsigned long long outside) {
+    if (fill == 0 || outside == 0) return FIIM_OK;
+    const int n = (int)M.n;
+    const long nnz = M.nnz;
     std::vector<int> crp(n + 1), cci(nnz);
     std::vector<double> cv(nnz);
     FIIM_CUDA(cudaMemcpy(crp.data(), M.rp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
@@ -449,9 +474,29 @@ int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, con
         FIIM_CUDA(cudaMemcpy(M.ci, cci.data(), sizeof(int) * c, cudaMemcpyHostToDevice));
         FIIM_CUDA(cudaMemcpy(M.v, cv.data(), sizeof(double) * c, cudaMemcpyHostToDevice));
     }
-    hrp.swap(nrp);
+    M.hrp.swap(nrp);
     M.rows_same = false;   // the stored offsets are the filtered ones
-    signature(M, hrp.data());
+    signature(M, M.hrp.data());
+    return FIIM_OK;
+}
+
+int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, const double *v, int fill,
+               bool device_src, cudaStream_t s, unsigned long long *d_count, unsigned long long *h_count) {
+    FIIM_TRY(upload_csr_async(M, nnz_cap, n, rp, ci, v, device_src, s));
+    if (fill == 0 || M.nnz == 0) return FIIM_OK;
+    FIIM_TRY(check_fill_launch(M, fill, s, d_count, h_count));
+    FIIM_CUDA(cudaStreamSynchronize(s));
+    return check_fill_finish(M, fill, *h_count);
+}
+
+// Uploads of the solver's matrices: every copy and triangle check issued, then one sync.
+static int upload_all(DevCsr *const *mats, const long *caps, const int *const *rps, const int *const *cis,
+                      const double *const *vs, const int *fills, const bool *dev, int count, int n, cudaStream_t s,
+                      unsigned long long *d_count, unsigned long long *h_count) {
+    for (int k = 0; k < count; ++k) FIIM_TRY(upload_csr_async(*mats[k], caps[k], n, rps[k], cis[k], vs[k], dev[k], s));
+    for (int k = 0; k < count; ++k) FIIM_TRY(check_fill_launch(*mats[k], fills[k], s, d_count + k, h_count + k));
+    FIIM_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < count; ++k) FIIM_TRY(check_fill_finish(*mats[k], fills[k], h_count[k]));
     return FIIM_OK;
 }
 
@@ -699,25 +744,26 @@ int Solver::create(int n_, const int *Ai, const int *Aj, const double *Av, const
     }
     st = static_cast<DState *>(arena.take(sizeof(DState)));
     partials = static_cast<double *>(arena.take(sizeof(double) * 4 * max_blocks));
-    d_count = static_cast<unsigned long long *>(arena.take(sizeof(unsigned long long)));
+    d_count = static_cast<unsigned long long *>(arena.take(sizeof(unsigned long long) * 5));
     fault = static_cast<int *>(arena.take(sizeof(int)));
     if (!st || !partials || !d_count || !fault) return set_error(FIIM_ENOMEM, "arena exhausted");
-    if (!hst) FIIM_CUDA(cudaHostAlloc(&hst, sizeof(DState) + 64, cudaHostAllocDefault));
-    h_count = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(hst) + sizeof(DState) + 32);
-    h_fault = reinterpret_cast<int *>(reinterpret_cast<char *>(hst) + sizeof(DState) + 48);
+    if (!hst) FIIM_CUDA(cudaHostAlloc(&hst, sizeof(DState) + 128, cudaHostAllocDefault));
+    h_count = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(hst) + sizeof(DState) + 32);  // 5
+    h_fault = reinterpret_cast<int *>(reinterpret_cast<char *>(hst) + sizeof(DState) + 80);
     FIIM_CUDA(cudaMemsetAsync(st, 0, sizeof(DState), stream));
     FIIM_CUDA(cudaMemsetAsync(fault, 0, sizeof(int), stream));
 
-    FIIM_TRY(upload_csr(A, capA, n, aRp, aCi, aV, 0, a_dev, stream, d_count, h_count));
-    FIIM_TRY(upload_csr(G, capG, n, Gi, Gj, Gv, 1, dev_src, stream, d_count, h_count));
-    FIIM_TRY(upload_csr(H, capH, n, hRp, hCi, hV, 2, h_dev, stream, d_count, h_count));
-    if (combined) {
-        FIIM_TRY(upload_csr(L, capL, n, Li, Lj, Lv, 2, dev_src, stream, d_count, h_count));
-        FIIM_TRY(upload_csr(U, capU, n, Ui, Uj, Uv, 1, dev_src, stream, d_count, h_count));
-    }
     FIIM_CUDA(cudaMemcpyAsync(IDv, IDv_, sizeof(double) * n,
                               dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
-    FIIM_CUDA(cudaStreamSynchronize(stream));
+    {
+        DevCsr *mats[] = {&A, &G, &H, &L, &U};
+        const long caps[] = {capA, capG, capH, capL, capU};
+        const int *rps[] = {aRp, Gi, hRp, Li, Ui}, *cis[] = {aCi, Gj, hCi, Lj, Uj};
+        const double *vs[] = {aV, Gv, hV, Lv, Uv};
+        const int fills[] = {0, 1, 2, 2, 1};
+        const bool dev[] = {a_dev, dev_src, h_dev, dev_src, dev_src};
+        FIIM_TRY(upload_all(mats, caps, rps, cis, vs, fills, dev, combined ? 5 : 3, n, stream, d_count, h_count));
+    }
 
     DevCsr *mats[] = {&A, &G, &H, &L, &U};
     for (int k = 0; k < (combined ? 5 : 3); ++k) {
@@ -750,15 +796,17 @@ int Solver::reload(const int *Ai, const int *Aj, const double *Av, const int *Gi
     const bool dev_src = (opt.memory == FIIM_MEM_DEVICE);
     const bool combined = (opt.variant == FIIM_ACIFIM && opt.mode == 'C' && opt.nr > 1);
     if (opt.issym) return set_error(FIIM_EARG, "reload does not serve symmetric input");
-    FIIM_TRY(upload_csr(A, capA, n, Ai, Aj, Av, 0, dev_src, stream, d_count, h_count));
-    FIIM_TRY(upload_csr(G, capG, n, Gi, Gj, Gv, 1, dev_src, stream, d_count, h_count));
-    FIIM_TRY(upload_csr(H, capH, n, Hi, Hj, Hv, 2, dev_src, stream, d_count, h_count));
-    if (combined) {
-        FIIM_TRY(upload_csr(L, capL, n, Li, Lj, Lv, 2, dev_src, stream, d_count, h_count));
-        FIIM_TRY(upload_csr(U, capU, n, Ui, Uj, Uv, 1, dev_src, stream, d_count, h_count));
-    }
     FIIM_CUDA(cudaMemcpyAsync(IDv, IDv_, sizeof(double) * n,
                               dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
+    {
+        DevCsr *mats[] = {&A, &G, &H, &L, &U};
+        const long caps[] = {capA, capG, capH, capL, capU};
+        const int *rps[] = {Ai, Gi, Hi, Li, Ui}, *cis[] = {Aj, Gj, Hj, Lj, Uj};
+        const double *vs[] = {Av, Gv, Hv, Lv, Uv};
+        const int fills[] = {0, 1, 2, 2, 1};
+        const bool dev[] = {dev_src, dev_src, dev_src, dev_src, dev_src};
+        FIIM_TRY(upload_all(mats, caps, rps, cis, vs, fills, dev, combined ? 5 : 3, n, stream, d_count, h_count));
+    }
     // Row blocks follow the new row offsets (rebuilt only where they changed); the graph
     // bakes in each block count.
     bool regraph = false;
