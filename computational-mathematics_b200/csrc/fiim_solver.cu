@@ -822,15 +822,17 @@ int Solver::reload(const int *Ai, const int *Aj, const double *Av, const int *Gi
 }
 
 // ------------------------------------------------------------------ solve
-int Solver::solve(const double *b_in, double *x_io, double tol, int nmax, fiim_result *res) {
+// solve_start enqueues the whole solve (input copies, start kernel, iteration graph, true
+// residual) and returns while it runs (with the device-driven loop; the host-driven loop
+// waits for it). solve_finish copies the scalars and x back and waits.
+int Solver::solve_start(const double *b_in, const double *x_in, double tol, int nmax) {
     FIIM_CUDA(cudaSetDevice(device));
     const bool dev_src = (opt.memory == FIIM_MEM_DEVICE);
     const cudaMemcpyKind in_kind = dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    const cudaMemcpyKind out_kind = dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     FIIM_CUDA(cudaEventRecord(ev0, stream));
     FIIM_CUDA(cudaMemsetAsync(fault, 0, sizeof(int), stream));
     FIIM_CUDA(cudaMemcpyAsync(b, b_in, sizeof(double) * n, in_kind, stream));
-    FIIM_CUDA(cudaMemcpyAsync(x, x_io, sizeof(double) * n, in_kind, stream));
+    FIIM_CUDA(cudaMemcpyAsync(x, x_in, sizeof(double) * n, in_kind, stream));
 
     DState h = {};
     h.tol = tol;
@@ -844,7 +846,8 @@ int Solver::solve(const double *b_in, double *x_io, double tol, int nmax, fiim_r
     FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
     // Start: r = b - A x, r0 = r, p = r, ro = ||r0|| (AFIIM/src/bicgstab.cpp:151-165).
     FIIM_CUDA(launch_spmv(A, stream, x, EpiInit{b, p, r0, r}, st, partials, fault));
-    int launches = 1;
+    pending_launches = 1;
+    host_loops = 0;
     if (use_cond) {
         FIIM_CUDA(cudaGraphLaunch(exec, stream));
     } else {
@@ -861,23 +864,28 @@ int Solver::solve(const double *b_in, double *x_io, double tol, int nmax, fiim_r
                 return set_error(FIIM_ETIMEOUT, "solve not finished after %d iterations", launched);
             chunk = std::min(chunk * 2, 16);
         }
-        hst->loops = launched;
+        host_loops = launched;
     }
     // FP64 true residual ||b - A x|| / ||b||.
     FIIM_CUDA(launch_spmv(A, stream, x, EpiResid{b, nullptr}, st, partials, fault));
-    launches += 1;
-    const int fallback_loops = hst->loops;
+    pending_launches += 1;
+    return FIIM_OK;
+}
+
+int Solver::solve_finish(double *x_io, fiim_result *res) {
+    const bool dev_src = (opt.memory == FIIM_MEM_DEVICE);
+    const cudaMemcpyKind out_kind = dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     FIIM_CUDA(cudaMemcpyAsync(hst, st, sizeof(DState), cudaMemcpyDeviceToHost, stream));
     FIIM_CUDA(cudaMemcpyAsync(h_fault, fault, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    FIIM_CUDA(cudaMemcpyAsync(x_io, x, sizeof(double) * n, out_kind, stream));
+    if (x_io) FIIM_CUDA(cudaMemcpyAsync(x_io, x, sizeof(double) * n, out_kind, stream));
     FIIM_CUDA(cudaEventRecord(ev1, stream));
     FIIM_CUDA(cudaStreamSynchronize(stream));
-    if (!use_cond) hst->loops = fallback_loops;
+    if (!use_cond) hst->loops = host_loops;
     float ms = 0.f;
     FIIM_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
     if (hst->info == -5) return set_error(FIIM_ETIMEOUT, "device loop guard tripped");
     if (*h_fault) return set_error(FIIM_ETIMEOUT, "a staged SpMV's bulk copy did not complete in time");
-    launches += hst->loops * kernels_per_iteration();
+    const int launches = pending_launches + hst->loops * kernels_per_iteration();
     last_launches = launches;
     if (res) {
         res->resval = hst->rc / hst->ro;
@@ -888,8 +896,13 @@ int Solver::solve(const double *b_in, double *x_io, double tol, int nmax, fiim_r
         res->device_ms = ms;
         res->launches = launches;
     }
-    if (opt.verbose) print_status(hst->info, hst->iter, hst->rc / hst->ro);
+    if (opt.verbose && x_io) print_status(hst->info, hst->iter, hst->rc / hst->ro);
     return FIIM_OK;
+}
+
+int Solver::solve(const double *b_in, double *x_io, double tol, int nmax, fiim_result *res) {
+    FIIM_TRY(solve_start(b_in, x_io, tol, nmax));
+    return solve_finish(x_io, res);
 }
 
 // The reference's termination messages (AFIIM/src/bicgstab.cpp:227-252,279-280;

@@ -49,6 +49,11 @@ struct Solver : SolverBase {
                const int *Li, const int *Lj, const double *Lv, const int *Ui, const int *Uj,
                const double *Uv);
     int solve(const double *b, double *x, double tol, int nmax, fiim_result *res);
+    // The two halves of solve: enqueue (returns while the device-driven loop runs), then copy
+    // the scalars and x (x_io == NULL: discard the result) and wait.
+    int solve_start(const double *b, const double *x, double tol, int nmax);
+    int solve_finish(double *x_io, fiim_result *res);
+    int pending_launches = 0, host_loops = 0;
     void destroy();
     size_t device_bytes() const { return arena.cap; }
 
