@@ -292,6 +292,13 @@ int fiim_solver_kernel_times(fiim_solver_t h, int reps, int max_kernels, double 
     return reinterpret_cast<fiim::Solver *>(h)->kernel_times(reps, max_kernels, ms, bytes, names, name_len);
 }
 
+int fiim_solver_kernel_times_seq(fiim_solver_t h, int reps, int max_kernels, double *ms, double *bytes,
+                                 char *names, int name_len, double *body_ms) {
+    if (!h || fiim_is_mixed(h) || !ms || !bytes || reps < 1) return fiim::set_error(FIIM_EARG, "bad argument");
+    return reinterpret_cast<fiim::Solver *>(h)->kernel_times(reps, max_kernels, ms, bytes, names, name_len, true,
+                                                             body_ms);
+}
+
 double fiim_solver_iteration_bytes(fiim_solver_t h) {
     if (!h || fiim_is_mixed(h)) return -1.0;
     return reinterpret_cast<fiim::Solver *>(h)->iteration_bytes();

@@ -964,7 +964,8 @@ int Solver::apply(int op, const double *in, double *out) {
 // scalars are reset so no kernel takes its early exit. Reports the mean device ms of
 // each launch and its algorithmic bytes: a matrix pass S(M) = nnz*(8+4) + 4*(n+1),
 // one read of the gathered vector, and every other vector read or written once.
-int Solver::kernel_times(int reps, int max_k, double *ms, double *bytes, char *names, int name_len) {
+int Solver::kernel_times(int reps, int max_k, double *ms, double *bytes, char *names, int name_len,
+                         bool in_sequence, double *body_ms) {
     FIIM_CUDA(cudaSetDevice(device));
     const bool combined = (opt.variant == FIIM_ACIFIM && opt.mode == 'C' && opt.nr > 1);
     if (combined) return set_error(FIIM_EARG, "kernel timing covers mode 'E' bodies");
@@ -982,6 +983,9 @@ int Solver::kernel_times(int reps, int max_k, double *ms, double *bytes, char *n
         {"update_xr", 8 * nv, [&] { k_update_xr<FinControl><<<stream_grid(k_update_xr<FinControl>, nn), kThreads, 0, stream>>>(nn, pc, sc, sv, t, r0, x, r, st, partials, FinControl{}); return cudaGetLastError(); }},
         {"update_p", 4 * nv, [&] { k_update_p<<<stream_grid(k_update_p, nn), kThreads, 0, stream>>>(nn, r, v, p, st, cudaGraphConditionalHandle{}, 0); return cudaGetLastError(); }},
     };
+    if (in_sequence)   // the body's second H product (K5), between the s update and G's product
+        items.insert(items.begin() + 4, Item{"H_spmv_scale", S(H) + 3 * nv, [&] {
+            return launch_spmv(H, stream, sv, EpiScale{tm, IDv}, st, partials, fault); }});
     // Scalars that keep every kernel on its full path; the solver's vectors are
     // scratch here (each solve starts from the caller's x and b).
     DState h = {};
@@ -990,6 +994,42 @@ int Solver::kernel_times(int reps, int max_k, double *ms, double *bytes, char *n
     *hst = h;
     FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
     const int k = std::min<int>((int)items.size(), max_k);
+    if (in_sequence) {
+        // The body in order, an event between consecutive launches; then the same body
+        // without the events in between, for the events' own cost.
+        std::vector<cudaEvent_t> ev(k + 1);
+        for (auto &e : ev) FIIM_CUDA(cudaEventCreate(&e));
+        std::vector<double> acc(k, 0.0);
+        for (int i = 0; i < k; ++i) FIIM_CUDA(items[i].go());   // warm
+        for (int rr = 0; rr < reps; ++rr) {
+            for (int i = 0; i < k; ++i) {
+                FIIM_CUDA(cudaEventRecord(ev[i], stream));
+                FIIM_CUDA(items[i].go());
+            }
+            FIIM_CUDA(cudaEventRecord(ev[k], stream));
+            FIIM_CUDA(cudaEventSynchronize(ev[k]));
+            for (int i = 0; i < k; ++i) {
+                float t_ms = 0.f;
+                FIIM_CUDA(cudaEventElapsedTime(&t_ms, ev[i], ev[i + 1]));
+                acc[i] += t_ms;
+            }
+        }
+        FIIM_CUDA(cudaEventRecord(ev[0], stream));
+        for (int rr = 0; rr < reps; ++rr)
+            for (int i = 0; i < k; ++i) FIIM_CUDA(items[i].go());
+        FIIM_CUDA(cudaEventRecord(ev[k], stream));
+        FIIM_CUDA(cudaEventSynchronize(ev[k]));
+        float whole = 0.f;
+        FIIM_CUDA(cudaEventElapsedTime(&whole, ev[0], ev[k]));
+        if (body_ms) *body_ms = whole / reps;
+        for (auto &e : ev) cudaEventDestroy(e);
+        for (int i = 0; i < k; ++i) {
+            ms[i] = acc[i] / reps;
+            bytes[i] = items[i].bytes;
+            if (names) std::snprintf(names + (size_t)i * name_len, name_len, "%s", items[i].name);
+        }
+        return k;
+    }
     for (int i = 0; i < k; ++i) {
         FIIM_CUDA(items[i].go());   // warm
         FIIM_CUDA(cudaEventRecord(ev0, stream));

@@ -63,7 +63,8 @@ struct Solver : SolverBase {
     int kernels_per_iteration() const;
     void print_status(int info, int iter, double rel) const;
     int apply(int op, const double *in, double *out);
-    int kernel_times(int reps, int max_k, double *ms, double *bytes, char *names, int name_len);
+    int kernel_times(int reps, int max_k, double *ms, double *bytes, char *names, int name_len,
+                     bool in_sequence = false, double *body_ms = nullptr);
     double iteration_bytes() const;
 };
 

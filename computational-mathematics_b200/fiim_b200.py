@@ -37,7 +37,7 @@ _PRECISIONS = {"fp64": FP64, "fp32": MIXED_FP32, "bf16": MIXED_BF16}
 EXPORTS = (
     "fiim_last_error", "fiim_dropin_cache", "fiim_options_default", "fiim_EPBiCGSTAB_afiim", "fiim_EPBiCGSTAB_pdfiim",
     "fiim_PBiCGSTAB_acifim", "fiim_solver_create", "fiim_solver_solve", "fiim_solver_device_bytes",
-    "fiim_solver_spmv_shape", "fiim_solver_apply", "fiim_solver_kernel_times", "fiim_solver_iteration_bytes",
+    "fiim_solver_spmv_shape", "fiim_solver_apply", "fiim_solver_kernel_times", "fiim_solver_kernel_times_seq", "fiim_solver_iteration_bytes",
     "fiim_solver_destroy", "fiim_batch_create", "fiim_batch_solve", "fiim_batch_destroy",
     "fiim_block_create", "fiim_block_solve", "fiim_block_destroy",
     "fiim_spmv", "fiim_prec_apply", "fiim_prec_apply_noalloc",
@@ -230,16 +230,24 @@ class Solver:
         _check(lib().fiim_solver_apply(self._h, C.c_int(0 if op == "A" else 1), _ptr(x), _ptr(y)))
         return y
 
-    def kernel_times(self, reps=20, max_kernels=16):
-        """Mean device ms and algorithmic bytes of each launch of the iteration body."""
+    def kernel_times(self, reps=20, max_kernels=16, in_sequence=False):
+        """Mean device ms and algorithmic bytes of each launch of the iteration body, each
+        replayed alone; with in_sequence, the body in order with an event between launches,
+        returned with the mean ms of the same body without those events."""
         ms, by = np.zeros(max_kernels), np.zeros(max_kernels)
         names = C.create_string_buffer(max_kernels * 32)
-        k = lib().fiim_solver_kernel_times(self._h, C.c_int(reps), C.c_int(max_kernels), _ptr(ms), _ptr(by),
-                                           names, C.c_int(32))
+        body = C.c_double(0.0)
+        if in_sequence:
+            k = lib().fiim_solver_kernel_times_seq(self._h, C.c_int(reps), C.c_int(max_kernels), _ptr(ms), _ptr(by),
+                                                   names, C.c_int(32), C.byref(body))
+        else:
+            k = lib().fiim_solver_kernel_times(self._h, C.c_int(reps), C.c_int(max_kernels), _ptr(ms), _ptr(by),
+                                               names, C.c_int(32))
         if k < 0:
             _check(k)
         raw = names.raw
-        return [(raw[i * 32:(i + 1) * 32].split(b"\0")[0].decode(), float(ms[i]), float(by[i])) for i in range(k)]
+        out = [(raw[i * 32:(i + 1) * 32].split(b"\0")[0].decode(), float(ms[i]), float(by[i])) for i in range(k)]
+        return (out, body.value) if in_sequence else out
 
     def iteration_bytes(self) -> float:
         return float(lib().fiim_solver_iteration_bytes(self._h))

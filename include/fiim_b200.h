@@ -157,6 +157,13 @@ int fiim_solver_apply(fiim_solver_t s, int op, const double *x, double *y);
 int fiim_solver_kernel_times(fiim_solver_t s, int reps, int max_kernels, double *ms, double *bytes,
                              char *names, int name_len);
 
+/* The same launches in the iteration body's order (both H products included), with a CUDA
+ * event between consecutive launches: each launch's time as it follows the previous one.
+ * *body_ms (if not NULL) receives the mean time of the same body without the events in
+ * between, so their own cost is known. Returns the number of launches (<= max). */
+int fiim_solver_kernel_times_seq(fiim_solver_t s, int reps, int max_kernels, double *ms, double *bytes,
+                                 char *names, int name_len, double *body_ms);
+
 /* Algorithmic bytes of one FP64 iteration: 2 S(A) + 2 S(G) + 2 S(H) + 32 * 8n, where
  * S(M) = 12 nnz(M) + 4 (n + 1). */
 double fiim_solver_iteration_bytes(fiim_solver_t s);
