@@ -293,6 +293,36 @@ def run_e2e(args, A, F, b, n, ws, dist):
 
 
 
+def run_small(args, dev):
+    """The small plain case (2D 5-point Poisson on a 128 x 128 grid, n = 16,384, b = A 1,
+    x0 = 0, AFIIM factors with drop tolerance 0.1, FP64, rtol 1e-8, NMAX 1000). The factors
+    are the ones the reference built for the committed fixture tests/golden/poisson128_afiim.npz
+    (data only). The working set fits in L2: the solve is bound by launch and reduction latency,
+    not HBM bandwidth."""
+    import torch
+    import fiim_b200 as FB
+    z = np.load(os.path.join(ROOT, "tests", "golden", "poisson128_afiim.npz"))
+    A = tuple(torch.from_numpy(z[k]).to(dev) for k in ("Ai", "Aj", "Av"))
+    F = {k: torch.from_numpy(z[k]).to(dev) for k in ("Gi", "Gj", "Gv", "IDv", "Hi", "Hj", "Hv")}
+    b = torch.from_numpy(z["b"]).to(dev)
+    x = torch.zeros_like(b)
+    S = FB.Solver(A, F, variant="afiim", memory="device")
+    for _ in range(max(args.warmup, 3)):
+        x.zero_()
+        S.solve(b, x, tol=1e-8, nmax=1000)
+    rr = []
+    for _ in range(max(args.steps, 20)):
+        x.zero_()
+        rr.append(S.solve(b, x, tol=1e-8, nmax=1000))
+    S.close()
+    ms = sum(q["device_ms"] for q in rr) / len(rr)
+    return {"workload": "poisson2d_128 (n=16,384) AFIIM eps 0.1 (reference-built factors) FP64 BiCGSTAB",
+            "solves_per_s": round(1000.0 / ms, 2), "ms_per_solve": round(ms, 4), "iterations": rr[-1]["iter"],
+            "us_per_iteration": round(1000.0 * ms / max(rr[-1]["iter"], 1), 2), "info": rr[-1]["info"],
+            "reference_iterations": int(z["iter"]), "reference_iteration_envelope": [int(v) for v in z["iter_env"]],
+            "bound": "latency (working set in L2)"}
+
+
 def run_partitioned(args, A, F, b, rank, ws, dist, dev):
     """The system split into ws contiguous row blocks, one per rank (fiim_dist_*: NCCL halo
     exchange before each product, gathered partial sums for the scalars). Strong scaling:
@@ -603,6 +633,11 @@ def run_ours(args):
     if not args.no_mrhs:
         multi_rhs = run_multi_rhs(args, rank, ws, dist)
 
+    # ---- the small plain case (config 0), latency-bound
+    small = None
+    if rank == 0 and ws == 1 and not args.no_small:
+        small = run_small(args, dev)
+
     # ---- row-partitioned solve of the one system (headline with --partition rows)
     part = None
     if args.partition == "rows" or (ws == 1 and not args.no_dist):
@@ -641,7 +676,7 @@ def run_ours(args):
                 "iteration_bytes": it_bytes, "true_relres": results[-1]["true_relres"],
                 "resval": results[-1]["resval"], "wall_ms_per_step": round(1000 * wall / args.steps, 4),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "mixed": mixed, "batched": batched, "multi_rhs": multi_rhs,
-                "partitioned": part, "replicas": replicas,
+                "partitioned": part, "replicas": replicas, "small_system": small,
                 "gpu_launches": launches,
                 "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
@@ -668,6 +703,7 @@ def main():
                     help="N > 1: replicas of the system per rank (weak scaling, default) or one system in "
                          "row blocks over the ranks (strong scaling)")
     ap.add_argument("--no-dist", action="store_true", help="skip the row-partitioned leg at N = 1")
+    ap.add_argument("--no-small", action="store_true", help="skip the small plain case (Poisson 128^2)")
     ap.add_argument("--cpu-sample-its", type=int, default=12)
     ap.add_argument("--ref-sample-its", type=int, default=10)
     ap.add_argument("--ref-iters", type=int, default=99,
