@@ -306,21 +306,35 @@ def run_small(args, dev):
     F = {k: torch.from_numpy(z[k]).to(dev) for k in ("Gi", "Gj", "Gv", "IDv", "Hi", "Hj", "Hv")}
     b = torch.from_numpy(z["b"]).to(dev)
     x = torch.zeros_like(b)
-    S = FB.Solver(A, F, variant="afiim", memory="device")
-    for _ in range(max(args.warmup, 3)):
-        x.zero_()
-        S.solve(b, x, tol=1e-8, nmax=1000)
-    rr = []
-    for _ in range(max(args.steps, 20)):
-        x.zero_()
-        rr.append(S.solve(b, x, tol=1e-8, nmax=1000))
-    S.close()
-    ms = sum(q["device_ms"] for q in rr) / len(rr)
-    return {"workload": "poisson2d_128 (n=16,384) AFIIM eps 0.1 (reference-built factors) FP64 BiCGSTAB",
-            "solves_per_s": round(1000.0 / ms, 2), "ms_per_solve": round(ms, 4), "iterations": rr[-1]["iter"],
-            "us_per_iteration": round(1000.0 * ms / max(rr[-1]["iter"], 1), 2), "info": rr[-1]["info"],
-            "reference_iterations": int(z["iter"]), "reference_iteration_envelope": [int(v) for v in z["iter_env"]],
-            "bound": "latency (working set in L2)"}
+    def timed(persist):
+        prev = os.environ.get("FIIM_PERSIST")
+        os.environ["FIIM_PERSIST"] = persist
+        try:
+            S = FB.Solver(A, F, variant="afiim", memory="device")
+        finally:
+            if prev is None:
+                del os.environ["FIIM_PERSIST"]
+            else:
+                os.environ["FIIM_PERSIST"] = prev
+        mode = S.mode()
+        for _ in range(max(args.warmup, 3)):
+            x.zero_()
+            S.solve(b, x, tol=1e-8, nmax=1000)
+        rr = []
+        for _ in range(max(args.steps, 20)):
+            x.zero_()
+            rr.append(S.solve(b, x, tol=1e-8, nmax=1000))
+        S.close()
+        ms = sum(q["device_ms"] for q in rr) / len(rr)
+        return {"solves_per_s": round(1000.0 / ms, 2), "ms_per_solve": round(ms, 4), "iterations": rr[-1]["iter"],
+                "us_per_iteration": round(1000.0 * ms / max(rr[-1]["iter"], 1), 2), "info": rr[-1]["info"],
+                "mode": {0: "WHILE graph", 1: "host-relaunched graph", 2: "one cooperative launch"}[mode]}
+    out = {"workload": "poisson2d_128 (n=16,384) AFIIM eps 0.1 (reference-built factors) FP64 BiCGSTAB",
+           "reference_iterations": int(z["iter"]), "reference_iteration_envelope": [int(v) for v in z["iter_env"]],
+           "bound": "latency (working set in L2)"}
+    out.update(timed("0"))
+    out["one_cooperative_launch"] = timed("1")
+    return out
 
 
 def run_partitioned(args, A, F, b, rank, ws, dist, dev):

@@ -292,6 +292,27 @@ int fiim_solver_kernel_times(fiim_solver_t h, int reps, int max_kernels, double 
     return reinterpret_cast<fiim::Solver *>(h)->kernel_times(reps, max_kernels, ms, bytes, names, name_len);
 }
 
+int fiim_solver_mode(fiim_solver_t h) {
+    if (!h) return fiim::set_error(FIIM_EARG, "bad handle");
+    if (fiim_is_mixed(h)) return 1;
+    auto *s = reinterpret_cast<fiim::Solver *>(h);
+    return s->persistent ? 2 : (s->use_cond ? 0 : 1);
+}
+
+int fiim_solver_set_wait_limit(fiim_solver_t h, int polls) {
+    if (!h || fiim_is_mixed(h) || polls < 1) return fiim::set_error(FIIM_EARG, "bad argument");
+    reinterpret_cast<fiim::Solver *>(h)->wait_limit = polls;
+    return FIIM_OK;
+}
+
+int fiim_solver_test_stall(fiim_solver_t h) {
+    if (!h || fiim_is_mixed(h)) return fiim::set_error(FIIM_EARG, "bad handle");
+    auto *s = reinterpret_cast<fiim::Solver *>(h);
+    if (!s->persistent) return fiim::set_error(FIIM_EARG, "the solver does not run as one cooperative launch");
+    s->stall_next = true;
+    return FIIM_OK;
+}
+
 int fiim_solver_kernel_times_seq(fiim_solver_t h, int reps, int max_kernels, double *ms, double *bytes,
                                  char *names, int name_len, double *body_ms) {
     if (!h || fiim_is_mixed(h) || !ms || !bytes || reps < 1) return fiim::set_error(FIIM_EARG, "bad argument");

@@ -31,6 +31,7 @@
 #include "fiim_internal.h"
 #include "fiim_kernels.cuh"
 #include "fiim_pipe.cuh"
+#include "fiim_persist.cuh"
 #include "fiim_solver.h"
 
 namespace fiim {
@@ -257,6 +258,9 @@ int set_tile(DevCsr &M, int tile, cudaStream_t s) {
 // (next block's stream and epilogue operands in registers), 2048 entries per block was the
 // fastest size for the 7-, 6- and 11-entry rows of the 3D convection-diffusion A, G and H.
 static int default_tile(const DevCsr &) { return 2048; }
+
+// Largest system the one-launch solve takes (its per-phase work stays a few microseconds).
+constexpr int kPersistMaxN = 65536;
 
 // Time each row-block size on this matrix and keep the fastest; cached by signature.
 // The choice changes speed only: every shape sums each row in storage order.
@@ -727,7 +731,7 @@ int Solver::create(int n_, const int *Ai, const int *Aj, const double *Av, const
     if (combined) bytes += csr_bytes(n, nL) + csr_bytes(n, nU);
     bytes += (size_t)(nvec + 1) * Arena::need(sizeof(double) * n);
     const int max_blocks = num_sms() * 32;
-    bytes += Arena::need(sizeof(DState)) + Arena::need(sizeof(double) * 4 * max_blocks) + 1024;
+    bytes += Arena::need(sizeof(DState)) + Arena::need(sizeof(double) * 4 * max_blocks) + Arena::need(16) + 1024;
     FIIM_TRY(arena.reserve(bytes));
     FIIM_TRY(carve_csr(arena, A, n, nA));
     FIIM_TRY(carve_csr(arena, G, n, nG));
@@ -746,7 +750,8 @@ int Solver::create(int n_, const int *Ai, const int *Aj, const double *Av, const
     partials = static_cast<double *>(arena.take(sizeof(double) * 4 * max_blocks));
     d_count = static_cast<unsigned long long *>(arena.take(sizeof(unsigned long long) * 5));
     fault = static_cast<int *>(arena.take(sizeof(int)));
-    if (!st || !partials || !d_count || !fault) return set_error(FIIM_ENOMEM, "arena exhausted");
+    pbar = static_cast<unsigned *>(arena.take(16));
+    if (!st || !partials || !d_count || !fault || !pbar) return set_error(FIIM_ENOMEM, "arena exhausted");
     if (!hst) FIIM_CUDA(cudaHostAlloc(&hst, sizeof(DState) + 128, cudaHostAllocDefault));
     h_count = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(hst) + sizeof(DState) + 32);  // 5
     h_fault = reinterpret_cast<int *>(reinterpret_cast<char *>(hst) + sizeof(DState) + 80);
@@ -776,6 +781,23 @@ int Solver::create(int n_, const int *Ai, const int *Aj, const double *Av, const
             // the same bits, in every process on the same GPU model.
             M.form = kFormRows;
             FIIM_TRY(set_tile(M, default_tile(M), stream));
+        }
+    }
+    {
+        // FIIM_PERSIST=1: systems of at most kPersistMaxN rows solve as one cooperative launch.
+        // Measured slower than the WHILE graph on B200 (Poisson 128^2: 41.7 against 34.7 us
+        // per iteration), so it is not the default.
+        const char *pe = std::getenv("FIIM_PERSIST");
+        const bool want = pe && pe[0] == '1' && n <= kPersistMaxN;
+        persistent = false;
+        if (want && !combined) {
+            int occ = 0, coop = 0;
+            FIIM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+            FIIM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_solve_persistent, kThreads, 0));
+            const int most = std::max(A.nblk, std::max(G.nblk, H.nblk));
+            const int max_blocks_p = num_sms() * 32;   // the partials buffer holds 2 x 4 per CTA
+            persist_grid = std::min({occ * num_sms(), std::max(most, 1), max_blocks_p / 2});
+            persistent = coop && occ > 0 && persist_grid > 0;
         }
     }
     FIIM_TRY(build_graph());
@@ -844,10 +866,14 @@ int Solver::solve_start(const double *b_in, const double *x_in, double tol, int 
     h.alpha_guard = (opt.variant == FIIM_ACIFIM);
     *hst = h;
     FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
+    host_loops = 0;
+    if (persistent) {
+        pending_launches = 1;
+        return launch_persistent();
+    }
     // Start: r = b - A x, r0 = r, p = r, ro = ||r0|| (AFIIM/src/bicgstab.cpp:151-165).
     FIIM_CUDA(launch_spmv(A, stream, x, EpiInit{b, p, r0, r}, st, partials, fault));
     pending_launches = 1;
-    host_loops = 0;
     if (use_cond) {
         FIIM_CUDA(cudaGraphLaunch(exec, stream));
     } else {
@@ -872,6 +898,28 @@ int Solver::solve_start(const double *b_in, const double *x_in, double tol, int 
     return FIIM_OK;
 }
 
+static PView pview(const DevCsr &M) {
+    return PView{M.rp, M.ci, M.v, M.rb, M.eb, M.nblk, M.cd, M.cb, M.narrow};
+}
+
+int Solver::launch_persistent() {
+    FIIM_CUDA(cudaMemsetAsync(pbar, 0, 16, stream));
+    if (stall_next) {
+        // Test hook: an arrival count that never reaches the grid size, so every CTA's first
+        // barrier wait runs out and the solve returns FIIM_ETIMEOUT.
+        const unsigned stuck[2] = {0x80000000u, 0u};
+        FIIM_CUDA(cudaMemcpyAsync(pbar, stuck, sizeof(stuck), cudaMemcpyHostToDevice, stream));
+        FIIM_CUDA(cudaStreamSynchronize(stream));
+        stall_next = false;
+    }
+    PersistArgs a{pview(A), pview(G), pview(H), n, x, b, r, r0, p, v, sv, t, pc, sc, tm, IDv, st, partials, pbar,
+                  fault, wait_limit};
+    void *args[] = {&a};
+    FIIM_CUDA(cudaLaunchCooperativeKernel((const void *)k_solve_persistent, dim3(persist_grid), dim3(kThreads), args, 0,
+                                          stream));
+    return FIIM_OK;
+}
+
 int Solver::solve_finish(double *x_io, fiim_result *res) {
     const bool dev_src = (opt.memory == FIIM_MEM_DEVICE);
     const cudaMemcpyKind out_kind = dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
@@ -884,7 +932,9 @@ int Solver::solve_finish(double *x_io, fiim_result *res) {
     float ms = 0.f;
     FIIM_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
     if (hst->info == -5) return set_error(FIIM_ETIMEOUT, "device loop guard tripped");
-    if (*h_fault) return set_error(FIIM_ETIMEOUT, "a staged SpMV's bulk copy did not complete in time");
+    if (*h_fault)
+        return set_error(FIIM_ETIMEOUT, persistent ? "the solve's grid barrier did not complete within its limit"
+                                                   : "a staged SpMV's bulk copy did not complete in time");
     const int launches = pending_launches + hst->loops * kernels_per_iteration();
     last_launches = launches;
     if (res) {

@@ -54,6 +54,13 @@ struct Solver : SolverBase {
     int solve_start(const double *b, const double *x, double tol, int nmax);
     int solve_finish(double *x_io, fiim_result *res);
     int pending_launches = 0, host_loops = 0;
+    // Small systems: the whole solve as one cooperative launch (fiim_persist.cuh).
+    bool persistent = false;
+    int persist_grid = 0;
+    unsigned *pbar = nullptr;    // grid barrier words
+    int wait_limit = 1 << 21;    // barrier polls (each a sleep of ~64 ns and a read) before a solve gives up
+    bool stall_next = false;     // test hook: the next solve's first barrier never completes
+    int launch_persistent();
     void destroy();
     size_t device_bytes() const { return arena.cap; }
 

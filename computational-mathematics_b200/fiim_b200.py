@@ -37,7 +37,8 @@ _PRECISIONS = {"fp64": FP64, "fp32": MIXED_FP32, "bf16": MIXED_BF16}
 EXPORTS = (
     "fiim_last_error", "fiim_dropin_cache", "fiim_options_default", "fiim_EPBiCGSTAB_afiim", "fiim_EPBiCGSTAB_pdfiim",
     "fiim_PBiCGSTAB_acifim", "fiim_solver_create", "fiim_solver_solve", "fiim_solver_device_bytes",
-    "fiim_solver_spmv_shape", "fiim_solver_apply", "fiim_solver_kernel_times", "fiim_solver_kernel_times_seq", "fiim_solver_iteration_bytes",
+    "fiim_solver_spmv_shape", "fiim_solver_apply", "fiim_solver_kernel_times", "fiim_solver_kernel_times_seq", "fiim_solver_mode",
+    "fiim_solver_set_wait_limit", "fiim_solver_test_stall", "fiim_solver_iteration_bytes",
     "fiim_solver_destroy", "fiim_batch_create", "fiim_batch_solve", "fiim_batch_destroy",
     "fiim_block_create", "fiim_block_solve", "fiim_block_destroy",
     "fiim_spmv", "fiim_prec_apply", "fiim_prec_apply_noalloc",
@@ -221,6 +222,21 @@ class Solver:
         t, f = C.c_int(0), C.c_int(0)
         _check(lib().fiim_solver_spmv_shape(self._h, C.c_int(which), C.byref(t), C.byref(f)))
         return t.value, f.value
+
+    def mode(self) -> int:
+        """0 device-driven WHILE graph, 1 host-relaunched graph, 2 one cooperative launch."""
+        rc = lib().fiim_solver_mode(self._h)
+        if rc < 0:
+            _check(rc)
+        return rc
+
+    def set_wait_limit(self, polls: int):
+        """Bound (in ~64 ns polls) on each grid-barrier wait of a one-launch solve."""
+        _check(lib().fiim_solver_set_wait_limit(self._h, C.c_int(polls)))
+
+    def test_stall(self):
+        """Make the next one-launch solve's first barrier unreachable (it must time out)."""
+        _check(lib().fiim_solver_test_stall(self._h))
 
     def apply(self, x, y, op="A"):
         """y = A x (op 'A') or y = M x (op 'M', the preconditioner) with the solver's kernels."""

@@ -164,6 +164,22 @@ int fiim_solver_kernel_times(fiim_solver_t s, int reps, int max_kernels, double 
 int fiim_solver_kernel_times_seq(fiim_solver_t s, int reps, int max_kernels, double *ms, double *bytes,
                                  char *names, int name_len, double *body_ms);
 
+/* How an FP64 solver runs its iteration loop: 0 a CUDA graph whose WHILE node repeats the
+ * body on the device (the default), 1 a one-iteration graph relaunched by the host
+ * (FIIM_GRAPH=host; also what a mixed-precision solver reports), 2 the whole solve as one
+ * cooperative launch with grid barriers between its phases (FIIM_PERSIST=1, systems of at
+ * most 65,536 rows). */
+int fiim_solver_mode(fiim_solver_t s);
+
+/* Bound on each grid-barrier wait of a one-launch solve, in polls (each a ~64 ns sleep and a
+ * read; default 2^21, one to two seconds). A wait that runs out ends the solve with
+ * FIIM_ETIMEOUT; the context stays usable. */
+int fiim_solver_set_wait_limit(fiim_solver_t s, int polls);
+
+/* Test hook for the bound above: the next solve of a one-launch solver starts with a barrier
+ * that can never complete, so it must end with FIIM_ETIMEOUT after the wait limit. */
+int fiim_solver_test_stall(fiim_solver_t s);
+
 /* Algorithmic bytes of one FP64 iteration: 2 S(A) + 2 S(G) + 2 S(H) + 32 * 8n, where
  * S(M) = 12 nnz(M) + 4 (n + 1). */
 double fiim_solver_iteration_bytes(fiim_solver_t s);

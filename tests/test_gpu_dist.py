@@ -40,7 +40,8 @@ def emulate(A, F, b, world, variant="pdfiim", tol=1e-8, nmax=1000, row_starts=No
     return x, r
 
 
-def test_world1_is_the_single_gpu_solve():
+def test_world1_is_the_single_gpu_solve(monkeypatch):
+    monkeypatch.setenv("FIIM_PERSIST", "0")   # the launched-kernel path the emulation shares
     A, F, b = system(16)
     x1, r1 = single(A, F, b)
     xe, re = emulate(A, F, b, 1)
