@@ -13,9 +13,9 @@
 //   * kept entries are sorted by index through their ranks.
 // Two passes over the rows: the first counts the kept entries of every row, the host turns
 // the counts into offsets, the second writes the entries and D^{-1}. A row whose pattern
-// outgrows the warp's shared memory (CAP members in a solve, 4 CAP in the set) is listed and
-// built again with a larger CAP; past the largest CAP the call returns FIIM_EARG and the host
-// construction serves.
+// outgrows the warp's shared memory (CAP members in a solve, 4 CAP in the set; 2048 at the
+// largest CAP) is listed and built again with a larger CAP; past the largest CAP the call
+// returns FIIM_EARG and the host construction serves.
 
 #include <cuda_runtime.h>
 
@@ -53,7 +53,9 @@ struct Out {
 
 template <int CAP>
 struct WarpSmem {
-    static constexpr int SET = 4 * CAP;
+    // Set capacity: 4 CAP, and 2048 at the largest CAP, where a warpsize cap keeps the solve
+    // small while wide rows (random columns, hundreds of entries) still grow the set.
+    static constexpr int SET = CAP >= 128 ? 2048 : 4 * CAP;
     int list[SET];
     int inds[CAP];
     int piv[CAP];

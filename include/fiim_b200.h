@@ -299,7 +299,7 @@ int fiim_pdfiim_build(int n, const int *Ai, const int *Aj, const double *Av, int
 /* The same construction on the GPU, with the same arguments, two-call protocol and
  * result, bit for bit: one warp per row, the row's pattern and its dense LU in the warp's
  * shared memory, two passes (counts, then entries at their offsets). A row whose pattern
- * outgrows 128 members in a solve (or 512 in its set) returns FIIM_EARG; the host
+ * outgrows 128 members in a solve (or 2048 in its set) returns FIIM_EARG; the host
  * construction has no such limit. Returns FIIM_ENODEV without an sm_100 device. */
 int fiim_pdfiim_build_gpu(int n, const int *Ai, const int *Aj, const double *Av, int prefill,
                           int lfill, int postfill, double ftol, int warpsize, char filttype,

@@ -78,6 +78,10 @@ def test_two_rank_sharding_and_max_over_ranks():
 
 # ----------------------------------------------------------------------------- row-partitioned solve
 def _system(N=6):
+    if N == "zipf":   # random columns: every rank's halo reaches every other rank
+        n = 600
+        A = FB.gen_zipf(n, FB.zipf_scale(n, mean=6.0, sample=n, seed=3), seed=3)
+        return A, FB.pdfiim_build(A, 0.1, 1, 1, 1, 16, "I", "B")
     A = FB.gen_convdiff3d(N, 0.5)
     F = FB.pdfiim_build(A, 0.05, 2, 2, 1)
     return A, F
@@ -152,13 +156,13 @@ def test_dist_plan_renumbers_monotonically(world):
                 assert p["nabove"] == 0
 
 
-def _dist_rank(rank, world, port, q):
+def _dist_rank(rank, world, port, q, which=6):
     """One rank: plan A, G, H; exchange the needs and the halo values over gloo as the
     solve does over NCCL; multiply; gather a partial dot product in rank order."""
     import torch
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
-    A, F = _system(6)
+    A, F = _system(which)
     n = len(A[0]) - 1
     rs = FB.dist_partition(A, F, world)
     lo, hi = int(rs[rank]), int(rs[rank + 1])
@@ -205,21 +209,23 @@ def _dist_rank(rank, world, port, q):
 
 
 @pytest.mark.timeout(180)
-@pytest.mark.parametrize("world", [2, 3])
-def test_dist_halo_exchange_reproduces_global_products(world):
+@pytest.mark.parametrize("world,which", [(2, 6), (3, 6), (3, "zipf")])
+def test_dist_halo_exchange_reproduces_global_products(world, which):
     """Ranks exchanging halos by their plans compute every row of A x, G x and H x exactly as
-    the single-system product (bit for bit), and all ranks hold the same gathered sum."""
+    the single-system product (bit for bit), and all ranks hold the same gathered sum; on a
+    stencil (neighbouring ranks) and on random columns (every rank exchanges with every
+    other)."""
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_dist_rank, args=(r, world, port, q)) for r in range(world)]
+    procs = [ctx.Process(target=_dist_rank, args=(r, world, port, q, which)) for r in range(world)]
     for p in procs:
         p.start()
     out = dict(q.get(timeout=150) for _ in procs)
     for p in procs:
         p.join(timeout=30)
         assert p.exitcode == 0
-    A, F = _system(6)
+    A, F = _system(which)
     n = len(A[0]) - 1
     x = FB.rand_normal(n, 11)
     for name, M, fill in (("A", A, 0), ("G", (F["Gi"], F["Gj"], F["Gv"]), 1), ("H", (F["Hi"], F["Hj"], F["Hv"]), 2)):

@@ -90,6 +90,20 @@ def test_uneven_blocks_and_single_rows():
         assert np.linalg.norm(xw - x1) / np.linalg.norm(x1) < 1e-6
 
 
+def test_random_columns_all_ranks_exchange():
+    """A Zipf matrix with random columns: every block's halo reaches every other block."""
+    n = 20000
+    A = FB.gen_zipf(n, FB.zipf_scale(n, sample=n, seed=21), seed=21)
+    F = FB.pdfiim_build(A, 0.1, 1, 1, 1, 32, "I", "B", gpu=True)
+    b = FB.rand_normal(n, 4)
+    x1, r1 = single(A, F, b, variant="afiim")
+    for world in (3, 5):
+        xw, rw = emulate(A, F, b, world, variant="afiim")
+        print(f"zipf world {world}: iter {rw['iter']} (1 GPU {r1['iter']}), info {rw['info']}")
+        assert rw["info"] == r1["info"] == 0 and abs(rw["iter"] - r1["iter"]) <= 2
+        assert np.linalg.norm(xw - x1) / np.linalg.norm(x1) < 1e-6
+
+
 def test_sherman2_within_the_reference_envelope():
     """sherman2 with the reference's own PDFIIM factors (golden): each partition's iteration
     count lies within +-2 of the oracle's rounding envelope and ends with the oracle's info."""
