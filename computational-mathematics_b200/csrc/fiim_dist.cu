@@ -699,7 +699,8 @@ extern "C" int fiim_dist_create(fiim_dist_t *out, int rank, int world, const uns
         D.d_scratch = nullptr;
         return set_error(FIIM_ENOMEM, "device allocation failed");
     }
-    auto fail = [](int rc) { return rc; };   // the handle's destructor releases everything
+    // From here on every early return releases the communicator and buffers through the
+    // handle's destructor.
     // Local checks and parts; every rank learns every status before the plan exchange.
     int rc = check_starts(world, row_starts);
     if (rc == FIIM_OK) rc = check_options(R.opt);
@@ -718,7 +719,7 @@ extern "C" int fiim_dist_create(fiim_dist_t *out, int rank, int world, const uns
         for (int l = 0; l < NL && rc == FIIM_OK; ++l) rc = make_part(rank, world, row_starts, rps[l], cis[l], vs[l], fills[l], P[l], R.L[l]);
     }
     const int agreed = D.agree(rc);
-    if (agreed != FIIM_OK) return fail(agreed);
+    if (agreed != FIIM_OK) return agreed;
     // Plan exchange: every rank tells each owner which of its rows it needs, per matrix.
     for (int l = 0; l < NL; ++l) {
         Layout &Ll = R.L[l];
@@ -727,7 +728,7 @@ extern "C" int fiim_dist_create(fiim_dist_t *out, int rank, int world, const uns
         int *dc = nullptr;
         if (cudaMalloc(&dc, sizeof(int) * (world + (size_t)world * world)) != cudaSuccess) {
             cudaGetLastError();
-            return fail(set_error(FIIM_ENOMEM, "device allocation failed"));
+            return set_error(FIIM_ENOMEM, "device allocation failed");
         }
         std::unique_ptr<int, decltype(&cudaFree)> dc_guard(dc, &cudaFree);
         FIIM_CUDA(cudaMemcpyAsync(dc, cnt.data(), sizeof(int) * world, cudaMemcpyHostToDevice, R.stream));
@@ -744,7 +745,7 @@ extern "C" int fiim_dist_create(fiim_dist_t *out, int rank, int world, const uns
         int *dl = nullptr;
         if (cudaMalloc(&dl, sizeof(int) * (ssum + rsum + 1)) != cudaSuccess) {
             cudaGetLastError();
-            return fail(set_error(FIIM_ENOMEM, "device allocation failed"));
+            return set_error(FIIM_ENOMEM, "device allocation failed");
         }
         std::unique_ptr<int, decltype(&cudaFree)> dl_guard(dl, &cudaFree);
         int *dneed = dl + ssum;   // my needs, by owner, in halo order
@@ -780,12 +781,12 @@ extern "C" int fiim_dist_create(fiim_dist_t *out, int rank, int world, const uns
     }
     {
         const int a = D.agree(rc);
-        if (a != FIIM_OK) return fail(a);
+        if (a != FIIM_OK) return a;
     }
     rc = R.setup(P, IDv);
     {
         const int a = D.agree(rc);
-        if (a != FIIM_OK) return fail(a);
+        if (a != FIIM_OK) return a;
     }
     // One body with the state marked done resolves every launch shape; then the body is
     // captured as a graph with its NCCL operations (FIIM_DIST_GRAPH=0: direct launches).
