@@ -92,8 +92,26 @@ int heuristic_vec(long n, long nnz);
 void signature(DevCsr &M, const int *host_rp);
 size_t csr_bytes(long n, long nnz);
 int carve_csr(Arena &ar, DevCsr &M, long n, long nnz);
+// Host-to-device copies from pageable memory through a ring of pinned buffers: a chunk is
+// copied into a pinned buffer by all host threads while the previous chunks' DMA runs, which
+// moves pageable data several times faster than a copy from pageable memory (staged by the
+// driver one page run at a time). Pinned sources and small copies go straight to
+// cudaMemcpyAsync. As with that call, the source is read completely before copy() returns;
+// the DMA from the pinned buffers may still be in flight.
+struct Stager {
+    static constexpr int kBufs = 4;
+    static constexpr size_t kChunk = size_t(16) << 20;
+    static constexpr size_t kMinStaged = size_t(4) << 20;
+    void *buf[kBufs] = {};
+    cudaEvent_t ev[kBufs] = {};
+    bool pending[kBufs] = {};
+    int next = 0;
+    int copy(void *dst, const void *src, size_t bytes, cudaStream_t s);
+    void release();
+};
+
 int upload_csr_async(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, const double *v, bool device_src,
-                     cudaStream_t s);
+                     cudaStream_t s, Stager *stager = nullptr);
 int check_fill_launch(DevCsr &M, int fill, cudaStream_t s, unsigned long long *d_count, unsigned long long *h_count);
 int check_fill_finish(DevCsr &M, int fill, unsigned long long outside);
 int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, const double *v, int fill,

@@ -394,8 +394,62 @@ void signature(DevCsr &M, const int *host_rp) {
 // fill 1 keeps col >= row, fill 2 keeps col <= row (AFIIM/src/bicgstab.cpp:140-147). The check
 // runs on the device; the rare matrix with entries outside its triangle is compacted on the
 // host. A caller uploading several matrices issues every copy and check before one sync.
+int Stager::copy(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+    cudaPointerAttributes attr{};
+    const bool pageable = cudaPointerGetAttributes(&attr, src) == cudaSuccess && attr.type == cudaMemoryTypeUnregistered;
+    cudaGetLastError();
+    if (!pageable || bytes < kMinStaged) {
+        FIIM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+        return FIIM_OK;
+    }
+    if (!buf[0]) {
+        for (int k = 0; k < kBufs; ++k) {
+            if (cudaHostAlloc(&buf[k], kChunk, cudaHostAllocDefault) != cudaSuccess) {
+                cudaGetLastError();
+                release();
+                FIIM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));   // no pinned memory
+                return FIIM_OK;
+            }
+            FIIM_CUDA(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
+        }
+    }
+    const char *in = static_cast<const char *>(src);
+    char *out = static_cast<char *>(dst);
+    for (size_t off = 0; off < bytes; off += kChunk) {
+        const size_t len = std::min(kChunk, bytes - off);
+        const int k = next;
+        next = (next + 1) % kBufs;
+        if (pending[k]) FIIM_CUDA(cudaEventSynchronize(ev[k]));   // the buffer's previous DMA
+        char *pb = static_cast<char *>(buf[k]);
+        const long parts = (long)((len + (size_t(1) << 20) - 1) >> 20);
+#pragma omp parallel for schedule(static)
+        for (long q = 0; q < parts; ++q) {
+            const size_t a = (size_t)q << 20, e = std::min(len, a + (size_t(1) << 20));
+            std::memcpy(pb + a, in + off + a, e - a);
+        }
+        FIIM_CUDA(cudaMemcpyAsync(out + off, pb, len, cudaMemcpyHostToDevice, s));
+        FIIM_CUDA(cudaEventRecord(ev[k], s));
+        pending[k] = true;
+    }
+    return FIIM_OK;
+}
+
+void Stager::release() {
+    for (int k = 0; k < kBufs; ++k) {
+        if (ev[k]) {
+            cudaEventSynchronize(ev[k]);
+            cudaEventDestroy(ev[k]);
+        }
+        if (buf[k]) cudaFreeHost(buf[k]);
+        ev[k] = nullptr;
+        buf[k] = nullptr;
+        pending[k] = false;
+    }
+    next = 0;
+}
+
 int upload_csr_async(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, const double *v, bool device_src,
-                     cudaStream_t s) {
+                     cudaStream_t s, Stager *stager) {
     std::vector<int> &hrp = M.hrp;
     const bool had = (M.n == n && (long)hrp.size() == (long)n + 1);
     M.n = n;
@@ -420,16 +474,21 @@ int upload_csr_async(DevCsr &M, long nnz_cap, int n, const int *rp, const int *c
         if (nnz > nnz_cap) return set_error(FIIM_EARG, "matrix has %ld entries, capacity %ld", nnz, nnz_cap);
         if (nnz < 0) return set_error(FIIM_EARG, "negative row offset at n");
         M.nnz = nnz;
+        auto h2d = [&](void *dst, const void *src, size_t bytes) -> int {
+            if (stager) return stager->copy(dst, src, bytes, s);
+            FIIM_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, s));
+            return FIIM_OK;
+        };
         if (nnz > 0) {
-            FIIM_CUDA(cudaMemcpyAsync(M.ci, ci, sizeof(int) * nnz, kind, s));
-            FIIM_CUDA(cudaMemcpyAsync(M.v, v, sizeof(double) * nnz, kind, s));
+            FIIM_TRY(h2d(M.ci, ci, sizeof(int) * nnz));
+            FIIM_TRY(h2d(M.v, v, sizeof(double) * nnz));
         }
         // The device keeps the previous upload's offsets (hrp mirrors them): copy only on change.
         M.rows_same = had && std::memcmp(hrp.data(), rp, sizeof(int) * (n + 1)) == 0;
         if (!M.rows_same) {
             hrp.resize(n + 1);
             std::memcpy(hrp.data(), rp, sizeof(int) * (n + 1));
-            FIIM_CUDA(cudaMemcpyAsync(M.rp, rp, sizeof(int) * (n + 1), kind, s));
+            FIIM_TRY(h2d(M.rp, rp, sizeof(int) * (n + 1)));
         }
     }
     signature(M, hrp.data());
@@ -496,8 +555,9 @@ int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, con
 // Uploads of the solver's matrices: every copy and triangle check issued, then one sync.
 static int upload_all(DevCsr *const *mats, const long *caps, const int *const *rps, const int *const *cis,
                       const double *const *vs, const int *fills, const bool *dev, int count, int n, cudaStream_t s,
-                      unsigned long long *d_count, unsigned long long *h_count) {
-    for (int k = 0; k < count; ++k) FIIM_TRY(upload_csr_async(*mats[k], caps[k], n, rps[k], cis[k], vs[k], dev[k], s));
+                      unsigned long long *d_count, unsigned long long *h_count, Stager *stager) {
+    for (int k = 0; k < count; ++k)
+        FIIM_TRY(upload_csr_async(*mats[k], caps[k], n, rps[k], cis[k], vs[k], dev[k], s, stager));
     for (int k = 0; k < count; ++k) FIIM_TRY(check_fill_launch(*mats[k], fills[k], s, d_count + k, h_count + k));
     FIIM_CUDA(cudaStreamSynchronize(s));
     for (int k = 0; k < count; ++k) FIIM_TRY(check_fill_finish(*mats[k], fills[k], h_count[k]));
@@ -758,8 +818,8 @@ int Solver::create(int n_, const int *Ai, const int *Aj, const double *Av, const
     FIIM_CUDA(cudaMemsetAsync(st, 0, sizeof(DState), stream));
     FIIM_CUDA(cudaMemsetAsync(fault, 0, sizeof(int), stream));
 
-    FIIM_CUDA(cudaMemcpyAsync(IDv, IDv_, sizeof(double) * n,
-                              dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
+    if (dev_src) FIIM_CUDA(cudaMemcpyAsync(IDv, IDv_, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+    else FIIM_TRY(stager.copy(IDv, IDv_, sizeof(double) * n, stream));
     {
         DevCsr *mats[] = {&A, &G, &H, &L, &U};
         const long caps[] = {capA, capG, capH, capL, capU};
@@ -767,7 +827,8 @@ int Solver::create(int n_, const int *Ai, const int *Aj, const double *Av, const
         const double *vs[] = {aV, Gv, hV, Lv, Uv};
         const int fills[] = {0, 1, 2, 2, 1};
         const bool dev[] = {a_dev, dev_src, h_dev, dev_src, dev_src};
-        FIIM_TRY(upload_all(mats, caps, rps, cis, vs, fills, dev, combined ? 5 : 3, n, stream, d_count, h_count));
+        FIIM_TRY(upload_all(mats, caps, rps, cis, vs, fills, dev, combined ? 5 : 3, n, stream, d_count, h_count,
+                             &stager));
     }
 
     DevCsr *mats[] = {&A, &G, &H, &L, &U};
@@ -818,8 +879,8 @@ int Solver::reload(const int *Ai, const int *Aj, const double *Av, const int *Gi
     const bool dev_src = (opt.memory == FIIM_MEM_DEVICE);
     const bool combined = (opt.variant == FIIM_ACIFIM && opt.mode == 'C' && opt.nr > 1);
     if (opt.issym) return set_error(FIIM_EARG, "reload does not serve symmetric input");
-    FIIM_CUDA(cudaMemcpyAsync(IDv, IDv_, sizeof(double) * n,
-                              dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
+    if (dev_src) FIIM_CUDA(cudaMemcpyAsync(IDv, IDv_, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream));
+    else FIIM_TRY(stager.copy(IDv, IDv_, sizeof(double) * n, stream));
     {
         DevCsr *mats[] = {&A, &G, &H, &L, &U};
         const long caps[] = {capA, capG, capH, capL, capU};
@@ -827,7 +888,8 @@ int Solver::reload(const int *Ai, const int *Aj, const double *Av, const int *Gi
         const double *vs[] = {Av, Gv, Hv, Lv, Uv};
         const int fills[] = {0, 1, 2, 2, 1};
         const bool dev[] = {dev_src, dev_src, dev_src, dev_src, dev_src};
-        FIIM_TRY(upload_all(mats, caps, rps, cis, vs, fills, dev, combined ? 5 : 3, n, stream, d_count, h_count));
+        FIIM_TRY(upload_all(mats, caps, rps, cis, vs, fills, dev, combined ? 5 : 3, n, stream, d_count, h_count,
+                             &stager));
     }
     // Row blocks follow the new row offsets (rebuilt only where they changed); the graph
     // bakes in each block count.
@@ -853,8 +915,13 @@ int Solver::solve_start(const double *b_in, const double *x_in, double tol, int 
     const cudaMemcpyKind in_kind = dev_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     FIIM_CUDA(cudaEventRecord(ev0, stream));
     FIIM_CUDA(cudaMemsetAsync(fault, 0, sizeof(int), stream));
-    FIIM_CUDA(cudaMemcpyAsync(b, b_in, sizeof(double) * n, in_kind, stream));
-    FIIM_CUDA(cudaMemcpyAsync(x, x_in, sizeof(double) * n, in_kind, stream));
+    if (dev_src) {
+        FIIM_CUDA(cudaMemcpyAsync(b, b_in, sizeof(double) * n, in_kind, stream));
+        FIIM_CUDA(cudaMemcpyAsync(x, x_in, sizeof(double) * n, in_kind, stream));
+    } else {
+        FIIM_TRY(stager.copy(b, b_in, sizeof(double) * n, stream));
+        FIIM_TRY(stager.copy(x, x_in, sizeof(double) * n, stream));
+    }
 
     DState h = {};
     h.tol = tol;
@@ -985,6 +1052,7 @@ void Solver::destroy() {
     stream = nullptr;
     if (hst) cudaFreeHost(hst);
     hst = nullptr;
+    stager.release();
     arena.release();
 }
 

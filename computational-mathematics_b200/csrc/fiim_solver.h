@@ -54,6 +54,7 @@ struct Solver : SolverBase {
     int solve_start(const double *b, const double *x, double tol, int nmax);
     int solve_finish(double *x_io, fiim_result *res);
     int pending_launches = 0, host_loops = 0;
+    Stager stager;               // host-to-device copies from pageable memory
     // Small systems: the whole solve as one cooperative launch (fiim_persist.cuh).
     bool persistent = false;
     int persist_grid = 0;
