@@ -674,6 +674,7 @@ extern "C" int fiim_dist_create(fiim_dist_t *out, int rank, int world, const uns
                                 const int *Hi, const int *Hj, const double *Hv, const fiim_options *opt) {
     if (!out || !id || world < 1 || rank < 0 || rank >= world) return set_error(FIIM_EARG, "bad rank, world or id");
     *out = nullptr;
+    FIIM_TRY(check_device(nullptr));   // FIIM_ENODEV without a device
     const NcclApi *api = nccl_api();
     if (!api) return set_error(FIIM_ENODEV, "libnccl.so.2 could not be loaded (set FIIM_NCCL_LIB)");
     if (device >= 0) FIIM_CUDA(cudaSetDevice(device));

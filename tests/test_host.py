@@ -67,6 +67,20 @@ def test_no_gpu_fails_loudly():
         FB.EPBiCGSTAB(64, A[2], A[1], A[0], np.ones(64), 1e-8, 10, A[2], A[1], A[0], np.ones(64), A[2], A[1],
                       A[0], x)
     assert not x.any()
+    # the GPU factor construction and the row-partitioned solve
+    with pytest.raises(FB.FiimError) as e:
+        FB.pdfiim_build(A, 0.05, gpu=True)
+    assert e.value.rc == FB.FIIM_ENODEV
+    Fh = FB.pdfiim_build(A, 0.05)
+    with pytest.raises(FB.FiimError) as e:
+        FB.dist_emulate(A, Fh, np.ones(64), x, 2)
+    assert e.value.rc == FB.FIIM_ENODEV
+    rs = FB.dist_partition(A, Fh, 1)
+    Al, Fl = FB.dist_local(A, Fh, rs, 0)
+    with pytest.raises(FB.FiimError) as e:
+        FB.DistSolver(0, 1, bytes(128), rs, Al, Fl)
+    assert e.value.rc == FB.FIIM_ENODEV
+    assert not x.any()
 
 
 def test_bad_arguments_rejected_before_device():
