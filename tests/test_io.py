@@ -10,8 +10,9 @@ import fiim_b200 as FB
 import pyoracle as O
 from conftest import load_golden
 
-REF_SHERMAN2 = "/root/reference/AFIIM/example/sherman2.mtx"
-REF_SHERMAN2_RHS = "/root/reference/AFIIM/example/sherman2_rhs1.mtx"
+REFERENCE = os.environ.get("FIIM_REFERENCE", "/root/reference")   # the reference tree, where present
+REF_SHERMAN2 = os.path.join(REFERENCE, "AFIIM/example/sherman2.mtx")
+REF_SHERMAN2_RHS = os.path.join(REFERENCE, "AFIIM/example/sherman2_rhs1.mtx")
 
 
 def write_mtx(path, n, rows, cols, vals, symmetry="general"):
