@@ -777,8 +777,10 @@ extern "C" int fiim_dist_create(fiim_dist_t *out, int rank, int world, const uns
             needs[q].assign(got.begin() + off, got.begin() + off + scnt[q]);
             off += scnt[q];
         }
-        rc = set_sends(Ll, R.lo, R.hi, needs);
-        if (rc != FIIM_OK) break;
+        // A bad request is recorded, not acted on: every rank keeps issuing the same NCCL
+        // operations for every matrix, and the ranks agree on the status afterwards.
+        const int src = set_sends(Ll, R.lo, R.hi, needs);
+        if (rc == FIIM_OK) rc = src;
     }
     {
         const int a = D.agree(rc);
