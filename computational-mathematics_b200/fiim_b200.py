@@ -12,8 +12,12 @@ back as ``(resval, iter, info)`` with the reference's ``info`` codes (0 converge
 CPU fallback.
 
 ``Solver`` wraps the handle API (set up once, solve many times) for host (numpy) or
-device (torch CUDA tensor) arrays. Generators and the host PDFIIM construction are
-exposed for tests and benchmarks.
+device (torch CUDA tensor) arrays, in FP64 or mixed precision; ``BatchSolver`` and
+``BlockSolver`` wrap the batched uneven systems and the multi-RHS block solve;
+``DistSolver`` is one rank of a solve split into row blocks over several GPUs
+(``dist_emulate`` runs all blocks on one GPU). Generators, the PDFIIM construction (host or
+GPU), the Matrix Market readers and the factor file are exposed for tests, benchmarks and
+callers without the reference library.
 """
 from __future__ import annotations
 
