@@ -156,6 +156,29 @@ def test_dist_plan_renumbers_monotonically(world):
                 assert p["nabove"] == 0
 
 
+def test_dist_plan_edge_cases():
+    """Rows without entries, a single rank (no halo), and a block of one row."""
+    n = 10
+    rp = np.array([0, 2, 2, 2, 5, 5, 6, 8, 8, 9, 10], np.int32)       # rows 1, 2, 4, 7 empty
+    ci = np.array([0, 9, 1, 3, 8, 5, 0, 6, 8, 9], np.int32)
+    v = np.arange(10, dtype=float)
+    M = (rp, ci, v)
+    p = FB.dist_plan(0, 1, np.array([0, n]), FB.dist_rows(M, 0, n), 0)
+    assert p["nbelow"] == 0 and p["nabove"] == 0 and len(p["halo"]) == 0
+    assert np.array_equal(p["cols"], ci) and np.array_equal(p["rp"], rp)
+    rs = np.array([0, 3, 4, n])
+    for r in range(3):
+        lo, hi = int(rs[r]), int(rs[r + 1])
+        q = FB.dist_plan(r, 3, rs, FB.dist_rows(M, lo, hi), 0)
+        ext = np.concatenate([q["halo"][:q["nbelow"]], np.arange(lo, hi), q["halo"][q["nbelow"]:]])
+        assert np.array_equal(ext[q["cols"]], ci[rp[lo]:rp[hi]])
+        assert np.array_equal(q["rp"], rp[lo:hi + 1] - rp[lo])
+    with pytest.raises(FB.FiimError):
+        FB.dist_plan(0, 2, np.array([0, 5, 5]), FB.dist_rows(M, 0, 5), 0)   # a rank without rows
+    with pytest.raises(FB.FiimError):
+        FB.dist_plan(2, 2, np.array([0, 5, n]), FB.dist_rows(M, 0, 5), 0)   # rank out of range
+
+
 def _dist_rank(rank, world, port, q, which=6):
     """One rank: plan A, G, H; exchange the needs and the halo values over gloo as the
     solve does over NCCL; multiply; gather a partial dot product in rank order."""
