@@ -83,6 +83,54 @@ def test_no_gpu_fails_loudly():
     assert not x.any()
 
 
+C_PROGRAM = r'''
+#include <stdio.h>
+#include <stdlib.h>
+#include "fiim_b200.h"
+int main(void) {
+    fiim_options o;
+    fiim_options_default(&o);
+    if (o.variant != FIIM_AFIIM || o.precision != FIIM_FP64 || o.mode != 'E') return 1;
+    long nnz = fiim_gen_poisson2d(8, 8, NULL, NULL, NULL);
+    int *Ai = malloc(sizeof(int) * 65), *Aj = malloc(sizeof(int) * nnz);
+    double *Av = malloc(sizeof(double) * nnz);
+    fiim_gen_poisson2d(8, 8, Ai, Aj, Av);
+    int ng = 0, nh = 0;
+    if (fiim_pdfiim_build(64, Ai, Aj, Av, 2, 2, 1, 0.05, -1, 'I', 'B', &ng, &nh, NULL, NULL, NULL, NULL, NULL,
+                          NULL, NULL) != FIIM_OK) return 2;
+    int *Gi = malloc(sizeof(int) * 65), *Gj = malloc(sizeof(int) * ng), *Hi = malloc(sizeof(int) * 65),
+        *Hj = malloc(sizeof(int) * nh);
+    double *Gv = malloc(sizeof(double) * ng), *Hv = malloc(sizeof(double) * nh), *D = malloc(sizeof(double) * 64);
+    if (fiim_pdfiim_build(64, Ai, Aj, Av, 2, 2, 1, 0.05, -1, 'I', 'B', &ng, &nh, Gv, Gj, Gi, D, Hv, Hj, Hi) != FIIM_OK)
+        return 3;
+    if (Gi[64] != ng || Hi[64] != nh) return 4;
+    fiim_solver_t h;
+    int rc = fiim_solver_create(&h, 0, NULL, NULL, NULL, NULL, NULL, NULL, NULL, NULL, NULL, NULL, NULL, NULL,
+                                NULL, NULL, NULL, NULL, &o);
+    if (rc != FIIM_EARG || fiim_last_error()[0] == 0) return 5;
+    printf("%d %d %d\n", (int)nnz, ng, nh);
+    return 0;
+}
+'''
+
+
+def test_c_program_builds_and_calls_the_library(tmp_path):
+    """A C99 program includes include/fiim_b200.h, links libfiim_b200.so and calls host-side
+    entry points (options, a generator, the two-call PDFIIM construction, argument errors)."""
+    src = tmp_path / "t.c"
+    src.write_text(C_PROGRAM)
+    exe = tmp_path / "t"
+    pkg = os.path.dirname(FB.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-L", pkg,
+                    "-lfiim_b200", f"-Wl,-rpath,{pkg}", "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, out
+    nnz, ng, nh = (int(v) for v in out.stdout.split())
+    A = FB.gen_poisson2d(8)
+    F = FB.pdfiim_build(A, 0.05, 2, 2, 1)
+    assert nnz == len(A[1]) and ng == len(F["Gj"]) and nh == len(F["Hj"])
+
+
 def test_bad_arguments_rejected_before_device():
     lib = FB.lib()
     h = C.c_void_p(0)
