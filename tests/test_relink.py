@@ -16,6 +16,7 @@ test_gpu_solve.py (info, iterations within the reference's rounding envelope +-2
 """
 import os
 import re
+import shutil
 import subprocess
 
 import numpy as np
@@ -66,7 +67,16 @@ def write_system(g, d):
 
 def run(prog, g, d, args, timeout=300):
     a, r = write_system(g, d)
-    env = dict(os.environ, OMP_NUM_THREADS="1")
+    if not os.access(prog, os.X_OK):
+        # a copy of the repository that dropped the mode bits: run a private copy (the
+        # library is then found through LD_LIBRARY_PATH instead of the run path)
+        local = os.path.join(d, os.path.basename(prog))
+        shutil.copyfile(prog, local)
+        os.chmod(local, 0o755)
+        prog = local
+    pkg = os.path.dirname(LIB)
+    env = dict(os.environ, OMP_NUM_THREADS="1",
+               LD_LIBRARY_PATH=os.pathsep.join(filter(None, [pkg, os.environ.get("LD_LIBRARY_PATH")])))
     return subprocess.run([prog, a, r, *args], cwd=d, capture_output=True, text=True, env=env, timeout=timeout)
 
 
