@@ -17,6 +17,9 @@
 // Values are parsed with std::from_chars, correctly rounded like the C library's strtod that
 // the reference's fscanf("%lg") uses.
 
+#include <omp.h>
+
+#include <algorithm>
 #include <cctype>
 #include <charconv>
 #include <cstdint>
@@ -60,6 +63,29 @@ struct MtxBuf {
 };
 thread_local MtxBuf g_mtx;
 
+// Token readers over [p, e): whitespace (space, tab, newline, carriage return) separates
+// tokens, as for fscanf. A real may carry a leading '+', which from_chars does not take.
+inline bool is_space(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\r'; }
+inline void skip_space(const char *&p, const char *e) {
+    while (p < e && is_space(*p)) p++;
+}
+inline bool tok_integer(const char *&p, const char *e, long &x) {
+    skip_space(p, e);
+    auto r = std::from_chars(p, e, x);
+    if (r.ec != std::errc()) return false;
+    p = r.ptr;
+    return true;
+}
+inline bool tok_real(const char *&p, const char *e, double &x) {
+    skip_space(p, e);
+    const char *b = p;
+    if (b < e && *b == '+') ++b;
+    auto r = std::from_chars(b, e, x, std::chars_format::general);
+    if (r.ec != std::errc()) return false;
+    p = r.ptr;
+    return true;
+}
+
 struct Reader {
     std::string text;
     size_t pos = 0;
@@ -72,28 +98,87 @@ struct Reader {
         if (!out.empty() && out.back() == '\r') out.pop_back();
         return true;
     }
-    void skip_space() {
-        while (pos < text.size() && (text[pos] == ' ' || text[pos] == '\t' || text[pos] == '\n' || text[pos] == '\r'))
-            pos++;
-    }
-    bool integer(long &x) {
-        skip_space();
-        const char *b = text.data() + pos, *e = text.data() + text.size();
-        auto r = std::from_chars(b, e, x);
-        if (r.ec != std::errc()) return false;
-        pos += r.ptr - b;
+    template <typename T, bool (*F)(const char *&, const char *, T &)>
+    bool token(T &x) {
+        const char *p = text.data() + pos;
+        if (!F(p, text.data() + text.size(), x)) return false;
+        pos = p - text.data();
         return true;
     }
-    bool real(double &x) {
-        skip_space();
-        const char *b = text.data() + pos, *e = text.data() + text.size();
-        if (b < e && *b == '+') ++b;
-        auto r = std::from_chars(b, e, x, std::chars_format::general);
-        if (r.ec != std::errc()) return false;
-        pos = r.ptr - text.data();
-        return true;
-    }
+    bool integer(long &x) { return token<long, tok_integer>(x); }
+    bool real(double &x) { return token<double, tok_real>(x); }
 };
+
+// Files with fewer entries are read on one thread.
+constexpr long kParallelEntries = 1 << 16;
+
+// The coordinate entries of a large file, parsed in pieces on all host threads. The text
+// after the size line is cut at line starts into pieces; each piece is read as whole
+// (row, col, value) triples, and the pieces are joined in file order. It returns false, and
+// the caller reads the entries on one thread, when any piece is not a run of whole triples
+// (an entry broken across a cut, or anything that is not an entry) or when the pieces hold
+// fewer than Z entries: the one-thread reader then gives its own result or error. Otherwise
+// I, J and val hold the first Z triples as read (1-based, unchecked).
+bool parse_entries_parallel(const char *b, const char *e, long Z, std::vector<int> &I, std::vector<int> &J,
+                            std::vector<double> &val) {
+    const int T = std::max(1, omp_get_max_threads());
+    const int P = 4 * T;
+    std::vector<const char *> cut(P + 1);
+    cut[0] = b;
+    cut[P] = e;
+    for (int q = 1; q < P; ++q) {
+        const char *c = b + (size_t)(e - b) * q / P;
+        if (c < cut[q - 1]) c = cut[q - 1];
+        while (c < e && c[-1] != '\n') c++;
+        cut[q] = c;
+    }
+    struct Piece {
+        std::vector<int> ij;   // row, col pairs; 0 stands for a value outside 1..INT_MAX
+        std::vector<double> v;
+        bool ok = true;
+    };
+    std::vector<Piece> pc(P);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(T)
+    for (int q = 0; q < P; ++q) {
+        Piece &k = pc[q];
+        const char *p = cut[q], *end = cut[q + 1];
+        size_t lines = 1;   // one entry per line, as written: sizes the piece's arrays
+        for (const char *c = p; (c = static_cast<const char *>(std::memchr(c, '\n', end - c))); ++c) lines++;
+        k.ij.reserve(2 * lines);
+        k.v.reserve(lines);
+        auto as_index = [](long a) { return (a < 1 || a > 0x7fffffffL) ? 0 : (int)a; };
+        for (;;) {
+            skip_space(p, end);
+            if (p >= end) break;
+            long a = 0, c = 0;
+            double x = 0.0;
+            if (!tok_integer(p, end, a) || !tok_integer(p, end, c) || !tok_real(p, end, x) ||
+                (p < end && !is_space(*p))) {
+                k.ok = false;
+                break;
+            }
+            k.ij.push_back(as_index(a));
+            k.ij.push_back(as_index(c));
+            k.v.push_back(x);
+        }
+    }
+    std::vector<long> at(P + 1, 0);
+    for (int q = 0; q < P; ++q) {
+        if (!pc[q].ok) return false;
+        at[q + 1] = at[q] + (long)pc[q].v.size();
+    }
+    if (at[P] < Z) return false;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(T)
+    for (int q = 0; q < P; ++q) {
+        const long lo = at[q], hi = std::min(at[q + 1], Z);
+        for (long k = lo; k < hi; ++k) {
+            I[k] = pc[q].ij[2 * (k - lo)];
+            J[k] = pc[q].ij[2 * (k - lo) + 1];
+            val[k] = pc[q].v[k - lo];
+        }
+    }
+    return true;
+}
 
 int slurp(const char *path, std::string &out) {
     std::FILE *f = std::fopen(path, "rb");
@@ -179,7 +264,26 @@ int fiim_read_mtx(const char *path, int form, int *n, int *nnz, int *issym, int 
     if (M > 0x7ffffffeL || Z > 0x3fffffffL) return fiim::set_error(FIIM_EARG, "matrix too large for int32 CSR");
     std::vector<int> I(Z), J(Z);
     std::vector<double> val(Z);
-    for (long k = 0; k < Z; ++k) {
+    bool par = Z >= kParallelEntries &&
+               parse_entries_parallel(rd.text.data() + rd.pos, rd.text.data() + rd.text.size(), Z, I, J, val);
+    if (par) {
+        bool ok = true;
+#pragma omp parallel for reduction(&& : ok)
+        for (long k = 0; k < Z; ++k) {
+            const int a = I[k], b = J[k];
+            if (a < 1 || a > M || b < 1 || b > N) {
+                ok = false;
+            } else if (sym && form == 1) {
+                I[k] = b - 1;
+                J[k] = a - 1;
+            } else {
+                I[k] = a - 1;
+                J[k] = b - 1;
+            }
+        }
+        par = ok;   // otherwise the one-thread reader below reports the first bad entry
+    }
+    for (long k = 0; !par && k < Z; ++k) {
         long a = 0, b = 0;
         double x = 0.0;
         if (!rd.integer(a) || !rd.integer(b) || !rd.real(x))
@@ -220,6 +324,7 @@ int fiim_read_mtx(const char *path, int form, int *n, int *nnz, int *issym, int 
         m.ci[at] = J[k];
         m.v[at] = val[k];
     }
+#pragma omp parallel for schedule(dynamic, 4096) if (Z >= kParallelEntries)
     for (long i = 0; i < N; ++i)
         if (m.rp[i + 1] - 1 > m.rp[i]) qsort_pairs(m.ci.data(), m.v.data(), m.rp[i], m.rp[i + 1] - 1);
     *n = m.n;

@@ -61,6 +61,86 @@ def test_reader_matches_reference_reader(tmp_path, symmetry, dups):
     assert np.array_equal(Ai, Ri) and np.array_equal(Aj, Rj) and np.array_equal(Av, Rv)
 
 
+# Files of at least 65,536 entries are parsed in pieces on all host threads; these cases
+# hold 150,000 and more, so they take that path.
+LARGE_N, LARGE_M = 20000, 150000
+
+
+@pytest.mark.parametrize("symmetry,dups", [("general", 0), ("general", 3000), ("symmetric", 0),
+                                           ("symmetric", 2000)])
+def test_large_reader_matches_reference_reader(tmp_path, symmetry, dups):
+    """The piecewise parse of a large file gives the reference reader's arrays bit for bit."""
+    if not O.have_ref("afiim"):
+        pytest.skip("reference library not built")
+    rows, cols, vals = random_entries(LARGE_N, LARGE_M, 7 + dups, lower=(symmetry == "symmetric"), dups=dups)
+    path = str(tmp_path / "m.mtx")
+    write_mtx(path, LARGE_N, rows, cols, vals, symmetry)
+    (Ai, Aj, Av), _ = FB.read_mtx(path)
+    Ri, Rj, Rv = O.read_matrix(path)
+    assert np.array_equal(Ai, Ri) and np.array_equal(Aj, Rj) and np.array_equal(Av, Rv)
+    if symmetry == "symmetric":
+        (Ui, Uj, Uv), sym = FB.read_mtx(path, form="pdfiim")
+        assert sym and len(Uj) == len(rows)
+        r_of = np.repeat(np.arange(LARGE_N), np.diff(Ui))
+        assert (Uj >= r_of).all()
+
+
+def _layout(rows, cols, vals, how):
+    """Entry text laid out otherwise than one entry per line; the reference reads tokens
+    with fscanf, whatever the line breaks."""
+    ent = [f"{i + 1} {j + 1} {float(v)!r}" for i, j, v in zip(rows, cols, vals)]
+    if how == "several_per_line":
+        return "\n".join("  ".join(ent[k:k + 3]) for k in range(0, len(ent), 3)) + "\n"
+    if how == "broken_entries":
+        return "".join(e.replace(" ", "\n", 1) + "\n" if k % 7 == 0 else e + "\n" for k, e in enumerate(ent))
+    if how == "blank_lines_crlf":
+        return "".join(e + ("\r\n\r\n" if k % 5 == 0 else "\r\n") for k, e in enumerate(ent))
+    if how == "signs_and_exponents":
+        return "".join(f"{i + 1}\t{j + 1}\t{'+' if v >= 0 else ''}{float(v):.17e}\n"
+                       for i, j, v in zip(rows, cols, vals))
+    if how == "trailing_text":
+        return "\n".join(ent) + "\n% not an entry\nend of file\n"
+    raise ValueError(how)
+
+
+@pytest.mark.parametrize("how", ["several_per_line", "broken_entries", "blank_lines_crlf", "signs_and_exponents",
+                                 "trailing_text"])
+def test_large_reader_layouts_match_reference_reader(tmp_path, how):
+    """Line layouts that a piece cannot split on (entries broken across lines, text after
+    the entries) and ones it can (several entries per line, blank lines, CRLF, signs):
+    either way the arrays are the reference reader's."""
+    if not O.have_ref("afiim"):
+        pytest.skip("reference library not built")
+    rows, cols, vals = random_entries(LARGE_N, LARGE_M, 3)
+    path = str(tmp_path / "m.mtx")
+    with open(path, "w", newline="") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n")
+        f.write(f"{LARGE_N} {LARGE_N} {len(rows)}\n")
+        f.write(_layout(rows, cols, vals, how))
+    (Ai, Aj, Av), _ = FB.read_mtx(path)
+    Ri, Rj, Rv = O.read_matrix(path)
+    assert np.array_equal(Ai, Ri) and np.array_equal(Aj, Rj) and np.array_equal(Av, Rv)
+
+
+def test_large_reader_errors_name_the_entry(tmp_path):
+    """A bad entry in a large file is reported with its position, as for a small one; a file
+    with fewer entries than its size line declares is rejected."""
+    rows, cols, vals = random_entries(LARGE_N, LARGE_M, 4)
+    rows = rows.copy()
+    rows[100000] = LARGE_N + 5
+    path = str(tmp_path / "m.mtx")
+    write_mtx(path, LARGE_N, rows, cols, vals)
+    with pytest.raises(FB.FiimError, match=rf"entry 100001 \({LARGE_N + 6}, \d+\) is outside"):
+        FB.read_mtx(path)
+    rows[100000] = 0
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n")
+        f.write(f"{LARGE_N} {LARGE_N} {len(rows) + 10}\n")
+        f.writelines(f"{i + 1} {j + 1} {float(v)!r}\n" for i, j, v in zip(rows, cols, vals))
+    with pytest.raises(FB.FiimError, match=rf"entry {len(rows) + 1} is malformed"):
+        FB.read_mtx(path)
+
+
 def test_pdfiim_form_keeps_the_upper_triangle(tmp_path):
     """PDFIIM's reader (PDFIIM/src/rw_matrix.cpp:104-150) reads a symmetric file as its mirror
     image: the lower-stored entries become the upper triangle, flagged symmetric. Its
