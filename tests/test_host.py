@@ -250,3 +250,15 @@ def test_host_pdfiim_rejects_unserved_patterns():
     for patt in "LU":
         with pytest.raises(FB.FiimError):
             FB.pdfiim_build(A, 0.05, patt=patt)
+
+
+def test_block_diag_matches_scipy():
+    """The batched handle's concatenation: block-diagonal CSR in global numbering, with the
+    systems' first rows."""
+    import scipy.sparse as sp
+    mats = [FB.gen_convdiff2d(s, 1.0 + s, 0.7, 0.5) for s in (3, 5, 4)]
+    (Ai, Aj, Av), rows = FB.block_diag(mats)
+    ref = sp.block_diag([sp.csr_matrix((m[2], m[1], m[0])) for m in mats], format="csr")
+    assert np.array_equal(Ai, ref.indptr) and np.array_equal(Aj, ref.indices) and np.array_equal(Av, ref.data)
+    assert list(rows) == [0, 9, 34, 50]
+    assert Ai.dtype == np.int32 and Aj.dtype == np.int32
