@@ -166,7 +166,18 @@ def PBiCGSTAB(n, Av, Aj, Ai, b, tol, NMAX, Gv, Gj, Gi, IDv, Hv, Hj, Hi, Lv, Lj, 
 
 
 # ----------------------------------------------------------------------------- handle API
-class Solver:
+class _Handle:
+    """A library handle: close() frees it; a with-block closes it on leaving."""
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+        return False
+
+
+class Solver(_Handle):
     """Set up once (upload, SpMV shape tuning, graph capture); solve many times.
 
     A: (Ai, Aj, Av); F: dict with Gi, Gj, Gv, IDv, Hi, Hj, Hv (and Li.., Ui.. for mode 'C').
@@ -360,7 +371,7 @@ def dist_unique_id() -> bytes:
     return bytes(buf)
 
 
-class DistSolver:
+class DistSolver(_Handle):
     """One rank of a row-partitioned solve (one process per GPU). Collective: every rank
     constructs it with the same uid, world and row_starts, and calls solve together.
 
@@ -429,7 +440,7 @@ def block_diag(mats):
     return (Ai.astype(np.int32), Aj.astype(np.int32), Av), sys_rows
 
 
-class BatchSolver:
+class BatchSolver(_Handle):
     """Many independent systems in one device-driven loop (fiim_batch_*).
 
     systems: list of (A, F) with A = (Ai, Aj, Av) and F = {Gi, Gj, Gv, IDv, Hi, Hj, Hv}.
@@ -482,7 +493,7 @@ class BatchSolver:
             pass
 
 
-class BlockSolver:
+class BlockSolver(_Handle):
     """k <= 32 right-hand sides of one system, sharing the sparse products (fiim_block_*).
     B, X: n x k row-major FP64 (numpy, or torch CUDA tensors with memory='device')."""
 

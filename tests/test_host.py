@@ -262,3 +262,23 @@ def test_block_diag_matches_scipy():
     assert np.array_equal(Ai, ref.indptr) and np.array_equal(Aj, ref.indices) and np.array_equal(Av, ref.data)
     assert list(rows) == [0, 9, 34, 50]
     assert Ai.dtype == np.int32 and Aj.dtype == np.int32
+
+
+def test_handles_close_on_leaving_a_with_block():
+    """Solver, DistSolver, BatchSolver and BlockSolver are context managers whose exit calls
+    close(), also when the block raises."""
+    for cls in (FB.Solver, FB.DistSolver, FB.BatchSolver, FB.BlockSolver):
+        assert issubclass(cls, FB._Handle)
+
+    class Probe(FB._Handle):
+        closed = 0
+
+        def close(self):
+            Probe.closed += 1
+
+    with Probe() as h:
+        assert isinstance(h, Probe)
+    with pytest.raises(ValueError):
+        with Probe():
+            raise ValueError("inside")
+    assert Probe.closed == 2
