@@ -16,8 +16,8 @@ NMAX 1200. A step is one full solve. Synthetic data (the reference names no data
 
 --impl reference times the reference's own EPBiCGSTAB (oracle/_ref: the reference's
 sources compiled against the project's MKL shim, OpenMP on all host cores) on the same
-system with the reference's own pdfiim factors; each step is a bounded sample (a capped
-number of iterations), scaled to solves/s by the full solve's iteration count.
+system, built with numpy (no library of this project is loaded), with the reference's own
+pdfiim factors; each step is one full solve, the EPBiCGSTAB call alone timed.
 
 Multi-GPU (torchrun): by default one full replica per rank (nothing is exchanged during a
 solve), value = total solves / max-over-ranks time, weak scaling. --partition rows splits the
@@ -64,13 +64,77 @@ def workload(N):
     return A, b
 
 
-def config(N, nnz, extra=None):
-    c = {"workload": f"convdiff3d_{N} (n={N ** 3:,}, nnz={nnz:,}) PDFIIM eps 0.05 (2,2,1) FP64 BiCGSTAB",
-         "n": N ** 3, "nnz": int(nnz), "tol": 1e-8, "nmax": 1200,
-         "l2": "inputs larger than L2 (A+G+H+vectors >> 126 MB), no flush"}
-    if extra:
-        c.update(extra)
-    return c
+# The same system built without the library, for the reference arm: a process that times the
+# reference maps none of this project's code. Both restate fiim_gen.cpp (fiim_gen_convdiff3d,
+# fiim_rand_normal) operation for operation, so the arrays are the library's bit for bit
+# (tests/test_bench_contract.py compares them).
+_U64 = np.uint64
+
+
+def _splitmix64(s):
+    """Returns (advanced state, output) of splitmix64 on a uint64 array (wrapping arithmetic)."""
+    s = s + _U64(0x9E3779B97F4A7C15)
+    z = s
+    z = (z ^ (z >> _U64(30))) * _U64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> _U64(27))) * _U64(0x94D049BB133111EB)
+    return s, z ^ (z >> _U64(31))
+
+
+def rand_normal_host(n, seed):
+    """fiim_rand_normal: stream i is seeded from (seed, i); Box-Muller of its next two draws.
+    log and cos are libm's, through the math module, as the library calls them."""
+    import math
+    idx = np.arange(n, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        s = _U64(seed) ^ (_U64(0xD1B54A32D192ED03) * (idx + _U64(1)))
+        s, _ = _splitmix64(s)
+        s, z1 = _splitmix64(s)
+        s, z2 = _splitmix64(s)
+    u1 = (z1 >> _U64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    u2 = (z2 >> _U64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    u1 = np.where(u1 < 1e-300, 1e-300, u1)
+    log, cos, sqrt = math.log, math.cos, math.sqrt
+    return np.array([sqrt(-2.0 * log(a)) * cos(6.283185307179586 * c) for a, c in zip(u1.tolist(), u2.tolist())])
+
+
+def convdiff3d_host(N, peclet=0.5):
+    """fiim_gen_convdiff3d: 7-point upwind convection-diffusion, entries of a row in the
+    order z-1, y-1, x-1, diagonal, x+1, y+1, z+1."""
+    n, NN = N ** 3, N * N
+    i = np.arange(n, dtype=np.int64)
+    x, y, z = i % N, (i // N) % N, i // NN
+    keep = np.stack([z > 0, y > 0, x > 0, np.ones(n, bool), x < N - 1, y < N - 1, z < N - 1], axis=1)
+    cols = i[:, None] + np.array([-NN, -N, -1, 0, 1, N, NN], np.int64)[None, :]
+    lo, hi = -1.0 - peclet, -1.0
+    vals = np.broadcast_to(np.array([lo, lo, lo, 6.0 + 3.0 * peclet, hi, hi, hi]), (n, 7))
+    Ai = np.zeros(n + 1, np.int32)
+    Ai[1:] = np.cumsum(keep.sum(axis=1))
+    return Ai, cols[keep].astype(np.int32), vals[keep].copy()
+
+
+def workload_host(N):
+    return convdiff3d_host(N, 0.5), rand_normal_host(N ** 3, SEED)
+
+
+def repo_libraries():
+    """Shared objects of this repository mapped into this process (from /proc/self/maps)."""
+    out = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if len(line.split()) >= 6 else ""
+                if path.endswith(".so") and path.startswith(ROOT + os.sep):
+                    out.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(out)
+
+
+def config(N, nnz):
+    """The workload, identical in both arms' lines."""
+    return {"workload": f"convdiff3d_{N} (n={N ** 3:,}, nnz={nnz:,}) PDFIIM eps 0.05 (2,2,1) FP64 BiCGSTAB",
+            "n": N ** 3, "nnz": int(nnz), "tol": 1e-8, "nmax": 1200,
+            "l2": "inputs larger than L2 (A+G+H+vectors >> 126 MB), no flush"}
 
 
 class Clocks:
@@ -140,7 +204,9 @@ class Clocks:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_init():
+def dist_init(backend="nccl"):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE); NCCL for the barrier
+    and the max over ranks. backend 'gloo' is the CPU dry run of the launcher."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     if ws == 1:
         return 0, 1, None
@@ -148,8 +214,14 @@ def dist_init():
     import torch
     import torch.distributed as dist
     rank, local = int(os.environ["RANK"]), int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    if backend == "gloo":
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+    else:
+        if local >= torch.cuda.device_count():
+            raise SystemExit(f"rank {rank}: local rank {local} but only {torch.cuda.device_count()} GPUs visible")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    print(f"bench: rank {rank} of {ws} ({backend}, local rank {local})", file=sys.stderr, flush=True)
     return rank, ws, dist
 
 
@@ -162,33 +234,52 @@ def max_over_ranks(dist, v):
     if dist is None:
         return v
     import torch
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device="cpu" if dist.get_backend() == "gloo" else "cuda")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
 
+def launch_ranks(args):
+    """`bench.py --gpus N` started without torchrun: start the N ranks on this node (one process
+    per GPU, rendezvous on 127.0.0.1) with the same arguments, and return their status."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    print("bench: starting " + " ".join(cmd), file=sys.stderr, flush=True)
+    return subprocess.call(cmd)
+
+
+def run_dry(args):
+    """The launcher and timing protocol without a GPU (gloo): every rank runs W untimed and K
+    timed steps between barriers, rank r's step lasting (r + 1) x 10 ms, and rank 0 prints the
+    max over ranks. Nothing is solved: the line says dry_run and carries no metric."""
+    rank, ws, dist = dist_init("gloo")
+    step = lambda: time.sleep(0.01 * (rank + 1))
+    for _ in range(args.warmup):
+        step()
+    barrier(dist)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    mine = time.perf_counter() - t0
+    barrier(dist)
+    worst = max_over_ranks(dist, mine)
+    if rank == 0:
+        print(json.dumps({"dry_run": True, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1000 * worst / args.steps, "rank0_ms_per_step": 1000 * mine / args.steps}),
+              flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 # ---------------------------------------------------------------------------- CPU reference
-def reference_sample(A, b, F, iters_full, sample_its, kind):
-    """Time the reference's own EPBiCGSTAB (or the oracle port) for `sample_its` iterations."""
-    sys.path.insert(0, ORACLE)
-    import pyoracle as O
-    n = len(b)
-    if kind == "reference":
-        threads = os.cpu_count() or 1
-        O.set_threads(threads, "pdfiim")
-        t0 = time.perf_counter()
-        x, res, it, info = O.ref_solve("pdfiim", A, b, F, tol=1e-8, nmax=sample_its)
-        dt = time.perf_counter() - t0
-    else:
-        threads = 1
-        t0 = time.perf_counter()
-        x, res, it, info = O.bicgstab("pdfiim", A, b, F, tol=1e-8, nmax=sample_its)
-        dt = time.perf_counter() - t0
-    per_iter = dt / max(it, 1)
-    return {"value": 1.0 / (per_iter * iters_full), "per_iter_s": per_iter, "threads": threads, "its": it, "dt": dt}
-
-
 def cpu_kind():
+    """'reference' when the reference compiled against the MKL shim is present (oracle/_ref),
+    else 'port' (the plain-C restatement, one thread)."""
     sys.path.insert(0, ORACLE)
     import pyoracle as O
     if O.have_ref("pdfiim"):
@@ -197,43 +288,97 @@ def cpu_kind():
     return "port"
 
 
+class CpuSolves:
+    """Full solves of the benchmark system by the reference's own EPBiCGSTAB
+    (PDFIIM/src/bicgstab.cpp:80-310, OpenMP on every host core through the MKL shim), with the
+    reference's own pdfiim factors (PDFIIM/src/parPrec.cpp:95-588). The system is held as the
+    reference's sparseMatrix objects, built once: each step times the EPBiCGSTAB call alone.
+    Without oracle/_ref, the restatement (one thread) stands in, on a bounded sample of
+    `port_its` iterations scaled to a full solve's count (a full 1-thread solve takes minutes)."""
+
+    def __init__(self, A, b, port_its=12):
+        sys.path.insert(0, ORACLE)
+        import pyoracle as O
+        self.O, self.A, self.b, self.port_its = O, A, b, port_its
+        self.kind = cpu_kind()
+        t0 = time.perf_counter()
+        if self.kind == "reference":
+            self.threads = os.cpu_count() or 1
+            O.set_threads(self.threads, "pdfiim")
+            self.F = O.pdfiim_build(A, **PDFIIM_PARAMS)
+            self.sys = O.RefPdfiimSystem(A, self.F)
+        else:
+            self.threads = 1
+            self.F = None
+        self.setup_s = time.perf_counter() - t0
+        self.its_full = None
+
+    def factors(self):
+        return self.F
+
+    def step(self):
+        """One step: (seconds, iterations, info, x); a full solve (reference) or the sample."""
+        if self.kind == "reference":
+            x, res, it, info, secs = self.sys.run(self.b, tol=1e-8, nmax=1200)
+            self.its_full = it
+            return secs, it, info, x
+        if self.F is None:
+            # the port has no construction of its own: the reference's factors equal the
+            # library's bit for bit (tests/test_host.py), so the port uses those
+            import fiim_b200 as FB
+            self.F = FB.pdfiim_build(self.A, **PDFIIM_PARAMS)
+        t0 = time.perf_counter()
+        x, res, it, info = self.O.bicgstab("pdfiim", self.A, self.b, self.F, tol=1e-8, nmax=self.port_its)
+        dt = time.perf_counter() - t0
+        return dt, it, info, x
+
+    def describe(self, steps, its_full, dt_total):
+        if self.kind == "reference":
+            return (f"{steps} full solves of the {len(self.b):,}-row system ({its_full} iterations each, "
+                    f"{dt_total:.1f} s), the EPBiCGSTAB call alone timed; sparseMatrix objects built once")
+        return (f"{steps} x {self.port_its} iterations of the restatement (one thread, {dt_total:.1f} s), "
+                f"scaled by a full solve's {its_full} iterations")
+
+    def close(self):
+        if self.kind == "reference":
+            self.sys.close()
+
+
 def run_reference(args):
-    rank, ws, dist = (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), None)
+    """The reference arm: the reference's own CPU solve on this box's host cores. It builds the
+    system with numpy (workload_host), so this process maps no library of this project."""
+    rank = int(os.environ.get("RANK", "0"))
+    ws = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
     if rank != 0:
         return 0
-    sys.path.insert(0, ORACLE)
-    import pyoracle as O
-    kind = cpu_kind()
-    A, b = workload(args.size)
+    A, b = workload_host(args.size)
     nnz = int(A[0][-1])
-    threads = os.cpu_count() or 1
-    if kind == "reference":
-        O.set_threads(threads, "pdfiim")
-        F = O.pdfiim_build(A, **PDFIIM_PARAMS)
-        # iterations of the full solve: the reference's own count on this system
-        iters_full = args.ref_iters
-    else:
-        import fiim_b200 as FB
-        F = FB.pdfiim_build(A, **PDFIIM_PARAMS)
-        iters_full = args.ref_iters
-    sample_its = args.ref_sample_its
+    cs = CpuSolves(A, b)
     for _ in range(args.warmup):
-        reference_sample(A, b, F, iters_full, max(2, sample_its // 4), kind)
-    vals, dts = [], []
+        cs.step()
+    secs, its, infos = [], [], []
     for _ in range(args.steps):
-        r = reference_sample(A, b, F, iters_full, sample_its, kind)
-        vals.append(r["value"])
-        dts.append(r["dt"])
-    v = float(np.median(vals))
-    sample = (f"{sample_its} BiCGSTAB iterations of the {args.size}^3 system per step, scaled by the full solve's "
-              f"{iters_full} iterations")
+        s, it, info, _ = cs.step()
+        secs.append(s)
+        its.append(it)
+        infos.append(info)
+    if cs.kind == "reference":
+        its_full, tot = int(np.median(its)), sum(secs)
+    else:
+        # the port's samples stop at port_its; a full solve takes the reference's 99 on this system
+        its_full, tot = 99, sum(s * 99 / max(it, 1) for s, it in zip(secs, its))
+    v = args.steps / tot
+    cs.close()
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": ws,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * float(np.mean(dts)),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": config(args.size, nnz, {"iterations_per_solve": iters_full}),
-            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": threads if kind == "reference" else 1,
-                             "kind": kind, "sample": sample},
-            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "data": "synthetic", "config": config(args.size, nnz),
+            "iterations": its_full, "info": infos[-1], "setup_s": round(cs.setup_s, 2),
+            "parallelism": f"host, {cs.threads} OpenMP threads",
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cs.threads, "kind": cs.kind,
+                             "sample": cs.describe(args.steps, its_full, sum(secs))},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "libraries_loaded": repo_libraries()}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -561,7 +706,7 @@ def run_multi_rhs(args, rank=0, world=1, dist=None):
 def run_ours(args):
     import torch
     import fiim_b200 as FB
-    rank, ws, dist = dist_init()
+    rank, ws, dist = dist_init("nccl")
     dev = torch.device("cuda", torch.cuda.current_device() if ws > 1 else 0)
     torch.cuda.set_device(dev)
     t0 = time.perf_counter()
@@ -596,6 +741,7 @@ def run_ours(args):
     dev_ms_max = max_over_ranks(dist, dev_ms)
     iters = [r["iter"] for r in results]
     assert all(r["info"] == 0 for r in results), results[0]
+    x_fp64 = tx.cpu().numpy()
     value = args.steps * ws / (dev_ms_max / 1000.0)
     it_bytes = S.iteration_bytes()
     hbm_gbs = sum(iters) * it_bytes / (dev_ms / 1000.0) / 1e9
@@ -635,7 +781,7 @@ def run_ours(args):
     S.close()
 
     # ---- mixed precision: FP64 iterative refinement around an FP32 inner BiCGSTAB
-    mixed = None
+    mixed, mixed_x = None, {}
     if not args.no_mixed:
         mixed = {"fp64_to_1e-10": fp64_10}
         fp64_8 = dev_ms / args.steps
@@ -652,6 +798,7 @@ def run_ours(args):
             ms = sum(q["device_ms"] for q in rr) / len(rr)
             err = float(torch.linalg.norm(tx - x_ref10) / torch.linalg.norm(x_ref10))
             same = fp64_10["ms"] if mtol == 1e-10 else fp64_8
+            mixed_x[f"{prec}_to_{mtol:g}"] = tx.cpu().numpy()
             mixed[f"{prec}_to_{mtol:g}"] = {
                 "solves_per_s": round(1000.0 / ms, 4), "ms_per_solve": round(ms, 4), "tol": mtol,
                 "inner_tol": 1e-5, "refine_steps": rr[-1]["refine_steps"], "inner_iterations": rr[-1]["iter"],
@@ -685,21 +832,36 @@ def run_ours(args):
     if args.partition == "rows" or (ws == 1 and not args.no_dist):
         part = run_partitioned(args, A, F, b, rank, ws, dist, dev)
 
-    # ---- CPU baseline (rank 0, N = 1): bounded sample of the reference's solve
+    # ---- CPU baseline (rank 0, N = 1): full solves by the reference's own EPBiCGSTAB with its
+    # own pdfiim factors; its solutions also give the GPU solutions' distance from the
+    # reference's (FP64 to 1e-8, and the mixed legs against its solution to 1e-10).
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        kind = cpu_kind()
-        Fc = F
-        if kind == "reference":
-            sys.path.insert(0, ORACLE)
-            import pyoracle as O
-            O.set_threads(os.cpu_count() or 1, "pdfiim")
-            Fc = O.pdfiim_build(A, **PDFIIM_PARAMS)
-        its = int(np.median(iters))
-        r = reference_sample(A, b, Fc, its, args.cpu_sample_its, kind)
-        cpu = {"value": r["value"], "unit": "solves/s", "cores": r["threads"], "kind": kind,
-               "sample": f"{r['its']} BiCGSTAB iterations of the full {args.size}^3 solve ({r['dt']:.1f} s), "
-                         f"scaled by the GPU solve's {its} iterations"}
+        cs = CpuSolves(A, b)
+        cs.step()                                   # warm-up
+        secs, its = [], []
+        for _ in range(args.cpu_solves):
+            s_, it_, info_, x_ref = cs.step()
+            secs.append(s_)
+            its.append(it_)
+        if cs.kind == "reference":
+            its_full, tot = its[-1], sum(secs)
+        else:
+            its_full = int(np.median(iters))
+            tot = sum(s_ * its_full / max(it_, 1) for s_, it_ in zip(secs, its))
+        cpu = {"value": len(secs) / tot, "unit": "solves/s", "cores": cs.threads, "kind": cs.kind,
+               "sample": cs.describe(len(secs), its_full, sum(secs)), "iterations": its_full}
+        if cs.kind == "reference":
+            nx = np.linalg.norm(x_ref)
+            cpu["gpu_vs_reference"] = {"iterations": [iters[-1], its_full],
+                                       "x_rel_diff": float(np.linalg.norm(x_fp64 - x_ref) / nx)}
+            if mixed_x:
+                x10, _, it10, _, _ = cs.sys.run(b, tol=1e-10, nmax=1200)
+                n10 = np.linalg.norm(x10)
+                cpu["gpu_vs_reference"]["reference_iterations_to_1e-10"] = it10
+                for key, xm in mixed_x.items():
+                    mixed[key]["rel_err_vs_reference_fp64_1e-10_solution"] = float(np.linalg.norm(xm - x10) / n10)
+        cs.close()
 
     if rank == 0:
         headline, scaling, par, ms_step = value, "weak", f"replicas x{ws}", dev_ms_max / args.steps
@@ -712,8 +874,8 @@ def run_ours(args):
         line = {"metric": METRIC, "value": round(headline, 4), "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True,
                 "scaling": scaling, "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": config(args.size, nnz, {"iterations": iters[0], "parallelism": par,
-                                                  "setup_s": round(t_setup, 2)}),
+                "config": config(args.size, nnz), "iterations": iters[0], "parallelism": par,
+                "setup_s": round(t_setup, 2),
                 "hbm_gbs": round(hbm_gbs, 1), "hbm_frac": round(hbm_gbs / peak, 4),
                 "iteration_bytes": it_bytes, "true_relres": results[-1]["true_relres"],
                 "resval": results[-1]["resval"], "wall_ms_per_step": round(1000 * wall / args.steps, 4),
@@ -746,20 +908,27 @@ def main():
                          "row blocks over the ranks (strong scaling)")
     ap.add_argument("--no-dist", action="store_true", help="skip the row-partitioned leg at N = 1")
     ap.add_argument("--no-small", action="store_true", help="skip the small plain case (Poisson 128^2)")
-    ap.add_argument("--cpu-sample-its", type=int, default=12)
-    ap.add_argument("--ref-sample-its", type=int, default=10)
-    ap.add_argument("--ref-iters", type=int, default=99,
-                    help="iterations of the full 128^3 solve (the reference's own count, for scaling samples)")
+    ap.add_argument("--cpu-solves", type=int, default=3, help="timed full solves of the CPU baseline leg")
     # DRAM bytes per launch of the dominant kernel (H's SpMV) from an ncu capture of the
     # 96^3 case (read + write = 0.842 x its algorithmic bytes: the column stream is stored as
     # 16-bit offsets), scaled to the 128^3 launch by the units processed (entries and rows,
     # which the traffic is proportional to).
     ap.add_argument("--ncu-traffic", type=float, default=278.8e6,
                     help="dram bytes per launch of the dominant kernel from an ncu capture")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="no GPU: check the rank launcher and max-over-ranks timing over gloo (solves nothing)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
-    return run_reference(args) if args.impl == "reference" else run_ours(args)
+    if args.impl == "reference":
+        return run_reference(args)
+    ws_env = os.environ.get("WORLD_SIZE")
+    if ws_env is None and args.gpus > 1:
+        return launch_ranks(args)
+    if ws_env is not None and int(ws_env) != args.gpus:
+        print(f"error: --gpus {args.gpus} but WORLD_SIZE={ws_env}: no result", file=sys.stderr)
+        return 2
+    return run_dry(args) if args.dry_run else run_ours(args)
 
 
 if __name__ == "__main__":

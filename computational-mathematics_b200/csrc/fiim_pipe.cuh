@@ -113,14 +113,17 @@ k_spmv_pipe(CsrView<double> M, const int *__restrict__ rb, int nblk, const doubl
         const int r0 = __ldg(rb + blk), r1 = __ldg(rb + blk + 1);
         const int e0 = __ldg(M.rp + r0), e1 = __ldg(M.rp + r1);
         if (staged(blk)) {
-            const bool ok = mbar_wait(buf ? bar1 : bar0, buf ? phase1 : phase0);
+            const uint32_t cur = buf ? phase1 : phase0;
+            const bool ok = mbar_wait(buf ? bar1 : bar0, cur);
             if (buf) phase1 ^= 1u;
             else phase0 ^= 1u;
             if (__syncthreads_or(!ok)) {
-                // A copy did not complete in time: flag it, give the other buffer's copy a
-                // bounded chance to land, and stop this CTA.
+                // A copy did not complete in time: flag it, give this buffer's copy and the
+                // other buffer's copy one more bounded wait each, and stop this CTA, so that
+                // no copy is left writing into shared memory it no longer owns.
                 if (threadIdx.x == 0) {
                     atomicExch(fault, 1);
+                    if (!ok) mbar_wait(buf ? bar1 : bar0, cur);
                     if (nxt < nblk && staged(nxt)) mbar_wait(buf ? bar0 : bar1, buf ? phase0 : phase1);
                 }
                 return;

@@ -59,7 +59,7 @@ struct Solver : SolverBase {
     bool persistent = false;
     int persist_grid = 0;
     unsigned *pbar = nullptr;    // grid barrier words
-    int wait_limit = 1 << 21;    // barrier polls (each a sleep of ~64 ns and a read) before a solve gives up
+    int wait_limit = 1 << 21;    // barrier polls (back-to-back acquire loads of the barrier word) before a solve gives up
     bool stall_next = false;     // test hook: the next solve's first barrier never completes
     int launch_persistent();
     void destroy();

@@ -246,7 +246,8 @@ class Solver(_Handle):
         return rc
 
     def set_wait_limit(self, polls: int):
-        """Bound (in ~64 ns polls) on each grid-barrier wait of a one-launch solve."""
+        """Bound on each grid-barrier wait of a one-launch solve, in polls (back-to-back acquire
+        loads of the barrier word, no sleep between them)."""
         _check(lib().fiim_solver_set_wait_limit(self._h, C.c_int(polls)))
 
     def test_stall(self):

@@ -34,7 +34,8 @@ extern "C" {
 #define FIIM_ECUDA (-2)     /* a CUDA runtime call failed; see fiim_last_error() */
 #define FIIM_ENOMEM (-3)    /* device allocation failed */
 #define FIIM_ENODEV (-4)    /* no CUDA device, or the device is not sm_100 */
-#define FIIM_ETIMEOUT (-5)  /* the solve did not finish within the host-side iteration guard */
+#define FIIM_ETIMEOUT (-5)  /* the solve did not finish in time: the host-side iteration guard, or a
+                               bounded device-side wait (grid barrier, bulk copy) that ran out */
 
 /* ---- solver variants: whose control flow is reproduced --------------------- */
 #define FIIM_AFIIM 0  /* AFIIM/src/bicgstab.cpp:87-297: maxmsteps = min(max(n,500)/50, 20)      */
@@ -171,8 +172,8 @@ int fiim_solver_kernel_times_seq(fiim_solver_t s, int reps, int max_kernels, dou
  * most 65,536 rows). */
 int fiim_solver_mode(fiim_solver_t s);
 
-/* Bound on each grid-barrier wait of a one-launch solve, in polls (each a ~64 ns sleep and a
- * read; default 2^21, one to two seconds). A wait that runs out ends the solve with
+/* Bound on each grid-barrier wait of a one-launch solve, in polls (back-to-back acquire loads
+ * of the barrier word, no sleep between them; default 2^21, about one to two seconds). A wait that runs out ends the solve with
  * FIIM_ETIMEOUT; the context stays usable. */
 int fiim_solver_set_wait_limit(fiim_solver_t s, int polls);
 
@@ -261,7 +262,9 @@ int fiim_prec_apply(int n, const int *Gi, const int *Gj, const double *Gv, const
  * loads the library's device code keeps until the process exits; n above 1,048,576 rows
  * returns FIIM_EARG. The first call on each device looks up that array's device address
  * (with the device current) and keeps it; make that first call before any stream
- * capture. All calls on a device share the array, so calls that overlap on the GPU race
+ * capture. The kept address belongs to the device's current context: after a
+ * cudaDeviceReset of that device, do not call this entry point there again in the same
+ * process (the array may be placed elsewhere in the new context). All calls on a device share the array, so calls that overlap on the GPU race
  * on it; each call overwrites all n entries it reads. Arrays and stream as for
  * fiim_prec_apply. */
 int fiim_prec_apply_noalloc(int n, const int *Gi, const int *Gj, const double *Gv,

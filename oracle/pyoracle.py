@@ -16,6 +16,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
+# The reference tree: FIIM_REFERENCE, else a checkout named `reference` beside this repository.
+REFERENCE = os.environ.get("FIIM_REFERENCE",
+                           os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -26,12 +29,9 @@ _libs: dict[str, C.CDLL] = {}
 def build(ref: bool = True) -> None:
     """Compile the restatement (always) and, when the reference tree exists, oracle/_ref."""
     targets = ["restatement"]
-    if ref and os.path.isdir(os.environ.get("FIIM_REFERENCE", "/root/reference")):
-        targets.append("ref")
-    env = dict(os.environ)
-    if "FIIM_REFERENCE" in env:
-        targets.append("REF=" + env["FIIM_REFERENCE"])
-    subprocess.run(["make", "-s", "-C", HERE, *targets], check=True, env=env)
+    if ref and os.path.isdir(REFERENCE):
+        targets += ["ref", "REF=" + REFERENCE]
+    subprocess.run(["make", "-s", "-C", HERE, *targets], check=True)
 
 
 def have_ref(pkg: str = "afiim") -> bool:
@@ -267,3 +267,41 @@ def ref_solve(variant, A, b, F, tol=1e-8, nmax=500, x0=None, issym=False, mode="
     else:
         raise ValueError(variant)
     return x, resval.value, it.value, info.value
+
+
+class RefPdfiimSystem:
+    """The reference's PDFIIM system held as its own sparseMatrix objects and std::vectors
+    (built once), so that each run() times the reference's EPBiCGSTAB call by itself
+    (PDFIIM/src/bicgstab.cpp:80-310), without marshalling the arrays into it."""
+
+    def __init__(self, A, F, issym=False):
+        lib = _lib("pdfiim")
+        lib.ref_pdfiim_prepare.restype = C.c_void_p
+        lib.ref_pdfiim_run.restype = C.c_double
+        self._lib = lib
+        self._keep = [_d(A[2]), _i(A[1]), _i(A[0]), _d(F["Gv"]), _i(F["Gj"]), _i(F["Gi"]), _d(F["IDv"])]
+        if issym:
+            self._keep += [np.zeros(1), np.zeros(1, np.int32), np.zeros(1, np.int32)]
+        else:
+            self._keep += [_d(F["Hv"]), _i(F["Hj"]), _i(F["Hi"])]
+        self.n = len(self._keep[2]) - 1
+        self._h = lib.ref_pdfiim_prepare(C.c_int(self.n), C.c_int(int(issym)), *[a.ctypes for a in self._keep])
+
+    def run(self, b, tol=1e-8, nmax=1200, x0=None):
+        """One EPBiCGSTAB call. Returns (x, resval, iter, info, seconds inside the call)."""
+        x = np.zeros(self.n) if x0 is None else _d(x0).copy()
+        resval, it, info = C.c_double(0), C.c_int(0), C.c_int(-1)
+        secs = self._lib.ref_pdfiim_run(C.c_void_p(self._h), _d(b).ctypes, x.ctypes, C.c_double(tol),
+                                        C.c_int(nmax), C.byref(resval), C.byref(it), C.byref(info))
+        return x, resval.value, it.value, info.value, secs
+
+    def close(self):
+        if self._h:
+            self._lib.ref_pdfiim_release(C.c_void_p(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -9,6 +9,7 @@
 //   -DREF_ACIFIM : acifim (ACIFIM/src/prec.hpp:126-151) + PBiCGSTAB (ACIFIM/src/bicgstab.hpp:94-120)
 // Each package becomes its own shared object (oracle/_ref/libref_<pkg>.so).
 
+#include <chrono>
 #include <cstring>
 #include <cstdlib>
 #include <string>
@@ -220,6 +221,43 @@ void ref_pdfiim_solve(int n, int issym, double *Av, int *Aj, int *Ai, double *b,
     EPBiCGSTAB(A, B, tol, NMAX, G, ID, H, X, resval, iter, verbose, info);
     std::memcpy(x, X.data(), sizeof(double) * n);
 }
+
+// A caller of the reference holds its system as sparseMatrix objects and std::vectors for
+// as long as it solves. For timing the reference's call alone, the objects are built once
+// here (ref_pdfiim_prepare) and each ref_pdfiim_run times EPBiCGSTAB by itself
+// (PDFIIM/src/bicgstab.cpp:80-310): copying b and x in and out lies outside the clock.
+struct PdfiimSystem {
+    sparseMatrix<int, int, double> A, G, H;
+    std::vector<double> B, ID, X;
+};
+
+void *ref_pdfiim_prepare(int n, int issym, double *Av, int *Aj, int *Ai, double *Gv, int *Gj,
+                         int *Gi, double *IDv, double *Hv, int *Hj, int *Hi) {
+    auto *s = new PdfiimSystem;
+    to_sparse(n, Ai[n], Av, Aj, Ai, issym ? SYMMETRIC : GENERAL, s->A);
+    to_sparse(n, Gi[n], Gv, Gj, Gi, UPPERTRI, s->G);
+    if (!issym) to_sparse(n, Hi[n], Hv, Hj, Hi, LOWERTRI, s->H);
+    s->ID.assign(IDv, IDv + n);
+    s->B.assign(n, 0.0);
+    s->X.assign(n, 0.0);
+    return s;
+}
+
+// Returns the seconds spent inside EPBiCGSTAB (steady clock).
+double ref_pdfiim_run(void *h, const double *b, double *x, double tol, int NMAX, double *resval,
+                      int *iter, int *info) {
+    auto *s = static_cast<PdfiimSystem *>(h);
+    const size_t n = s->B.size();
+    std::memcpy(s->B.data(), b, sizeof(double) * n);
+    std::memcpy(s->X.data(), x, sizeof(double) * n);
+    const auto t0 = std::chrono::steady_clock::now();
+    EPBiCGSTAB(s->A, s->B, tol, NMAX, s->G, s->ID, s->H, s->X, resval, iter, 0, info);
+    const auto t1 = std::chrono::steady_clock::now();
+    std::memcpy(x, s->X.data(), sizeof(double) * n);
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+void ref_pdfiim_release(void *h) { delete static_cast<PdfiimSystem *>(h); }
 #endif
 
 }  // extern "C"

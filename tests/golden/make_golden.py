@@ -97,7 +97,7 @@ def save(name, arrays, meta):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("FIIM_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=os.environ.get("FIIM_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference")))
     args = ap.parse_args()
     for pkg in ("afiim", "pdfiim", "acifim"):
         O.set_threads(1, pkg)

@@ -73,7 +73,7 @@ def check_batch(systems, variant, precision, nmax=2000, extra=None):
         xo, info, lo, hi, spread = envelope(variant, A, bk, rounded(F, precision), nmax, **(extra or {}))
         it = int(res["iter"][k])
         print(f"{variant}/{precision} system {k} n={len(bk)}: gpu iter {it} info {res['info'][k]} | "
-              f"oracle envelope [{lo},{hi}] info {info} | x diff {np.linalg.norm(xk - xo) / np.linalg.norm(xo):.2e}")
+              f"oracle envelope [{lo},{hi}] info {info} | x diff {np.linalg.norm(xk - xo) / max(np.linalg.norm(xo), 1e-300):.2e}")
         assert res["info"][k] == info
         assert lo - 2 <= it <= hi + 2
         if info == 0:

@@ -10,7 +10,7 @@ import fiim_b200 as FB
 import pyoracle as O
 from conftest import load_golden
 
-REFERENCE = os.environ.get("FIIM_REFERENCE", "/root/reference")   # the reference tree, where present
+REFERENCE = O.REFERENCE   # the reference tree, where present
 REF_SHERMAN2 = os.path.join(REFERENCE, "AFIIM/example/sherman2.mtx")
 REF_SHERMAN2_RHS = os.path.join(REFERENCE, "AFIIM/example/sherman2_rhs1.mtx")
 
