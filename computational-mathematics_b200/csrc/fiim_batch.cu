@@ -277,6 +277,7 @@ struct BatchSolver : SolverBase {
         g.alpha_guard = (opt.variant == FIIM_ACIFIM);
         g.active = nsys;
         g.loops = 0;
+        g.loops_total = 0;
         *hg = g;
         FIIM_CUDA(cudaMemcpyAsync(bs.g, hg, sizeof(bt::BGlobal), cudaMemcpyHostToDevice, stream));
         FIIM_CUDA(cudaMemsetAsync(bs.done, 0, sizeof(int) * nsys, stream));
@@ -333,6 +334,29 @@ struct BatchSolver : SolverBase {
         return FIIM_OK;
     }
 
+    // The loop until no system is active: the WHILE graph, or (FIIM_GRAPH=host) a one-body
+    // graph relaunched by the host.
+    int run_loop(int nmax) {
+        if (!host_loop) {
+            FIIM_CUDA(cudaGraphLaunch(exec, stream));
+            return FIIM_OK;
+        }
+        int launched = 0, chunk = 1;
+        for (;;) {
+            for (int q = 0; q < chunk; ++q) FIIM_CUDA(cudaGraphLaunch(exec, stream));
+            launched += chunk;
+            FIIM_CUDA(cudaMemcpyAsync(hg, bs.g, sizeof(bt::BGlobal), cudaMemcpyDeviceToHost, stream));
+            FIIM_CUDA(cudaStreamSynchronize(stream));
+            if (hg->active <= 0) break;
+            if (launched > std::max(nmax, 0) + 2)
+                return set_error(FIIM_ETIMEOUT, "batch not finished after %d iterations", launched);
+            chunk = std::min(chunk * 2, 16);
+        }
+        hg->loops = launched;
+        FIIM_CUDA(cudaMemcpyAsync(&bs.g->loops, &hg->loops, sizeof(int), cudaMemcpyHostToDevice, stream));
+        return FIIM_OK;
+    }
+
     int solve(const double *b_in, double *x_io, double tol, int nmax, int *iter, int *info, double *resval,
               double *true_relres, fiim_result *summary) {
         FIIM_CUDA(cudaSetDevice(device));
@@ -344,25 +368,29 @@ struct BatchSolver : SolverBase {
         FIIM_TRY(reset_state(tol, nmax));
         FIIM_CUDA(spmv(A, A.M.v, x, bt::BEpiInit{b, p, r0, r}));
         FIIM_CUDA(finish<1>(A, bt::BEpiInit{b, p, r0, r}));
-        if (!host_loop) {
-            FIIM_CUDA(cudaGraphLaunch(exec, stream));
-        } else {
-            int launched = 0, chunk = 1;
-            for (;;) {
-                for (int q = 0; q < chunk; ++q) FIIM_CUDA(cudaGraphLaunch(exec, stream));
-                launched += chunk;
-                FIIM_CUDA(cudaMemcpyAsync(hg, bs.g, sizeof(bt::BGlobal), cudaMemcpyDeviceToHost, stream));
-                FIIM_CUDA(cudaStreamSynchronize(stream));
-                if (hg->active <= 0) break;
-                if (launched > std::max(nmax, 0) + 2)
-                    return set_error(FIIM_ETIMEOUT, "batch not finished after %d iterations", launched);
-                chunk = std::min(chunk * 2, 16);
-            }
-            hg->loops = launched;
-            FIIM_CUDA(cudaMemcpyAsync(&bs.g->loops, &hg->loops, sizeof(int), cudaMemcpyHostToDevice, stream));
-        }
+        FIIM_TRY(run_loop(nmax));
         FIIM_CUDA(spmv(A, A.M.v, x, bt::BEpiResid{b}));
         FIIM_CUDA((finish<2, false>(A, bt::BEpiResid{b})));
+        // Verified: systems whose FP64 true residual misses the target restart from their
+        // current x (the others stay finished), until none misses or the rounds run out.
+        int rounds = 0, extra = 0;   // restart rounds; launches outside the loop bodies
+        while (opt.verified && rounds < opt.max_restarts) {
+            ++extra;
+            bt::k_bverify<<<std::max(1, std::min((nsys + kThreads - 1) / kThreads, num_sms())), kThreads, 0, stream>>>(
+                nsys, bs);
+            FIIM_CUDA(cudaGetLastError());
+            FIIM_CUDA(cudaMemcpyAsync(hg, bs.g, sizeof(bt::BGlobal), cudaMemcpyDeviceToHost, stream));
+            FIIM_CUDA(cudaStreamSynchronize(stream));
+            if (hg->active < 0) return set_error(FIIM_ETIMEOUT, "device loop guard tripped");
+            if (hg->active == 0) break;
+            ++rounds;
+            extra += 4;
+            FIIM_CUDA(spmv(A, A.M.v, x, bt::BEpiRestart{{b, p, r0, r}}));
+            FIIM_CUDA(finish<1>(A, bt::BEpiRestart{{b, p, r0, r}}));
+            FIIM_TRY(run_loop(nmax));
+            FIIM_CUDA(spmv(A, A.M.v, x, bt::BEpiResid{b}));
+            FIIM_CUDA((finish<2, false>(A, bt::BEpiResid{b})));
+        }
         FIIM_CUDA(cudaMemcpyAsync(x_io, x, sizeof(double) * N, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                                   stream));
         FIIM_CUDA(cudaEventRecord(ev1, stream));
@@ -396,9 +424,9 @@ struct BatchSolver : SolverBase {
             summary->info = worst;
             summary->resval = 0.0;
             summary->true_relres = worst_rel;
-            summary->refine_steps = 0;
+            summary->refine_steps = rounds;
             summary->device_ms = ms;
-            summary->launches = 4 + hg->loops * 14;
+            summary->launches = 4 + extra + (hg->loops_total + hg->loops) * 14;
         }
         return FIIM_OK;
     }

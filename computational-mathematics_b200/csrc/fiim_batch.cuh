@@ -19,6 +19,7 @@ namespace bt {
 struct BGlobal {
     double tol, eps;
     int nmax, alpha_guard, active, loops;
+    int loops_total;   // verified solves: loop bodies of the runs before the current one
 };
 
 // Finished-system flags per row block of one matrix (batched solve; NULL elsewhere):
@@ -59,6 +60,45 @@ struct BFinInit {   // ro = ||r0||, m1 = ro^2, rc = ro (AFIIM/src/bicgstab.cpp:1
         if (bs.g->nmax <= 0) retire(bs, k, bs.g->nmax == 0 ? 3 : -1);
     }
 };
+// Verified solves: a system re-enters the loop from its current x. As at the start,
+// r = r0 = p = b - A x and rc = ||r||, m1 = rc^2 (AFIIM/src/bicgstab.cpp:161-165), and the
+// stagnation and divergence counters restart; ro (the test's reference norm, ||b - A x0||)
+// and the iteration count carry on.
+struct BFinRestart {
+    __device__ void finish(BState &bs, int k, const double *t) const {
+        bs.rc[k] = sqrt(t[0]);
+        bs.m1[k] = bs.rc[k] * bs.rc[k];
+        bs.stag[k] = 0;
+        bs.msteps[k] = 0;
+    }
+};
+
+// Verified solves: the FP64 true residual ||b - A x|| (ts, from BEpiResid) of a system that
+// left the loop converged (info 0) must be below tol * ro, the reference's test applied to
+// the true residual in place of the recurrence one. A system that misses it is marked
+// running again (its row blocks unflagged) and counted in active; the runs' loop counts are
+// folded into loops_total.
+__device__ __forceinline__ bool verify_misses(const BState &bs, int k) {
+    if (bs.info[k] != 0 || bs.ts[k] == 0.0) return false;
+    return !(sqrt(bs.ts[k]) < bs.g->tol * bs.ro[k]);
+}
+
+static __global__ void __launch_bounds__(kThreads) k_bverify(int nsys, BState bs) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        bs.g->loops_total += bs.g->loops;
+        bs.g->loops = 0;
+    }
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nsys; k += gridDim.x * blockDim.x) {
+        if (!verify_misses(bs, k)) continue;
+        bs.done[k] = 0;
+        bs.info[k] = -1;
+        for (int m = 0; m < 3; ++m)
+            if (bs.bf[m].flag)
+                for (int b = bs.bf[m].sys_blk[k]; b < bs.bf[m].sys_blk[k + 1]; ++b) bs.bf[m].flag[b] = 0;
+        atomicAdd(&bs.g->active, 1);
+    }
+}
+
 struct BFinS {
     __device__ void finish(BState &bs, int k, const double *t) const {
         bs.r2[k] = t[0];
@@ -150,6 +190,9 @@ struct BEpiInit {
         red[0] += pi * pi;
     }
     __device__ void finish(BState &bs, int k, const double *t) const { BFinInit{}.finish(bs, k, t); }
+};
+struct BEpiRestart : BEpiInit {
+    __device__ void finish(BState &bs, int k, const double *t) const { BFinRestart{}.finish(bs, k, t); }
 };
 struct BEpiResid {
     FIIM_EPI(2, true, false);

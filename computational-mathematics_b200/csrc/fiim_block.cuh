@@ -144,6 +144,9 @@ struct KEpiInit {
     }
     __device__ void finish(BState &bs, int j, const double *t) const { bt::BFinInit{}.finish(bs, j, t); }
 };
+struct KEpiRestart : KEpiInit {
+    __device__ void finish(BState &bs, int j, const double *t) const { bt::BFinRestart{}.finish(bs, j, t); }
+};
 struct KEpiResid {
     FIIM_BEPI(2, true, false);
     const double *__restrict__ b;

@@ -203,6 +203,8 @@ void fiim_options_default(fiim_options *o) {
     o->inner_tol = 1e-5;
     o->inner_nmax = 1000;
     o->max_refine = 50;
+    o->verified = 0;
+    o->max_restarts = 4;
 }
 
 int fiim_EPBiCGSTAB_afiim(int n, double *Av, int *Aj, int *Ai, double *b, double tol, int NMAX,

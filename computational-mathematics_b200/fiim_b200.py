@@ -48,6 +48,7 @@ EXPORTS = (
     "fiim_spmv", "fiim_prec_apply", "fiim_prec_apply_noalloc",
     "fiim_gen_poisson2d", "fiim_gen_convdiff3d", "fiim_gen_convdiff2d", "fiim_gen_batch_params",
     "fiim_gen_zipf", "fiim_gen_zipf_mean", "fiim_rand_normal", "fiim_model_rhs", "fiim_pdfiim_build", "fiim_pdfiim_build_gpu",
+    "fiim_acifim_build",
     "fiim_read_mtx", "fiim_read_rhs", "fiim_factors_save", "fiim_factors_load",
     "fiim_dist_unique_id", "fiim_dist_partition", "fiim_dist_plan", "fiim_dist_create", "fiim_dist_solve",
     "fiim_dist_destroy", "fiim_dist_emulate",
@@ -63,7 +64,8 @@ class FiimError(RuntimeError):
 class Options(C.Structure):
     _fields_ = [("variant", C.c_int), ("issym", C.c_int), ("precision", C.c_int), ("memory", C.c_int),
                 ("mode", C.c_char), ("nr", C.c_int), ("autotune", C.c_int), ("verbose", C.c_int),
-                ("inner_tol", C.c_double), ("inner_nmax", C.c_int), ("max_refine", C.c_int)]
+                ("inner_tol", C.c_double), ("inner_nmax", C.c_int), ("max_refine", C.c_int),
+                ("verified", C.c_int), ("max_restarts", C.c_int)]
 
 
 class Result(C.Structure):
@@ -447,9 +449,13 @@ class BatchSolver(_Handle):
     systems: list of (A, F) with A = (Ai, Aj, Av) and F = {Gi, Gj, Gv, IDv, Hi, Hj, Hv}.
     precision: 'fp64' | 'fp32' | 'bf16' storage of G and H.
     memory: 'host' (numpy b, x) or 'device' (the concatenated arrays are uploaded here; b, x
-    are torch CUDA tensors)."""
+    are torch CUDA tensors).
+    verified: a system that passes the reference's recurrence test must also have an FP64
+    true residual below tol * ||b - A x0||, else it restarts from its current x (at most
+    max_restarts rounds); off, the loop stops as the reference's does."""
 
-    def __init__(self, systems, variant="acifim", precision="fp64", memory="host"):
+    def __init__(self, systems, variant="acifim", precision="fp64", memory="host", verified=False,
+                 max_restarts=4):
         A, sys_rows = block_diag([s[0] for s in systems])
         G, _ = block_diag([(s[1]["Gi"], s[1]["Gj"], s[1]["Gv"]) for s in systems])
         H, _ = block_diag([(s[1]["Hi"], s[1]["Hj"], s[1]["Hv"]) for s in systems])
@@ -461,6 +467,8 @@ class BatchSolver(_Handle):
         o.variant = _VARIANTS[variant]
         o.precision = _PRECISIONS[precision]
         o.memory = MEM_DEVICE if memory == "device" else MEM_HOST
+        o.verified = int(verified)
+        o.max_restarts = max_restarts
         self._h = C.c_void_p(0)
         arrs = [_i(A[0]), _i(A[1]), _d(A[2]), _i(G[0]), _i(G[1]), _d(G[2]), _d(D), _i(H[0]), _i(H[1]), _d(H[2])]
         if memory == "device":
@@ -496,14 +504,18 @@ class BatchSolver(_Handle):
 
 class BlockSolver(_Handle):
     """k <= 32 right-hand sides of one system, sharing the sparse products (fiim_block_*).
-    B, X: n x k row-major FP64 (numpy, or torch CUDA tensors with memory='device')."""
+    B, X: n x k row-major FP64 (numpy, or torch CUDA tensors with memory='device').
+    verified: as for BatchSolver, per right-hand side."""
 
-    def __init__(self, A, F, nrhs, variant="afiim", precision="fp64", memory="host"):
+    def __init__(self, A, F, nrhs, variant="afiim", precision="fp64", memory="host", verified=False,
+                 max_restarts=4):
         o = Options()
         lib().fiim_options_default(C.byref(o))
         o.variant = _VARIANTS[variant]
         o.precision = _PRECISIONS[precision]
         o.memory = MEM_DEVICE if memory == "device" else MEM_HOST
+        o.verified = int(verified)
+        o.max_restarts = max_restarts
         self.memory, self.k, self.n = memory, nrhs, len(A[0]) - 1
         conv = (lambda a, ints: a) if memory == "device" else (lambda a, ints: _i(a) if ints else _d(a))
         arrs = [conv(A[0], 1), conv(A[1], 1), conv(A[2], 0), conv(F["Gi"], 1), conv(F["Gj"], 1), conv(F["Gv"], 0),
@@ -657,6 +669,31 @@ def pdfiim_build(A, ftol, prefill=1, lfill=1, postfill=1, warpsize=-1, filttype=
          "Hi": np.zeros(n + 1, np.int32)}
     _check(fn(*args, C.byref(ng), C.byref(nh), _ptr(F["Gv"]), _ptr(F["Gj"]), _ptr(F["Gi"]),
                                _ptr(F["IDv"]), _ptr(F["Hv"]), _ptr(F["Hj"]), _ptr(F["Hi"])))
+    return F
+
+
+def acifim_build(A, dtol1, dtol2, elem_per_rowcol=30, growth=5, eta=0.0, shift=0.0, coeff=2.0,
+                 element_limit=200, filtit=30, with_lu=False):
+    """ACIFIM construction on the host (the same factors as ACIFIM/src/prec.cpp:127-1052; the
+    defaults are the example driver's, ACIFIM/example/example.cpp:42-47). Returns a factor
+    dict (with Li.., Ui.. when with_lu). Raises FiimError when the construction fails (a NaN
+    Schur complement, where the reference returns 1). Safe to call from several threads."""
+    Ai, Aj, Av = _i(A[0]), _i(A[1]), _d(A[2])
+    n = len(Ai) - 1
+    nnz = np.zeros(4, np.int32)
+    L = lib()
+    args = (C.c_int(n), _ptr(Ai), _ptr(Aj), _ptr(Av), C.c_double(dtol1), C.c_double(dtol2), C.c_int(elem_per_rowcol),
+            C.c_int(growth), C.c_double(eta), C.c_double(shift), C.c_double(coeff), C.c_int(element_limit),
+            C.c_int(filtit), _ptr(nnz))
+    _check(L.fiim_acifim_build(*args, *([None] * 13)))
+    ng, nh, nl, nu = (int(v) for v in nnz)
+    F = {"Gv": np.zeros(ng), "Gj": np.zeros(ng, np.int32), "Gi": np.zeros(n + 1, np.int32), "IDv": np.zeros(n),
+         "Hv": np.zeros(nh), "Hj": np.zeros(nh, np.int32), "Hi": np.zeros(n + 1, np.int32)}
+    if with_lu:
+        F.update({"Lv": np.zeros(nl), "Lj": np.zeros(nl, np.int32), "Li": np.zeros(n + 1, np.int32),
+                  "Uv": np.zeros(nu), "Uj": np.zeros(nu, np.int32), "Ui": np.zeros(n + 1, np.int32)})
+    keys = ("Gv", "Gj", "Gi", "IDv", "Hv", "Hj", "Hi", "Lv", "Lj", "Li", "Uv", "Uj", "Ui")
+    _check(L.fiim_acifim_build(*args, *[_ptr(F.get(k)) for k in keys]))
     return F
 
 

@@ -108,9 +108,15 @@ typedef struct {
     double inner_tol;  /* mixed: inner FP32 BiCGSTAB relative tolerance (default 1e-5)     */
     int inner_nmax;    /* mixed: inner iteration cap per refinement step (default 1000)    */
     int max_refine;    /* mixed: outer refinement steps cap (default 50)                   */
+    int verified;      /* batched and block solves: 1 = a system (right-hand side) that     */
+                       /* passes the reference's recurrence test must also have an FP64    */
+                       /* true residual ||b - A x|| below tol * ||b - A x0||, or it restarts */
+                       /* BiCGSTAB from its current x (masked, the others stay finished);   */
+                       /* 0 (default): the recurrence test alone, as the reference stops    */
+    int max_restarts;  /* verified: restart rounds cap (default 4)                         */
 } fiim_options;
 
-/* Defaults: FIIM_AFIIM, FP64, host memory, mode 'E', nr 1, autotune 0. */
+/* Defaults: FIIM_AFIIM, FP64, host memory, mode 'E', nr 1, autotune 0, verified 0. */
 void fiim_options_default(fiim_options *opt);
 
 typedef struct {
@@ -207,7 +213,11 @@ int fiim_batch_create(fiim_batch_t *out, int nsys, const int *sys_rows, const in
 
 /* Solves every system. Per-system outputs (host arrays of nsys, any may be NULL): iter,
  * info (reference codes), resval (rc/ro, lagged as in the reference) and the FP64 true
- * residual ||b_k - A_k x_k|| / ||b_k||. summary: max iterations, worst info, device time. */
+ * residual ||b_k - A_k x_k|| / ||b_k||. summary: max iterations, worst info, device time,
+ * and in refine_steps the restart rounds of a verified solve (opt->verified). With
+ * opt->verified, a system's iter counts the iterations of all its runs, and a system that
+ * still misses the FP64 target after max_restarts rounds keeps info 0 and reports its
+ * true residual. */
 int fiim_batch_solve(fiim_batch_t s, const double *b, double *x, double tol, int NMAX,
                      int *iter, int *info, double *resval, double *true_relres,
                      fiim_result *summary);
@@ -308,6 +318,21 @@ int fiim_pdfiim_build_gpu(int n, const int *Ai, const int *Aj, const double *Av,
                           int lfill, int postfill, double ftol, int warpsize, char filttype,
                           char patt, int *nnzG, int *nnzH, double *Gv, int *Gj, int *Gi,
                           double *D, double *Hv, int *Hj, int *Hi);
+
+/* ACIFIM factor construction on the host: the same G, D^{-1}, H, L and U as acifim
+ * (ACIFIM/src/prec.cpp:127-1052, arguments as there; the example driver passes
+ * elemPerRowCol 30, growth 5, eta 0, shift 0, coeff 2, element_limit 200, filtit 30,
+ * ACIFIM/example/example.cpp:42-47), bit for bit. elemPerRowCol and growth only size the
+ * reference's buffers and do not change the result. Two calls: the first, with Gv == NULL,
+ * builds and returns nnz[0..3] = nnz(G), nnz(H), nnz(L), nnz(U), keeping the result in a
+ * buffer bound to the calling thread (so threads may build different systems at once);
+ * the second copies it out (L and U are skipped when their pointers are NULL). A NaN
+ * Schur complement, where the reference's acifim returns 1, returns FIIM_EARG. */
+int fiim_acifim_build(int n, const int *Ai, const int *Aj, const double *Av, double dtol1,
+                      double dtol2, int elemPerRowCol, int growth, double eta, double shift,
+                      double coeff, int element_limit, int filtit, int *nnz, double *Gv, int *Gj,
+                      int *Gi, double *IDv, double *Hv, int *Hj, int *Hi, double *Lv, int *Lj,
+                      int *Li, double *Uv, int *Uj, int *Ui);
 
 /* ===========================================================================
  * Row-partitioned solve of one system over several GPUs (one process per GPU).

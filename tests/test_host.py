@@ -13,7 +13,8 @@ import pytest
 
 import fiim_b200 as FB
 import pyoracle as O
-from conftest import ROOT
+from conftest import ROOT, sub
+import scipy.sparse as sp
 
 HEADER = os.path.join(ROOT, "include", "fiim_b200.h")
 
@@ -282,3 +283,95 @@ def test_handles_close_on_leaving_a_with_block():
         with Probe():
             raise ValueError("inside")
     assert Probe.closed == 2
+
+
+ACIFIM_KEYS = ("Gi", "Gj", "Gv", "IDv", "Hi", "Hj", "Hv", "Li", "Lj", "Lv", "Ui", "Uj", "Uv")
+
+
+def _same_factors(F, R):
+    for k in ACIFIM_KEYS:
+        assert F[k].dtype == np.asarray(R[k]).dtype and np.array_equal(F[k], R[k]), k
+
+
+@pytest.mark.parametrize("name,prefix,dtols", [("convdiff2d48_acifim", "", (0.1, 0.05)),
+                                               ("sherman2", "acifim_", (0.01, 0.01))])
+def test_host_acifim_matches_golden_factors(golden, name, prefix, dtols):
+    """The library's ACIFIM construction against the factors the reference built for the
+    committed fixtures (ACIFIM/src/prec.cpp:127-1052), all five factors bit for bit."""
+    g = golden(name)
+    F = FB.acifim_build((g["Ai"], g["Aj"], g["Av"]), *dtols, with_lu=True)
+    _same_factors(F, sub(g, prefix))
+
+
+def _random_system(n, seed, zero_diag=0):
+    rng = np.random.default_rng(seed)
+    rows, cols = [], []
+    for i in range(n):
+        k = int(rng.integers(1, 9))
+        c = rng.choice(n, k, replace=False)
+        rows.append(np.full(k + 1, i))
+        cols.append(np.concatenate([c, [i]]))
+    M = sp.csr_matrix((rng.uniform(-1, 1, sum(len(c) for c in cols)), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(n, n))
+    M.sum_duplicates()
+    M = M + sp.diags(np.abs(M).sum(axis=1).A1 * 1.2)
+    M = M.tocsr()
+    M.sort_indices()
+    if zero_diag:
+        for i in rng.choice(n, zero_diag, replace=False):
+            M[i, i] = 0.0
+    M.sort_indices()
+    return M.indptr.astype(np.int32), M.indices.astype(np.int32), M.data.copy()
+
+
+@pytest.mark.skipif(not O.have_ref("acifim"), reason="oracle/_ref not built")
+@pytest.mark.parametrize("case", [
+    dict(system="convdiff", k=3, dtols=(0.1, 0.05)),
+    dict(system="convdiff", k=6, dtols=(0.1, 0.05)),
+    dict(system="convdiff", k=9, dtols=(0.02, 0.01), element_limit=4, filtit=6, coeff=1.5),
+    dict(system="random", seed=1, dtols=(0.1, 0.05)),
+    dict(system="random", seed=2, dtols=(0.01, 0.005), element_limit=3, filtit=30, coeff=2.0),
+    dict(system="random", seed=3, dtols=(0.05, 0.05), shift=0.2, eta=0.5),
+    dict(system="random", seed=4, dtols=(0.1, 0.05), zero_diag=40),
+    dict(system="single", dtols=(0.1, 0.05)),
+])
+def test_host_acifim_matches_live_reference(case):
+    """Against the reference's own acifim, compiled here, on 2D convection-diffusion systems of
+    the batched benchmark's family, random nonsymmetric systems (repeated filter passes with
+    a small element limit, shift and eta, rows whose diagonal is zero) and a 1 x 1 system."""
+    case = dict(case)
+    system, dtols = case.pop("system"), case.pop("dtols")
+    if system == "convdiff":
+        side, diff, theta, pe = FB.batch_params(20261203, case.pop("k"))
+        A = FB.gen_convdiff2d(side, diff, theta, pe)
+    elif system == "random":
+        A = _random_system(3000, case.pop("seed"), case.pop("zero_diag", 0))
+    else:
+        A = (np.array([0, 1], np.int32), np.array([0], np.int32), np.array([2.5]))
+    R, cerr = O.acifim_build(A, *dtols, **case)
+    assert cerr == 0
+    _same_factors(FB.acifim_build(A, *dtols, with_lu=True, **case), R)
+
+
+def test_host_acifim_threads_build_independent_systems():
+    """Each thread keeps its own result between the sizing and copy-out calls, so systems
+    built on a thread pool come out as built one by one."""
+    from concurrent.futures import ThreadPoolExecutor
+    systems = [FB.gen_convdiff2d(*[FB.batch_params(7, k)[0]] + list(FB.batch_params(7, k)[1:])) for k in range(12)]
+    one = [FB.acifim_build(A, 0.1, 0.05) for A in systems]
+    with ThreadPoolExecutor(6) as ex:
+        par = list(ex.map(lambda A: FB.acifim_build(A, 0.1, 0.05), systems))
+    for F, R in zip(par, one):
+        assert all(np.array_equal(F[k], R[k]) for k in R)
+
+
+def test_host_acifim_nan_pivot_fails():
+    """A NaN in A reaches a Schur complement: the reference's acifim returns 1 there, the
+    library returns FIIM_EARG."""
+    A = FB.gen_convdiff2d(8, 1.0, 0.3, 0.5)
+    Av = A[2].copy()
+    Av[5] = np.nan
+    with pytest.raises(FB.FiimError):
+        FB.acifim_build((A[0], A[1], Av), 0.1, 0.05)
+    if O.have_ref("acifim"):
+        assert O.acifim_build((A[0], A[1], Av), 0.1, 0.05)[1] == 1
