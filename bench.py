@@ -569,10 +569,14 @@ def run_partitioned(args, A, F, b, rank, ws, dist, dev):
 
 def run_batched(args, rank=0, world=1, dist=None):
     """256 independent 2D convection-diffusion systems (side U{32..256}, diffusion log-U[0.1,10],
-    random direction, cell Peclet <= 1), each with factors from the library's PDFIIM
-    construction, solved (a) in one batched launch with FP32 factor storage, (b) in one
-    batched launch with FP64 factors, and (c) one after another with the FP64 single-system
-    solver. Loop control: ACIFIM's (divergence window 40, non-finite-alpha guard)."""
+    random direction, cell Peclet <= 1), each with ACIFIM factors (eps1 0.1, eps2 0.05, the
+    example driver's other parameters) from the library's construction (the reference's
+    acifim, bit for bit; one system per host thread), solved (a) in one batched launch with
+    FP32 factor storage, (b) the same with FP64 factors, both FP64-verified, (c) FP32 factors
+    stopped on the reference's recurrence test alone, and (d) one after another with the FP64
+    single-system solver. Loop control: ACIFIM's (divergence window 40, non-finite-alpha
+    guard), mode 'E'."""
+    from concurrent.futures import ThreadPoolExecutor
     import torch
     import fiim_b200 as FB
     # Systems are independent: with N ranks each solves a contiguous, nnz-balanced shard
@@ -580,16 +584,23 @@ def run_batched(args, rank=0, world=1, dist=None):
     # max-over-ranks time.
     sides = [FB.batch_params(SEED, k)[0] for k in range(args.batch)]
     lo, hi = FB.shard_by_nnz([5 * s * s for s in sides], world, rank)
-    systems = []
-    for k in range(lo, hi):
+
+    def one(k):
         side, diff, theta, pe = FB.batch_params(SEED, k)
         A = FB.gen_convdiff2d(side, diff, theta, pe)
-        F = FB.pdfiim_build(A, **PDFIIM_PARAMS)
-        systems.append((A, F, FB.rand_normal(side * side, SEED + 10 + k)))
+        return A, FB.acifim_build(A, 0.1, 0.05), FB.rand_normal(side * side, SEED + 10 + k)
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        systems = list(ex.map(one, range(lo, hi)))
+    setup = time.perf_counter() - t0
     b = np.concatenate([s[2] for s in systems])
     N = len(b)
     out = {"systems": len(systems), "rows": N, "nnz": int(sum(int(s[0][0][-1]) for s in systems)),
-           "tol": 1e-8, "loop": "ACIFIM", "factors": "PDFIIM eps 0.05 (2,2,1), library construction",
+           "factor_nnz": int(sum(len(s[1]["Gv"]) + len(s[1]["Hv"]) for s in systems)),
+           "tol": 1e-8, "loop": "ACIFIM", "factors": "ACIFIM eps1 0.1 eps2 0.05, library construction "
+                                                     "(the reference's acifim bit for bit)",
+           "setup_s": round(setup, 2),
            "verified": "FP64 true residual of every system below tol (masked restarts from x)"}
     # Inputs resident in HBM, as for the headline value: b and x are device arrays.
     tb = torch.from_numpy(b).cuda()
@@ -643,10 +654,12 @@ def run_batched(args, rank=0, world=1, dist=None):
 def run_multi_rhs(args, rank=0, world=1, dist=None):
     """Random nonsymmetric n = 4,000,000 system with Zipf(2.0) row lengths (mean 16, cap 512),
     uniform columns plus the diagonal, off-diagonals U(-1,1), diagonal 1.1 x the absolute row
-    sum; 32 right-hand sides N(0,1). Factors: the library's PDFIIM construction, eps 0.1
-    (prefill 1, lfill 1, postfill 1, warpsize 32), stored FP32 for the block solve. AFIIM
-    loop, tol 1e-8. Compared with the same 32 right-hand sides solved one after another by
-    the FP64 single-system solver.
+    sum; 32 right-hand sides N(0,1). Factors: AFIIM eps 0.1 (the example driver's other
+    parameters) from the library's construction (the reference's afiim bit for bit; sequential
+    in the rows, about two minutes at 4M on one host core), stored FP32 for the block solve;
+    --mrhs-factors pdfiim uses the library's PDFIIM eps 0.1 (1,1,1), warpsize 32 instead
+    (seconds). AFIIM loop, tol 1e-8, FP64-verified. Compared with the same 32 right-hand sides
+    solved one after another by the FP64 single-system solver.
 
     With N ranks the right-hand sides are sharded: each rank holds the matrix and factors
     and solves a contiguous share of the 32 columns as one block (no exchange on the data
@@ -659,7 +672,12 @@ def run_multi_rhs(args, rank=0, world=1, dist=None):
     t0 = time.perf_counter()
     scale = FB.zipf_scale(n, sample=min(n, 200000))
     A = FB.gen_zipf(n, scale)
-    F = FB.pdfiim_build(A, 0.1, 1, 1, 1, 32, "I", "B")
+    if args.mrhs_factors == "afiim":
+        F = FB.afiim_build(A, 0.1)
+        fdesc = "AFIIM eps 0.1, library construction (the reference's afiim bit for bit)"
+    else:
+        F = FB.pdfiim_build(A, 0.1, 1, 1, 1, 32, "I", "B")
+        fdesc = "PDFIIM eps 0.1 (1,1,1) warpsize 32, library construction"
     B = (np.stack([FB.rand_normal(n, SEED + 100 + j) for j in range(lo, hi)], axis=1).copy() if kr > 0
          else np.zeros((n, 0)))
     setup = time.perf_counter() - t0
@@ -669,7 +687,7 @@ def run_multi_rhs(args, rank=0, world=1, dist=None):
     tB = torch.from_numpy(B).to(dev)
     tX = torch.zeros_like(tB)
     out = {"n": n, "nnz": int(A[0][-1]), "rhs": k, "zipf_scale": round(scale, 4), "tol": 1e-8, "loop": "AFIIM",
-           "factors": "PDFIIM eps 0.1 (1,1,1) warpsize 32, library construction", "setup_s": round(setup, 1)}
+           "factors": fdesc, "factor_nnz": int(len(F["Gv"]) + len(F["Hv"])), "setup_s": round(setup, 1)}
     t, its_b, conv, worst, rounds = 0.0, 0, True, 0.0, 0
     if kr > 0:
         S = FB.BlockSolver(tA, tF, kr, variant="afiim", precision="fp32", memory="device", verified=True)
@@ -915,6 +933,9 @@ def main():
     ap.add_argument("--batch", type=int, default=256, help="systems in the batched leg")
     ap.add_argument("--no-mrhs", action="store_true", help="skip the multi-RHS leg")
     ap.add_argument("--mrhs-n", type=int, default=4000000, help="rows of the multi-RHS system")
+    ap.add_argument("--mrhs-factors", default="afiim", choices=["afiim", "pdfiim"],
+                    help="factors of the multi-RHS system: AFIIM eps 0.1 (the named config; about two minutes "
+                         "to build at 4M) or PDFIIM (seconds)")
     ap.add_argument("--partition", default="replicas", choices=["replicas", "rows"],
                     help="N > 1: replicas of the system per rank (weak scaling, default) or one system in "
                          "row blocks over the ranks (strong scaling)")

@@ -20,47 +20,16 @@
 
 #include "fiim_b200.h"
 #include "fiim_internal.h"
+#include "fiim_sweep.h"
 
 namespace {
 
-struct Entry {
-    int idx;
-    double v;
-};
-using List = std::vector<Entry>;
-
-// Sparse accumulator over [0, n): dense values and a chain of touched indices, newest first.
-struct Accum {
-    std::vector<double> val;
-    std::vector<int> link;   // -1: untouched; else the index touched before this one (-2: none)
-    int head = -2, count = 0;
-    explicit Accum(int n) : val(n, 0.0), link(n, -1) {}
-    // First touch assigns (as the reference does), later touches add.
-    void add(int k, double v) {
-        if (link[k] == -1) {
-            val[k] = v;
-            link[k] = head;
-            head = k;
-            ++count;
-        } else {
-            val[k] += v;
-        }
-    }
-    template <class F>
-    void walk(F f) const {
-        for (int q = 0, k = head; q < count; ++q, k = link[k]) f(k);
-    }
-    void clear() {
-        for (int q = 0, k = head; q < count; ++q) {
-            const int nx = link[k];
-            link[k] = -1;
-            val[k] = 0.0;
-            k = nx;
-        }
-        head = -2;
-        count = 0;
-    }
-};
+using fiim::sweep::Accum;
+using fiim::sweep::Entry;
+using fiim::sweep::Factors;
+using fiim::sweep::List;
+using fiim::sweep::rows_of;
+using fiim::sweep::rows_of_transposed;
 
 // Drop filter of t_b or t_c (prec.cpp:383-414, 535-565): entries with
 // |D^{-1}_k val_k| <= (m * tol) / norm_k are zeroed, first with m = 1; while more than
@@ -87,80 +56,12 @@ int drop(Accum &a, const std::vector<double> &idv, double tol, const std::vector
     return a.count - cut;
 }
 
-struct Factors {
-    int n = 0;
-    std::vector<int> Gi, Gj, Hi, Hj, Li, Lj, Ui, Uj;
-    std::vector<double> Gv, Hv, Lv, Uv, IDv;
-};
-
-// Rows of per-index lists as CSR, row i = lists[i] in order (G from G^T, U from U^T).
-void rows_of(const std::vector<List> &lists, std::vector<int> &rp, std::vector<int> &ci, std::vector<double> &v) {
-    const int n = (int)lists.size();
-    rp.assign(n + 1, 0);
-    for (int i = 0; i < n; ++i) rp[i + 1] = rp[i] + (int)lists[i].size();
-    ci.resize(rp[n]);
-    v.resize(rp[n]);
-    for (int i = 0, at = 0; i < n; ++i)
-        for (const Entry &e : lists[i]) {
-            ci[at] = e.idx;
-            v[at++] = e.v;
-        }
-}
-
-// Transposed lists as CSR: lists[i] holds (row, value) entries of column i; a row's entries
-// come out in ascending column order (H from H^T, L from L^T; prec.cpp:917-1003).
-void rows_of_transposed(const std::vector<List> &lists, std::vector<int> &rp, std::vector<int> &ci,
-                        std::vector<double> &v) {
-    const int n = (int)lists.size();
-    rp.assign(n + 1, 0);
-    for (const List &l : lists)
-        for (const Entry &e : l) rp[e.idx + 1]++;
-    for (int i = 0; i < n; ++i) rp[i + 1] += rp[i];
-    ci.resize(rp[n]);
-    v.resize(rp[n]);
-    std::vector<int> pos(rp.begin(), rp.end() - 1);
-    for (int i = 0; i < n; ++i)
-        for (const Entry &e : lists[i]) {
-            ci[pos[e.idx]] = i;
-            v[pos[e.idx]++] = e.v;
-        }
-}
-
 int build(int n, const int *Ai, const int *Aj, const double *Av, double dtol1, double dtol2, double eta,
           double shift, double coeff, int limit, int filtit, Factors &out) {
-    // A split into its diagonal, strictly lower rows (CSR, row order) and strictly upper
-    // columns (CSC, rows ascending) (prec.cpp:279-344). A zero or missing diagonal reads dtol2.
-    std::vector<double> d(n, 0.0);
-    std::vector<int> lp(n + 1, 0), up(n + 1, 0);
-    for (int i = 0; i < n; ++i)
-        for (int q = Ai[i]; q < Ai[i + 1]; ++q) {
-            if (Aj[q] > i) up[Aj[q] + 1]++;
-            else if (Aj[q] < i) lp[i + 1]++;
-        }
-    for (int i = 0; i < n; ++i) {
-        lp[i + 1] += lp[i];
-        up[i + 1] += up[i];
-    }
-    std::vector<int> lcol(lp[n]), urow(up[n]);
-    std::vector<double> lval(lp[n]), uval(up[n]);
-    {
-        std::vector<int> upos(up.begin(), up.end() - 1);
-        for (int i = 0, lq = 0; i < n; ++i) {
-            for (int q = Ai[i]; q < Ai[i + 1]; ++q) {
-                const int c = Aj[q];
-                if (c > i) {
-                    urow[upos[c]] = i;
-                    uval[upos[c]++] = Av[q];
-                } else if (c < i) {
-                    lcol[lq] = c;
-                    lval[lq++] = Av[q];
-                } else {
-                    d[i] = Av[q];
-                }
-            }
-            if (d[i] == 0.0) d[i] = dtol2;
-        }
-    }
+    fiim::sweep::Split a;
+    fiim::sweep::split(n, Ai, Aj, Av, dtol2, a);
+    const std::vector<double> &d = a.d, &lval = a.lval, &uval = a.uval;
+    const std::vector<int> &lp = a.lp, &lcol = a.lcol, &up = a.up, &urow = a.urow;
 
     std::vector<double> &idv = out.IDv;
     idv.assign(n, 0.0);

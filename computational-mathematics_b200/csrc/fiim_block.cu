@@ -11,6 +11,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -22,8 +24,29 @@
 
 namespace fiim {
 
+// Shape of one matrix's SpMM: lane-group width (row groups per warp = 32 / lanes) and the
+// right-hand sides each lane owns (its load width: 1 value, or 2 or 4 as 16-byte pairs).
+struct SpmmShape {
+    int lanes = 32, per_lane = 1;
+};
+
+// Candidate shapes for k right-hand sides: one value per lane in a group of the next power of
+// two >= k lanes (the default), two per lane (k even), four per lane (k a multiple of 4).
+static std::vector<SpmmShape> spmm_candidates(int k) {
+    auto p2 = [](int v) {
+        int p = 1;
+        while (p < v) p <<= 1;
+        return p;
+    };
+    std::vector<SpmmShape> c = {{std::max(4, p2(k)), 1}};
+    if (k % 2 == 0 && k >= 4) c.push_back({std::max(4, p2(k / 2)), 2});
+    if (k % 4 == 0 && k >= 8) c.push_back({std::max(2, p2(k / 4)), 4});
+    return c;
+}
+
 struct BlockSolver {
     int device = -1, n = 0, k = 0, kp = 32;
+    SpmmShape shp[3];   // A, G, H
     fiim_options opt{};
     cudaStream_t stream = nullptr;
     Arena arena;
@@ -41,26 +64,35 @@ struct BlockSolver {
 
     bk::Shape shape() const { return bk::Shape{n, k}; }
 
-    template <int KP, typename V, typename Epi>
-    cudaError_t spmm_kp(const DevCsr &M, const V *vals, const double *X, const Epi &epi) {
-        auto kern = bk::k_spmm<KP, V, Epi>;
-        const int g = grid_for(kern, (long)kWarps * (32 / KP), n);
+    template <int L, int VW, typename V, typename Epi>
+    cudaError_t spmm_lv(const DevCsr &M, const V *vals, const double *X, const Epi &epi) {
+        auto kern = bk::k_spmm<L, VW, V, Epi>;
+        const int g = grid_for(kern, (long)kWarps * (32 / L), n);
         kern<<<g, kThreads, 0, stream>>>(CsrView<V>{M.rp, M.ci, vals, n}, shape(), X, epi, bs, partials);
         return cudaGetLastError();
     }
+    // Matrix `which` (0 A, 1 G, 2 H) times the n x k block X, in that matrix's shape.
     template <typename V, typename Epi>
-    cudaError_t spmm(const DevCsr &M, const V *vals, const double *X, const Epi &epi) {
-        switch (kp) {
-            case 4: return spmm_kp<4>(M, vals, X, epi);
-            case 8: return spmm_kp<8>(M, vals, X, epi);
-            case 16: return spmm_kp<16>(M, vals, X, epi);
-            default: return spmm_kp<32>(M, vals, X, epi);
+    cudaError_t spmm(int which, const DevCsr &M, const V *vals, const double *X, const Epi &epi) {
+        const SpmmShape s = shp[which];
+        switch (s.per_lane * 64 + s.lanes) {
+            case 64 + 4: return spmm_lv<4, 1>(M, vals, X, epi);
+            case 64 + 8: return spmm_lv<8, 1>(M, vals, X, epi);
+            case 64 + 16: return spmm_lv<16, 1>(M, vals, X, epi);
+            case 64 + 32: return spmm_lv<32, 1>(M, vals, X, epi);
+            case 128 + 4: return spmm_lv<4, 2>(M, vals, X, epi);
+            case 128 + 8: return spmm_lv<8, 2>(M, vals, X, epi);
+            case 128 + 16: return spmm_lv<16, 2>(M, vals, X, epi);
+            case 256 + 2: return spmm_lv<2, 4>(M, vals, X, epi);
+            case 256 + 4: return spmm_lv<4, 4>(M, vals, X, epi);
+            case 256 + 8: return spmm_lv<8, 4>(M, vals, X, epi);
+            default: return cudaErrorInvalidValue;
         }
     }
     template <typename Epi>
-    cudaError_t spmm_f(const DevCsr &M, const float *v32, const double *X, const Epi &epi) {
-        if (opt.precision == FIIM_MIXED_FP32) return spmm(M, v32, X, epi);
-        return spmm(M, M.v, X, epi);
+    cudaError_t spmm_f(int which, const DevCsr &M, const float *v32, const double *X, const Epi &epi) {
+        if (opt.precision == FIIM_MIXED_FP32) return spmm(which, M, v32, X, epi);
+        return spmm(which, M, M.v, X, epi);
     }
 
     template <int KP>
@@ -89,13 +121,13 @@ struct BlockSolver {
     }
 
     int enqueue_iteration(bool cond, cudaGraphConditionalHandle h) {
-        FIIM_CUDA(spmm_f(H, H32, p, bk::KEpiScale{tm, IDv, k}));
-        FIIM_CUDA(spmm_f(G, G32, tm, bk::KEpiNorm{pc}));
-        FIIM_CUDA(spmm(A, A.v, pc, bk::KEpiAlpha{v, r0}));
+        FIIM_CUDA(spmm_f(2, H, H32, p, bk::KEpiScale{tm, IDv, k}));
+        FIIM_CUDA(spmm_f(1, G, G32, tm, bk::KEpiNorm{pc}));
+        FIIM_CUDA(spmm(0, A, A.v, pc, bk::KEpiAlpha{v, r0}));
         FIIM_TRY(updates(0, cond, h));
-        FIIM_CUDA(spmm_f(H, H32, sv, bk::KEpiScale{tm, IDv, k}));
-        FIIM_CUDA(spmm_f(G, G32, tm, bk::KEpiStore{sc}));
-        FIIM_CUDA(spmm(A, A.v, sc, bk::KEpiOmega{t, sv}));
+        FIIM_CUDA(spmm_f(2, H, H32, sv, bk::KEpiScale{tm, IDv, k}));
+        FIIM_CUDA(spmm_f(1, G, G32, tm, bk::KEpiStore{sc}));
+        FIIM_CUDA(spmm(0, A, A.v, sc, bk::KEpiOmega{t, sv}));
         FIIM_TRY(updates(1, cond, h));
         FIIM_TRY(updates(2, cond, h));
         return FIIM_OK;
@@ -226,7 +258,73 @@ struct BlockSolver {
         std::vector<int> mmv(32, mm);
         FIIM_CUDA(cudaMemcpyAsync(bs.maxmsteps, mmv.data(), sizeof(int) * 32, cudaMemcpyHostToDevice, stream));
         FIIM_CUDA(cudaStreamSynchronize(stream));
+        FIIM_TRY(choose_shapes());
         return build_graph();
+    }
+
+    // SpMM shapes: the first candidate (one right-hand side per lane) by default, so results
+    // repeat bit for bit from process to process; FIIM_BLOCK_SHAPE=lanes,per_lane forces one
+    // candidate for every matrix; opt.autotune times every candidate on each matrix (one
+    // product into a scratch block, best of 5 after a warm-up) and keeps the fastest. The
+    // products are the same bits in every shape; the fused dot products' summation tree
+    // follows the shape.
+    int choose_shapes() {
+        const std::vector<SpmmShape> cand = spmm_candidates(k);
+        for (auto &s : shp) s = cand[0];
+        if (const char *e = std::getenv("FIIM_BLOCK_SHAPE")) {
+            int l = 0, v = 0;
+            if (std::sscanf(e, "%d,%d", &l, &v) == 2)
+                for (const SpmmShape &c : cand)
+                    if (c.lanes == l && c.per_lane == v)
+                        for (auto &s : shp) s = c;
+            return FIIM_OK;
+        }
+        if (!opt.autotune || cand.size() == 1) return FIIM_OK;
+        FIIM_TRY(reset_state(0.0, 0, k));   // every right-hand side running: gated kernels work
+        FIIM_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * (size_t)n * k, stream));
+        const DevCsr *mats[3] = {&A, &G, &H};
+        for (int m = 0; m < 3; ++m) {
+            float best = 0.f;
+            for (const SpmmShape &c : cand) {
+                shp[m] = c;
+                float tot = 0.f;
+                for (int rep = 0; rep < 6; ++rep) {
+                    FIIM_CUDA(cudaEventRecord(ev0, stream));
+                    if (m == 0) FIIM_CUDA(spmm(0, A, A.v, x, bk::KEpiStore{t}));
+                    else FIIM_CUDA(spmm_f(m, *mats[m], m == 1 ? G32 : H32, x, bk::KEpiStore{t}));
+                    FIIM_CUDA(cudaEventRecord(ev1, stream));
+                    FIIM_CUDA(cudaEventSynchronize(ev1));
+                    float ms = 0.f;
+                    FIIM_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+                    if (rep > 0) tot = (rep == 1) ? ms : std::min(tot, ms);
+                }
+                if (&c == &cand[0] || tot < best) {
+                    best = tot;
+                    tuned[m] = c;
+                }
+            }
+            shp[m] = tuned[m];
+        }
+        return FIIM_OK;
+    }
+    SpmmShape tuned[3];
+
+    // y = A x (op 0) or y = M x (op 1, G D^{-1} H x) on n x k blocks, in the solver's shapes.
+    int apply(int op, const double *X, double *Y) {
+        FIIM_CUDA(cudaSetDevice(device));
+        const bool dev = (opt.memory == FIIM_MEM_DEVICE);
+        const size_t bytes = sizeof(double) * (size_t)n * k;
+        FIIM_CUDA(cudaMemcpyAsync(x, X, bytes, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
+        FIIM_TRY(reset_state(0.0, 0, k));
+        if (op == 0) {
+            FIIM_CUDA(spmm(0, A, A.v, x, bk::KEpiStore{t}));
+        } else {
+            FIIM_CUDA(spmm_f(2, H, H32, x, bk::KEpiScale{tm, IDv, k}));
+            FIIM_CUDA(spmm_f(1, G, G32, tm, bk::KEpiStore{t}));
+        }
+        FIIM_CUDA(cudaMemcpyAsync(Y, t, bytes, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream));
+        FIIM_CUDA(cudaStreamSynchronize(stream));
+        return FIIM_OK;
     }
 
     int solve(const double *B, double *X, double tol, int nmax, int *iter, int *info, double *resval,
@@ -238,9 +336,9 @@ struct BlockSolver {
         FIIM_CUDA(cudaMemcpyAsync(b, B, bytes, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
         FIIM_CUDA(cudaMemcpyAsync(x, X, bytes, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream));
         FIIM_TRY(reset_state(tol, nmax, k));
-        FIIM_CUDA(spmm(A, A.v, x, bk::KEpiInit{b, p, r0, r}));
+        FIIM_CUDA(spmm(0, A, A.v, x, bk::KEpiInit{b, p, r0, r}));
         FIIM_CUDA(cudaGraphLaunch(exec, stream));
-        FIIM_CUDA(spmm(A, A.v, x, bk::KEpiResid{b}));
+        FIIM_CUDA(spmm(0, A, A.v, x, bk::KEpiResid{b}));
         // Verified: right-hand sides whose FP64 true residual misses the target restart from
         // their current x (the others stay finished), until none misses or the rounds run out.
         int rounds = 0, extra = 0;   // restart rounds; launches outside the loop bodies
@@ -254,9 +352,9 @@ struct BlockSolver {
             if (hg->active == 0) break;
             ++rounds;
             extra += 2;
-            FIIM_CUDA(spmm(A, A.v, x, bk::KEpiRestart{{b, p, r0, r}}));
+            FIIM_CUDA(spmm(0, A, A.v, x, bk::KEpiRestart{{b, p, r0, r}}));
             FIIM_CUDA(cudaGraphLaunch(exec, stream));
-            FIIM_CUDA(spmm(A, A.v, x, bk::KEpiResid{b}));
+            FIIM_CUDA(spmm(0, A, A.v, x, bk::KEpiResid{b}));
         }
         FIIM_CUDA(cudaMemcpyAsync(X, x, bytes, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream));
         FIIM_CUDA(cudaEventRecord(ev1, stream));
@@ -342,6 +440,19 @@ int fiim_block_solve(fiim_block_t h, const double *B, double *X, double tol, int
     if (!h || !B || !X) return fiim::set_error(FIIM_EARG, "null argument");
     return reinterpret_cast<fiim::BlockSolver *>(h)->solve(B, X, tol, NMAX, iter, info, resval, true_relres,
                                                              summary);
+}
+
+int fiim_block_apply(fiim_block_t h, int op, const double *X, double *Y) {
+    if (!h || !X || !Y || (op != 0 && op != 1)) return fiim::set_error(FIIM_EARG, "bad fiim_block_apply arguments");
+    return reinterpret_cast<fiim::BlockSolver *>(h)->apply(op, X, Y);
+}
+
+int fiim_block_spmm_shape(fiim_block_t h, int which, int *lanes, int *per_lane) {
+    if (!h || which < 0 || which > 2 || !lanes || !per_lane) return fiim::set_error(FIIM_EARG, "bad arguments");
+    const auto &s = reinterpret_cast<fiim::BlockSolver *>(h)->shp[which];
+    *lanes = s.lanes;
+    *per_lane = s.per_lane;
+    return FIIM_OK;
 }
 
 int fiim_block_destroy(fiim_block_t h) {

@@ -3,10 +3,13 @@
 // scalars and termination, sharing every sparse product.
 //
 // Vectors are n x k, row-major (entry (i, j) at i*k + j), so the k values a gathered
-// column index needs are contiguous. Work mapping shared by all kernels: a lane group of
-// KP = next power of two >= k lanes takes one row, lane j of the group owns right-hand side
-// j; a warp holds 32/KP row groups; warps walk rows in grid-stride order.
-// Sparse products: the group loads the row's entries KP at a time (coalesced) and
+// column index needs are contiguous. Work mapping: a lane group of L lanes (a power of two)
+// takes one row and each lane owns VW consecutive right-hand sides (lane l: columns l*VW ..
+// l*VW + VW - 1; VW = 1, 2 or 4, loaded as one or two 16-byte pairs); a warp holds 32/L row
+// groups; warps walk rows in grid-stride order. The vector updates use VW = 1 and
+// L = next power of two >= k; the sparse products take their (L, VW) from the solver's shape
+// (the row groups per warp and the load width), which never changes a product.
+// Sparse products: the group loads the row's entries L at a time (coalesced) and
 // broadcasts them lane by lane, so each right-hand side's row sum is formed left to right
 // in storage order with rounded products (the reference's arithmetic, bit for bit).
 // Reductions are per right-hand side: lanes of equal j are combined within the warp and
@@ -27,21 +30,26 @@ struct Shape {
     int k;        // right-hand sides
 };
 
-// Per-RHS reduction over the CTA and the grid; every thread calls it (uniformly).
-template <int KP, int NR, class Fin>
-__device__ __forceinline__ void rhs_reduce(double (&v)[NR], int k, double *__restrict__ partials, BState &bs,
+// Per-RHS reduction over the CTA and the grid; every thread calls it (uniformly). A thread
+// holds the partials of its VW right-hand sides (lane % L) * VW + u, u < VW.
+template <int L, int VW, int NR, class Fin>
+__device__ __forceinline__ void rhs_reduce(double (&v)[VW][NR], int k, double *__restrict__ partials, BState &bs,
                                            const Fin &fin) {
     __shared__ double sm[kWarps][32][NR];
     __shared__ int last;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    // combine the row groups of the warp (lanes with the same j)
+    // combine the row groups of the warp (lanes with the same right-hand sides)
 #pragma unroll
-    for (int j = 0; j < NR; ++j)
+    for (int u = 0; u < VW; ++u)
 #pragma unroll
-        for (int o = KP; o < 32; o <<= 1) v[j] += __shfl_xor_sync(0xffffffffu, v[j], o);
-    if (lane < KP)
+        for (int j = 0; j < NR; ++j)
 #pragma unroll
-        for (int j = 0; j < NR; ++j) sm[w][lane][j] = v[j];
+            for (int o = L; o < 32; o <<= 1) v[u][j] += __shfl_xor_sync(0xffffffffu, v[u][j], o);
+    if (lane < L)
+#pragma unroll
+        for (int u = 0; u < VW; ++u)
+#pragma unroll
+            for (int j = 0; j < NR; ++j) sm[w][lane * VW + u][j] = v[u][j];
     __syncthreads();
     if (threadIdx.x < k) {
         const int jj = threadIdx.x;
@@ -165,17 +173,34 @@ __device__ __forceinline__ double wide(double v) { return v; }
 __device__ __forceinline__ double wide(float v) { return (double)v; }
 
 // ---------------------------------------------------------------- SpMM
-template <int KP, typename V, typename Epi>
+// X's VW values of one gathered row for a lane, from a 16-byte aligned address when VW > 1
+// (VW > 1 needs an even k and VW | k, so that row * k + l * VW is a multiple of VW).
+template <int VW>
+__device__ __forceinline__ void gather(const double *__restrict__ p, double (&x)[VW]) {
+    if constexpr (VW == 1) {
+        x[0] = __ldg(p);
+    } else {
+#pragma unroll
+        for (int u = 0; u < VW; u += 2) {
+            const double2 d = __ldg(reinterpret_cast<const double2 *>(p + u));
+            x[u] = d.x;
+            x[u + 1] = d.y;
+        }
+    }
+}
+
+template <int L, int VW, typename V, typename Epi>
 static __global__ void __launch_bounds__(kThreads)
 k_spmm(CsrView<V> M, Shape sh, const double *__restrict__ X, Epi epi, BState bs, double *__restrict__ partials) {
     if (Epi::GATED && bs.g->active <= 0) return;
-    double red[Epi::NR];
+    double red[VW][Epi::NR];
 #pragma unroll
-    for (int q = 0; q < Epi::NR; ++q) red[q] = 0.0;
-    const unsigned gmask = (KP == 32) ? 0xffffffffu : (((1u << KP) - 1u) << ((threadIdx.x & 31) / KP * KP));
-    (void)gmask;
-    FIIM_ROW_GROUPS(KP, row) {
+    for (int u = 0; u < VW; ++u)
+#pragma unroll
+        for (int q = 0; q < Epi::NR; ++q) red[u][q] = 0.0;
+    FIIM_ROW_GROUPS(L, row) {
         const bool live = row < sh.n;
+        const int j0 = j_ * VW;            // this lane's first right-hand side
         int beg = 0, len = 0;
         if (live) {
             beg = __ldg(M.rp + row);
@@ -183,28 +208,37 @@ k_spmm(CsrView<V> M, Shape sh, const double *__restrict__ X, Epi epi, BState bs,
         }
         // every group of the warp walks the longest row of the warp (uniform shuffles), and
         // within a trip only as many entries as the longest remaining row part holds
-        const int trips = __reduce_max_sync(0xffffffffu, (len + KP - 1) / KP);
-        double s = 0.0;
+        const int trips = __reduce_max_sync(0xffffffffu, (len + L - 1) / L);
+        double s[VW];
+#pragma unroll
+        for (int u = 0; u < VW; ++u) s[u] = 0.0;
         for (int t = 0; t < trips; ++t) {
-            const int q = t * KP + j_;
+            const int q = t * L + j_;
             int c = 0;
             double a = 0.0;
             if (q < len) {
                 c = ldi(M.ci + beg + q);
                 a = wide(ldm(M.v + beg + q));
             }
-            const int ne = (int)__reduce_max_sync(0xffffffffu, (unsigned)max(0, min(KP, len - t * KP)));
+            const int ne = (int)__reduce_max_sync(0xffffffffu, (unsigned)max(0, min(L, len - t * L)));
 #pragma unroll 4
             for (int e = 0; e < ne; ++e) {
-                const int ce = __shfl_sync(0xffffffffu, c, grp_ * KP + e);
-                const double ae = __shfl_sync(0xffffffffu, a, grp_ * KP + e);
-                if (t * KP + e < len && j_ < sh.k)
-                    s = __dadd_rn(s, __dmul_rn(ae, __ldg(X + (size_t)ce * sh.k + j_)));
+                const int ce = __shfl_sync(0xffffffffu, c, grp_ * L + e);
+                const double ae = __shfl_sync(0xffffffffu, a, grp_ * L + e);
+                if (t * L + e < len && j0 < sh.k) {
+                    double xv[VW];
+                    gather<VW>(X + (size_t)ce * sh.k + j0, xv);
+#pragma unroll
+                    for (int u = 0; u < VW; ++u) s[u] = __dadd_rn(s[u], __dmul_rn(ae, xv[u]));
+                }
             }
         }
-        if (live && j_ < sh.k && !(Epi::GATED && bs.done[j_])) epi.emit((size_t)row * sh.k + j_, s, red);
+        if (live && j0 < sh.k)
+#pragma unroll
+            for (int u = 0; u < VW; ++u)
+                if (!(Epi::GATED && bs.done[j0 + u])) epi.emit((size_t)row * sh.k + j0 + u, s[u], red[u]);
     }
-    if constexpr (Epi::REDUCES) rhs_reduce<KP, Epi::NR>(red, sh.k, partials, bs, epi);
+    if constexpr (Epi::REDUCES) rhs_reduce<L, VW, Epi::NR>(red, sh.k, partials, bs, epi);
 }
 
 // ---------------------------------------------------------------- updates (n x k)
@@ -222,16 +256,16 @@ static __global__ void __launch_bounds__(kThreads)
 k_kupdate_s(Shape sh, const double *__restrict__ r, const double *__restrict__ v, const double *__restrict__ x,
             double *__restrict__ s, BState bs, double *__restrict__ partials) {
     if (bs.g->active <= 0) return;
-    double red[2] = {0.0, 0.0};
+    double red[1][2] = {{0.0, 0.0}};
     FIIM_ROW_GROUPS(KP, row) {
         if (row >= sh.n || j_ >= sh.k || bs.done[j_]) continue;
         const size_t at = (size_t)row * sh.k + j_;
         const double ri = r[at], xi = x[at];
         s[at] = __dadd_rn(ri, __dmul_rn(-bs.alpha[j_], v[at]));
-        red[0] += ri * ri;
-        red[1] += xi * xi;
+        red[0][0] += ri * ri;
+        red[0][1] += xi * xi;
     }
-    rhs_reduce<KP, 2>(red, sh.k, partials, bs, KFinS{});
+    rhs_reduce<KP, 1, 2>(red, sh.k, partials, bs, KFinS{});
 }
 
 template <int KP>
@@ -240,7 +274,7 @@ k_kupdate_xr(Shape sh, const double *__restrict__ pc, const double *__restrict__
              const double *__restrict__ t, const double *__restrict__ r0, double *__restrict__ x,
              double *__restrict__ r, BState bs, double *__restrict__ partials) {
     if (bs.g->active <= 0) return;
-    double red[1] = {0.0};
+    double red[1][1] = {{0.0}};
     FIIM_ROW_GROUPS(KP, row) {
         if (row >= sh.n || j_ >= sh.k || bs.done[j_]) continue;
         const size_t at = (size_t)row * sh.k + j_;
@@ -251,9 +285,9 @@ k_kupdate_xr(Shape sh, const double *__restrict__ pc, const double *__restrict__
         x[at] = xi;
         const double ri = __dadd_rn(s[at], __dmul_rn(-om, t[at]));
         r[at] = ri;
-        red[0] += r0[at] * ri;
+        red[0][0] += r0[at] * ri;
     }
-    rhs_reduce<KP, 1>(red, sh.k, partials, bs, KFinControl{});
+    rhs_reduce<KP, 1, 1>(red, sh.k, partials, bs, KFinControl{});
 }
 
 template <int KP>

@@ -44,11 +44,11 @@ EXPORTS = (
     "fiim_solver_spmv_shape", "fiim_solver_apply", "fiim_solver_kernel_times", "fiim_solver_kernel_times_seq", "fiim_solver_mode",
     "fiim_solver_set_wait_limit", "fiim_solver_test_stall", "fiim_solver_iteration_bytes",
     "fiim_solver_destroy", "fiim_batch_create", "fiim_batch_solve", "fiim_batch_destroy",
-    "fiim_block_create", "fiim_block_solve", "fiim_block_destroy",
+    "fiim_block_create", "fiim_block_solve", "fiim_block_apply", "fiim_block_spmm_shape", "fiim_block_destroy",
     "fiim_spmv", "fiim_prec_apply", "fiim_prec_apply_noalloc",
     "fiim_gen_poisson2d", "fiim_gen_convdiff3d", "fiim_gen_convdiff2d", "fiim_gen_batch_params",
     "fiim_gen_zipf", "fiim_gen_zipf_mean", "fiim_rand_normal", "fiim_model_rhs", "fiim_pdfiim_build", "fiim_pdfiim_build_gpu",
-    "fiim_acifim_build",
+    "fiim_acifim_build", "fiim_afiim_build",
     "fiim_read_mtx", "fiim_read_rhs", "fiim_factors_save", "fiim_factors_load",
     "fiim_dist_unique_id", "fiim_dist_partition", "fiim_dist_plan", "fiim_dist_create", "fiim_dist_solve",
     "fiim_dist_destroy", "fiim_dist_emulate",
@@ -508,9 +508,10 @@ class BlockSolver(_Handle):
     verified: as for BatchSolver, per right-hand side."""
 
     def __init__(self, A, F, nrhs, variant="afiim", precision="fp64", memory="host", verified=False,
-                 max_restarts=4):
+                 max_restarts=4, autotune=False):
         o = Options()
         lib().fiim_options_default(C.byref(o))
+        o.autotune = int(autotune)
         o.variant = _VARIANTS[variant]
         o.precision = _PRECISIONS[precision]
         o.memory = MEM_DEVICE if memory == "device" else MEM_HOST
@@ -535,6 +536,20 @@ class BlockSolver(_Handle):
         _check(lib().fiim_block_solve(self._h, _ptr(B), _ptr(X), C.c_double(tol), C.c_int(nmax), _ptr(it),
                                       _ptr(info), _ptr(rv), _ptr(tr), C.byref(r)))
         return {"iter": it, "info": info, "resval": rv, "true_relres": tr, "summary": r.as_dict()}
+
+    def apply(self, X, Y, op="A"):
+        """Y = A X (op 'A') or Y = M X (op 'M') on n x k blocks with the solver's SpMM kernels."""
+        if self.memory != "device":
+            X = _d(X)
+            assert Y.dtype == np.float64 and Y.flags.c_contiguous
+        _check(lib().fiim_block_apply(self._h, C.c_int(0 if op == "A" else 1), _ptr(X), _ptr(Y)))
+        return Y
+
+    def spmm_shape(self, which):
+        """(lanes per row group, right-hand sides per lane) of matrix `which` (0 A, 1 G, 2 H)."""
+        lanes, per = C.c_int(0), C.c_int(0)
+        _check(lib().fiim_block_spmm_shape(self._h, C.c_int(which), C.byref(lanes), C.byref(per)))
+        return lanes.value, per.value
 
     def close(self):
         if self._h and self._h.value:
@@ -669,6 +684,24 @@ def pdfiim_build(A, ftol, prefill=1, lfill=1, postfill=1, warpsize=-1, filttype=
          "Hi": np.zeros(n + 1, np.int32)}
     _check(fn(*args, C.byref(ng), C.byref(nh), _ptr(F["Gv"]), _ptr(F["Gj"]), _ptr(F["Gi"]),
                                _ptr(F["IDv"]), _ptr(F["Hv"]), _ptr(F["Hj"]), _ptr(F["Hi"])))
+    return F
+
+
+def afiim_build(A, dtol, elem_per_rowcol=10, growth=5, eta=0.0, shift=0.0):
+    """AFIIM construction on the host (the same factors as AFIIM/src/prec.cpp:101-767; the
+    defaults are the example driver's, AFIIM/example/example.cpp:37-39). Returns a factor
+    dict. Sequential in the rows; safe to call from several threads."""
+    Ai, Aj, Av = _i(A[0]), _i(A[1]), _d(A[2])
+    n = len(Ai) - 1
+    ng, nh = C.c_int(0), C.c_int(0)
+    L = lib()
+    args = (C.c_int(n), _ptr(Ai), _ptr(Aj), _ptr(Av), C.c_double(dtol), C.c_int(elem_per_rowcol), C.c_int(growth),
+            C.c_double(eta), C.c_double(shift), C.byref(ng), C.byref(nh))
+    _check(L.fiim_afiim_build(*args, *([None] * 7)))
+    F = {"Gv": np.zeros(ng.value), "Gj": np.zeros(ng.value, np.int32), "Gi": np.zeros(n + 1, np.int32),
+         "IDv": np.zeros(n), "Hv": np.zeros(nh.value), "Hj": np.zeros(nh.value, np.int32),
+         "Hi": np.zeros(n + 1, np.int32)}
+    _check(L.fiim_afiim_build(*args, *[_ptr(F[k]) for k in ("Gv", "Gj", "Gi", "IDv", "Hv", "Hj", "Hi")]))
     return F
 
 

@@ -243,6 +243,20 @@ int fiim_block_solve(fiim_block_t s, const double *B, double *X, double tol, int
                      int *iter, int *info, double *resval, double *true_relres,
                      fiim_result *summary);
 
+/* Y = A X (op 0) or Y = G D^{-1} H X (op 1) on n x nrhs blocks with the solver's SpMM
+ * kernels (in opt->memory space); each right-hand side's row sums are the reference's, in
+ * storage order, whatever the shape. For inspection and tests. */
+int fiim_block_apply(fiim_block_t s, int op, const double *X, double *Y);
+
+/* SpMM shape of matrix `which` (0 A, 1 G, 2 H): lanes per row group (32 / lanes rows per
+ * warp) and right-hand sides per lane (its load width: 1, or 2 or 4 as 16-byte pairs).
+ * The default is one per lane in a group of the next power of two >= nrhs lanes, the same
+ * for every matrix, so results repeat bit for bit across processes; opt->autotune = 1 times
+ * every candidate shape on each matrix at set-up and keeps the fastest (the fused dot
+ * products' summation tree follows the shape, so tuned results may differ in the last
+ * bits from run to run). */
+int fiim_block_spmm_shape(fiim_block_t s, int which, int *lanes, int *per_lane);
+
 int fiim_block_destroy(fiim_block_t s);
 
 /* ===========================================================================
@@ -318,6 +332,18 @@ int fiim_pdfiim_build_gpu(int n, const int *Ai, const int *Aj, const double *Av,
                           int lfill, int postfill, double ftol, int warpsize, char filttype,
                           char patt, int *nnzG, int *nnzH, double *Gv, int *Gj, int *Gi,
                           double *D, double *Hv, int *Hj, int *Hi);
+
+/* AFIIM factor construction on the host: the same G, D^{-1}, H as afiim
+ * (AFIIM/src/prec.cpp:101-767, arguments as there; the example driver passes
+ * elemPerRowCol 10, growth 5, eta 0, shift 0, AFIIM/example/example.cpp:37-39), bit for
+ * bit. elemPerRowCol and growth only size the reference's buffers. The construction is
+ * sequential in the rows, as the reference's is. Two calls, as fiim_pdfiim_build: the first
+ * (Gv == NULL) builds and returns nnzG, nnzH; the second copies out. The result is kept per
+ * calling thread, so threads may build different systems at once. */
+int fiim_afiim_build(int n, const int *Ai, const int *Aj, const double *Av, double dtol,
+                     int elemPerRowCol, int growth, double eta, double shift, int *nnzG,
+                     int *nnzH, double *Gv, int *Gj, int *Gi, double *IDv, double *Hv, int *Hj,
+                     int *Hi);
 
 /* ACIFIM factor construction on the host: the same G, D^{-1}, H, L and U as acifim
  * (ACIFIM/src/prec.cpp:127-1052, arguments as there; the example driver passes

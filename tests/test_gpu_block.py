@@ -108,3 +108,56 @@ def test_block_verified_meets_the_fp64_target():
         assert tv < 1e-8 and abs(tv - rv["true_relres"][j]) <= 1e-6 * tv
     assert restarted >= 1
     assert rv["summary"]["refine_steps"] >= 1 and ru["summary"]["refine_steps"] == 0
+
+
+def _shapes(k):
+    """The candidate SpMM shapes for k right-hand sides (lanes per row group, RHS per lane)."""
+    p2 = lambda v: 1 << max(0, (v - 1).bit_length())
+    c = [(max(4, p2(k)), 1)]
+    if k % 2 == 0 and k >= 4:
+        c.append((max(4, p2(k // 2)), 2))
+    if k % 4 == 0 and k >= 8:
+        c.append((max(2, p2(k // 4)), 4))
+    return c
+
+
+@pytest.mark.parametrize("k", [32, 12, 6, 5])
+def test_block_products_bit_identical_in_every_shape(monkeypatch, k):
+    """A X and M X through the block kernels, in every candidate shape, equal the oracle's
+    single-vector products column by column, bit for bit (FP64 and FP32-stored factors)."""
+    import pyoracle as O
+    A, F = zipf_system(4000, 29)
+    n = len(A[0]) - 1
+    rng = np.random.default_rng(k)
+    X = rng.standard_normal((n, k))
+    for precision in ("fp64", "fp32"):
+        Fr = rounded(F, precision)
+        ref_a = np.stack([O.csr_mv(A[0], A[1], A[2], X[:, j]) for j in range(k)], axis=1)
+        ref_m = np.stack([O.prec_apply(Fr, X[:, j]) for j in range(k)], axis=1)
+        for lanes, per in _shapes(k):
+            monkeypatch.setenv("FIIM_BLOCK_SHAPE", f"{lanes},{per}")
+            S = FB.BlockSolver(A, F, k, precision=precision)
+            assert all(S.spmm_shape(m) == (lanes, per) for m in range(3))
+            Ya, Ym = S.apply(X, np.zeros((n, k))), S.apply(X, np.zeros((n, k)), op="M")
+            S.close()
+            assert np.array_equal(Ya, ref_a), (precision, lanes, per)
+            assert np.array_equal(Ym, ref_m), (precision, lanes, per)
+
+
+@pytest.mark.parametrize("shape", [(16, 2), (8, 4)])
+def test_block_solve_in_wide_shapes(monkeypatch, shape):
+    """The 32-RHS solve with two or four right-hand sides per lane: every right-hand side
+    inside the oracle's envelope."""
+    monkeypatch.setenv("FIIM_BLOCK_SHAPE", f"{shape[0]},{shape[1]}")
+    A = FB.gen_convdiff3d(12, 0.5)
+    F = FB.pdfiim_build(A, 0.05, 2, 2, 1, -1, "I", "B")
+    res = check_block(A, F, 32, "fp32", variant="pdfiim", seed=100)
+    assert (res["info"] == 0).all()
+
+
+def test_block_autotune_picks_a_candidate():
+    A, F = zipf_system(20000, 31)
+    S = FB.BlockSolver(A, F, 16, precision="fp32", autotune=True)
+    shapes = [S.spmm_shape(m) for m in range(3)]
+    S.close()
+    assert all(s in _shapes(16) for s in shapes), shapes

@@ -375,3 +375,43 @@ def test_host_acifim_nan_pivot_fails():
         FB.acifim_build((A[0], A[1], Av), 0.1, 0.05)
     if O.have_ref("acifim"):
         assert O.acifim_build((A[0], A[1], Av), 0.1, 0.05)[1] == 1
+
+
+@pytest.mark.parametrize("name,prefix,dtol", [("sherman2", "afiim9e-6_", 9e-6), ("sherman2", "afiim0.1_", 0.1),
+                                              ("poisson128_afiim", "", 0.1)])
+def test_host_afiim_matches_golden_factors(golden, name, prefix, dtol):
+    """The library's AFIIM construction against the factors the reference built for the
+    committed fixtures (AFIIM/src/prec.cpp:101-767), bit for bit."""
+    g = golden(name)
+    F = FB.afiim_build((g["Ai"], g["Aj"], g["Av"]), dtol)
+    R = sub(g, prefix)
+    for k in ("Gi", "Gj", "Gv", "IDv", "Hi", "Hj", "Hv"):
+        assert F[k].dtype == R[k].dtype and np.array_equal(F[k], R[k]), k
+
+
+@pytest.mark.skipif(not O.have_ref("afiim"), reason="oracle/_ref not built")
+@pytest.mark.parametrize("case", [
+    dict(system="zipf", n=20000, dtol=0.1),
+    dict(system="random", seed=5, dtol=0.05),
+    dict(system="random", seed=6, dtol=0.1, shift=0.1, eta=0.4),
+    dict(system="random", seed=7, dtol=0.02, zero_diag=30),
+    dict(system="convdiff", k=4, dtol=0.1),
+])
+def test_host_afiim_matches_live_reference(case):
+    """Against the reference's own afiim, compiled here: the multi-RHS benchmark's Zipf family,
+    random nonsymmetric systems (shift and eta, rows whose diagonal is zero), and a 2D
+    convection-diffusion system."""
+    case = dict(case)
+    system, dtol = case.pop("system"), case.pop("dtol")
+    if system == "zipf":
+        n = case.pop("n")
+        A = FB.gen_zipf(n, FB.zipf_scale(4000000, sample=200000))
+    elif system == "random":
+        A = _random_system(3000, case.pop("seed"), case.pop("zero_diag", 0))
+    else:
+        side, diff, theta, pe = FB.batch_params(20261203, case.pop("k"))
+        A = FB.gen_convdiff2d(side, diff, theta, pe)
+    R = O.afiim_build(A, dtol, **case)
+    F = FB.afiim_build(A, dtol, **case)
+    for k in ("Gi", "Gj", "Gv", "IDv", "Hi", "Hj", "Hv"):
+        assert F[k].dtype == R[k].dtype and np.array_equal(F[k], R[k]), k
