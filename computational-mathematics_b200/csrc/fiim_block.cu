@@ -264,9 +264,12 @@ struct BlockSolver {
 
     // SpMM shapes: the first candidate (one right-hand side per lane) by default, so results
     // repeat bit for bit from process to process; FIIM_BLOCK_SHAPE=lanes,per_lane forces one
-    // candidate for every matrix; opt.autotune times every candidate on each matrix (one
-    // product into a scratch block, best of 5 after a warm-up) and keeps the fastest. The
-    // products are the same bits in every shape; the fused dot products' summation tree
+    // candidate for every matrix; opt.autotune times, for every candidate given to all three
+    // matrices, the first half of the loop body's products in their order and with their
+    // epilogues (H p with the D^{-1} scale, G tm with ||pc||^2, A pc with r0 . v; best of 5
+    // after a warm-up) and keeps the fastest. Timing a product alone ranks the shapes
+    // differently: its epilogue streams and the previous product's output in L2 are missing.
+    // The products are the same bits in every shape; the fused dot products' summation tree
     // follows the shape.
     int choose_shapes() {
         const std::vector<SpmmShape> cand = spmm_candidates(k);
@@ -281,33 +284,34 @@ struct BlockSolver {
         }
         if (!opt.autotune || cand.size() == 1) return FIIM_OK;
         FIIM_TRY(reset_state(0.0, 0, k));   // every right-hand side running: gated kernels work
-        FIIM_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * (size_t)n * k, stream));
-        const DevCsr *mats[3] = {&A, &G, &H};
-        for (int m = 0; m < 3; ++m) {
-            float best = 0.f;
-            for (const SpmmShape &c : cand) {
-                shp[m] = c;
-                float tot = 0.f;
-                for (int rep = 0; rep < 6; ++rep) {
-                    FIIM_CUDA(cudaEventRecord(ev0, stream));
-                    if (m == 0) FIIM_CUDA(spmm(0, A, A.v, x, bk::KEpiStore{t}));
-                    else FIIM_CUDA(spmm_f(m, *mats[m], m == 1 ? G32 : H32, x, bk::KEpiStore{t}));
-                    FIIM_CUDA(cudaEventRecord(ev1, stream));
-                    FIIM_CUDA(cudaEventSynchronize(ev1));
-                    float ms = 0.f;
-                    FIIM_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
-                    if (rep > 0) tot = (rep == 1) ? ms : std::min(tot, ms);
-                }
-                if (&c == &cand[0] || tot < best) {
-                    best = tot;
-                    tuned[m] = c;
-                }
+        hg->alpha_guard = 0;                 // the timed alpha steps on zero vectors retire nothing
+        FIIM_CUDA(cudaMemcpyAsync(bs.g, hg, sizeof(bt::BGlobal), cudaMemcpyHostToDevice, stream));
+        for (double *vec : {p, tm, pc, v, r0})
+            FIIM_CUDA(cudaMemsetAsync(vec, 0, sizeof(double) * (size_t)n * k, stream));
+        float best = 0.f;
+        SpmmShape pick = cand[0];
+        for (const SpmmShape &c : cand) {
+            for (auto &s : shp) s = c;
+            float tot = 0.f;
+            for (int rep = 0; rep < 6; ++rep) {
+                FIIM_CUDA(cudaEventRecord(ev0, stream));
+                FIIM_CUDA(spmm_f(2, H, H32, p, bk::KEpiScale{tm, IDv, k}));
+                FIIM_CUDA(spmm_f(1, G, G32, tm, bk::KEpiNorm{pc}));
+                FIIM_CUDA(spmm(0, A, A.v, pc, bk::KEpiAlpha{v, r0}));
+                FIIM_CUDA(cudaEventRecord(ev1, stream));
+                FIIM_CUDA(cudaEventSynchronize(ev1));
+                float ms = 0.f;
+                FIIM_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+                if (rep > 0) tot = (rep == 1) ? ms : std::min(tot, ms);
             }
-            shp[m] = tuned[m];
+            if (&c == &cand[0] || tot < best) {
+                best = tot;
+                pick = c;
+            }
         }
+        for (auto &s : shp) s = pick;
         return FIIM_OK;
     }
-    SpmmShape tuned[3];
 
     // y = A x (op 0) or y = M x (op 1, G D^{-1} H x) on n x k blocks, in the solver's shapes.
     int apply(int op, const double *X, double *Y) {

@@ -93,15 +93,23 @@ __device__ __forceinline__ void rhs_reduce(double (&v)[VW][NR], int k, double *_
          base_ < sh.n; base_ += nw_ * (32 / (KP)), row = base_ + grp_)
 
 // ---------------------------------------------------------------- epilogues
+// emit(at, s, red) finishes entry `at` of the n x k output block from its row sum s;
+// emit2(at, s0, s1, red0, red1) finishes the two consecutive entries at, at + 1 (at even)
+// with the same arithmetic per entry, reading and writing both as one 16-byte pair (the
+// sparse products with two or four right-hand sides per lane).
 #define FIIM_BEPI(nr, reduces, gated)            \
     static constexpr int NR = nr;                \
     static constexpr bool REDUCES = reduces;     \
     static constexpr bool GATED = gated
 
+__device__ __forceinline__ void st2(double *p, double a, double b) { *reinterpret_cast<double2 *>(p) = make_double2(a, b); }
+__device__ __forceinline__ double2 ld2(const double *__restrict__ p) { return __ldg(reinterpret_cast<const double2 *>(p)); }
+
 struct KEpiStore {
     FIIM_BEPI(1, false, true);
     double *y;
     __device__ void emit(size_t at, double s, double (&)[NR]) const { y[at] = s; }
+    __device__ void emit2(size_t at, double s0, double s1, double (&)[NR], double (&)[NR]) const { st2(y + at, s0, s1); }
     __device__ void finish(BState &, int, const double *) const {}
 };
 struct KEpiScale {                 // y = d o (M x), d per row
@@ -110,12 +118,21 @@ struct KEpiScale {                 // y = d o (M x), d per row
     const double *__restrict__ d;
     int k;
     __device__ void emit(size_t at, double s, double (&)[NR]) const { y[at] = __dmul_rn(__ldg(d + at / k), s); }
+    __device__ void emit2(size_t at, double s0, double s1, double (&)[NR], double (&)[NR]) const {
+        const double di = __ldg(d + at / k);
+        st2(y + at, __dmul_rn(di, s0), __dmul_rn(di, s1));
+    }
     __device__ void finish(BState &, int, const double *) const {}
 };
 struct KEpiNorm {
     FIIM_BEPI(1, true, true);
     double *y;
     __device__ void emit(size_t at, double s, double (&r)[NR]) const { y[at] = s; r[0] += s * s; }
+    __device__ void emit2(size_t at, double s0, double s1, double (&ra)[NR], double (&rb)[NR]) const {
+        st2(y + at, s0, s1);
+        ra[0] += s0 * s0;
+        rb[0] += s1 * s1;
+    }
     __device__ void finish(BState &bs, int j, const double *t) const { bs.pc2[j] = t[0]; }
 };
 struct KEpiAlpha {
@@ -125,6 +142,12 @@ struct KEpiAlpha {
     __device__ void emit(size_t at, double s, double (&r)[NR]) const {
         y[at] = s;
         r[0] += __ldg(r0 + at) * s;
+    }
+    __device__ void emit2(size_t at, double s0, double s1, double (&ra)[NR], double (&rb)[NR]) const {
+        st2(y + at, s0, s1);
+        const double2 q = ld2(r0 + at);
+        ra[0] += q.x * s0;
+        rb[0] += q.y * s1;
     }
     __device__ void finish(BState &bs, int j, const double *t) const { bt::BEpiAlpha{}.finish(bs, j, t); }
 };
@@ -136,6 +159,14 @@ struct KEpiOmega {
         y[at] = s;
         r[0] += s * __ldg(sv + at);
         r[1] += s * s;
+    }
+    __device__ void emit2(size_t at, double s0, double s1, double (&ra)[NR], double (&rb)[NR]) const {
+        st2(y + at, s0, s1);
+        const double2 q = ld2(sv + at);
+        ra[0] += s0 * q.x;
+        ra[1] += s0 * s0;
+        rb[0] += s1 * q.y;
+        rb[1] += s1 * s1;
     }
     __device__ void finish(BState &bs, int j, const double *t) const { bs.omega[j] = t[0] / t[1]; }
 };
@@ -150,6 +181,15 @@ struct KEpiInit {
         r[at] = pi;
         red[0] += pi * pi;
     }
+    __device__ void emit2(size_t at, double s0, double s1, double (&ra)[NR], double (&rb)[NR]) const {
+        const double2 q = ld2(b + at);
+        const double p0 = __dadd_rn(q.x, __dmul_rn(-1.0, s0)), p1 = __dadd_rn(q.y, __dmul_rn(-1.0, s1));
+        st2(p + at, p0, p1);
+        st2(r0 + at, p0, p1);
+        st2(r + at, p0, p1);
+        ra[0] += p0 * p0;
+        rb[0] += p1 * p1;
+    }
     __device__ void finish(BState &bs, int j, const double *t) const { bt::BFinInit{}.finish(bs, j, t); }
 };
 struct KEpiRestart : KEpiInit {
@@ -162,6 +202,14 @@ struct KEpiResid {
         const double bi = b[at], ri = bi - s;
         red[0] += ri * ri;
         red[1] += bi * bi;
+    }
+    __device__ void emit2(size_t at, double s0, double s1, double (&ra)[NR], double (&rb)[NR]) const {
+        const double2 q = ld2(b + at);
+        const double ri0 = q.x - s0, ri1 = q.y - s1;
+        ra[0] += ri0 * ri0;
+        ra[1] += q.x * q.x;
+        rb[0] += ri1 * ri1;
+        rb[1] += q.y * q.y;
     }
     __device__ void finish(BState &bs, int j, const double *t) const {
         bs.ts[j] = t[0];
@@ -233,10 +281,21 @@ k_spmm(CsrView<V> M, Shape sh, const double *__restrict__ X, Epi epi, BState bs,
                 }
             }
         }
-        if (live && j0 < sh.k)
+        if (live && j0 < sh.k) {
+            const size_t at = (size_t)row * sh.k + j0;
+            bool all = true;   // every right-hand side of this lane still running
+            if constexpr (Epi::GATED)
 #pragma unroll
-            for (int u = 0; u < VW; ++u)
-                if (!(Epi::GATED && bs.done[j0 + u])) epi.emit((size_t)row * sh.k + j0 + u, s[u], red[u]);
+                for (int u = 0; u < VW; ++u) all = all && !bs.done[j0 + u];
+            if (VW > 1 && all) {
+#pragma unroll
+                for (int u = 0; u < VW; u += 2) epi.emit2(at + u, s[u], s[u + 1], red[u], red[u + 1]);
+            } else {
+#pragma unroll
+                for (int u = 0; u < VW; ++u)
+                    if (!(Epi::GATED && bs.done[j0 + u])) epi.emit(at + u, s[u], red[u]);
+            }
+        }
     }
     if constexpr (Epi::REDUCES) rhs_reduce<L, VW, Epi::NR>(red, sh.k, partials, bs, epi);
 }
