@@ -50,7 +50,7 @@ struct Arena {
 // Forms of the CSR-stream SpMV. Both give the same bits; they differ in how a row block's
 // streams reach shared memory: through registers, pipelined by one block (fiim_kernels.cuh),
 // or by bulk copies into two buffers (fiim_pipe.cuh).
-constexpr int kFormRows = 0, kFormBulk = 1;
+constexpr int kFormRows = 0, kFormBulk = 1, kFormWarp = 2;
 
 // A CSR matrix resident on the device. v holds FP64 values; v32 / v16 are optional
 // FP32 / BF16 copies for the mixed-precision inner solve.

@@ -486,6 +486,105 @@ k_spmv_rows(CsrView<double> M, const int *__restrict__ rb, const int *__restrict
     if constexpr (Epi::REDUCES) grid_reduce<Epi::NR>(red, partials, st, epi);
 }
 
+// Warp-block form of the CSR-stream SpMV: the same arithmetic as k_spmv_rows (rounded
+// products staged in shared memory, each row summed left to right by one thread), with row
+// blocks of at most 32 rows and WT - 1 entries that each warp takes on its own, in
+// grid-stride order over the warps. A warp synchronises only with itself (__syncwarp), so
+// the warps of a CTA do not wait for one another between blocks; the loop is pipelined by
+// one block per warp, as in k_spmv_rows. A row of WT or more entries is a block of its own,
+// summed by lane 0 over WT-sized chunks, still in storage order.
+template <int WT, typename Epi, bool NARROW = false>
+static __global__ void __launch_bounds__(kThreads)
+k_spmv_warp(CsrView<double> M, const int *__restrict__ rb, const int *__restrict__ eb, int nblk,
+            const double *__restrict__ x, Epi epi, DState *st, double *__restrict__ partials,
+            NarrowCols nc = NarrowCols{}) {
+    pdl_enter();
+    if (Epi::GATED && st != nullptr && st->done) return;
+    __shared__ double prod_all[kWarps][WT];
+    constexpr int PER = WT / 32;
+    const int lane = (int)threadIdx.x & 31, w = (int)threadIdx.x >> 5;
+    double *prod = prod_all[w];
+    const int gw = (int)blockIdx.x * kWarps + w, nw = (int)gridDim.x * kWarps;
+    double red[Epi::NR];
+#pragma unroll
+    for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
+    int r0 = 0, r1 = 0, e0 = 0, e1 = 0, rbeg = 0, rend = 0, cbase = 0;
+    double opnd = 0.0;
+    ColRegs<NARROW, PER> c;
+    double a[PER];
+    auto fetch = [&](int blk) {
+        r0 = __ldg(rb + blk);
+        r1 = __ldg(rb + blk + 1);
+        e0 = __ldg(eb + blk);
+        e1 = __ldg(eb + blk + 1);
+        if constexpr (NARROW) cbase = __ldg(nc.base + blk);
+        rbeg = rend = 0;
+        if (r0 + lane < r1) {
+            rbeg = __ldg(M.rp + r0 + lane);
+            rend = __ldg(M.rp + r0 + lane + 1);
+            if constexpr (HasPre<Epi>::value) opnd = epi.pre(r0 + lane);
+        }
+        if (e1 - e0 < WT) {
+            const int a0 = e0 & ~1;
+#pragma unroll
+            for (int u = 0; u < PER / 2; ++u) {
+                const int e = a0 + 2 * (lane + u * 32);
+                c.zero(u);
+                a[2 * u] = a[2 * u + 1] = 0.0;
+                if (e + 1 < e1) {
+                    c.load2(M.ci, nc, e, u);
+                    const double2 aa = ldm2(M.v + e);
+                    a[2 * u] = aa.x;
+                    a[2 * u + 1] = aa.y;
+                } else if (e < e1) {
+                    c.load1(M.ci, nc, e, u);
+                    a[2 * u] = ldm(M.v + e);
+                }
+            }
+        }
+    };
+    if (gw < nblk) fetch(gw);
+    for (int blk = gw; blk < nblk; blk += nw) {
+        const int nxt = blk + nw;
+        const int cr0 = r0, cr1 = r1, ce0 = e0, ce1 = e1, cb = rbeg - e0, ce = rend - e0, cbs = cbase;
+        const double copnd = opnd;
+        if (ce1 - ce0 < WT) {
+            const int a0 = ce0 & ~1;
+#pragma unroll
+            for (int u = 0; u < PER; ++u) {
+                const int e = a0 + 2 * (lane + (u >> 1) * 32) + (u & 1);
+                if (e >= ce0 && e < ce1) prod[e - ce0] = __dmul_rn(a[u], ldx(x + c.get(u, cbs)));
+            }
+            if (nxt < nblk) fetch(nxt);
+            __syncwarp();
+            if (cr0 + lane < cr1) {
+                double s = 0.0;
+                for (int k = cb; k < ce; ++k) s = __dadd_rn(s, prod[k]);
+                if constexpr (HasPre<Epi>::value) epi.emit_pre(cr0 + lane, s, copnd, red);
+                else epi.emit(cr0 + lane, s, red);
+            }
+            __syncwarp();
+        } else {
+            double s = 0.0;
+            for (int c0 = ce0; c0 < ce1; c0 += WT) {
+                const int c1 = min(c0 + WT, ce1);
+                for (int e = c0 + lane; e < c1; e += 32) {
+                    const int j = NARROW ? cbs + (int)__ldcs(nc.d + e) : ldi(M.ci + e);
+                    prod[e - c0] = __dmul_rn(ldm(M.v + e), ldx(x + j));
+                }
+                __syncwarp();
+                if (lane == 0)
+                    for (int k = 0; k < c1 - c0; ++k) s = __dadd_rn(s, prod[k]);
+                __syncwarp();
+            }
+            if (lane == 0) epi.emit(cr0, s, red);
+            if (nxt < nblk) fetch(nxt);
+        }
+    }
+    pdl_release();
+    if constexpr (Epi::REDUCES) grid_reduce<Epi::NR>(red, partials, st, epi);
+}
+
 // Narrow column stream for k_spmv_rows: per row block, base = smallest column + 32768 and
 // d[e] = column - base, when the block's columns span at most 65,536; otherwise *wide is set
 // and the matrix keeps its 32-bit columns. One CTA per block, grid-stride.

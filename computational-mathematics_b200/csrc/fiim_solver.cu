@@ -176,11 +176,28 @@ static cudaError_t spmv_pipe(cudaStream_t s, const DevCsr &M, const double *x, c
     return launch_k(kern, g, smem, s, view(M), M.rb, M.nblk, x, epi, st, partials, fault);
 }
 
+// Warp-block size of the kFormWarp CSR-stream (entries per warp block, 8 per lane).
+constexpr int kWarpTile = 256;
+
+template <typename Epi>
+static cudaError_t spmv_warp(cudaStream_t s, const DevCsr &M, const double *x, const Epi &epi, DState *st,
+                             double *partials) {
+    if (M.narrow) {
+        auto kern = k_spmv_warp<kWarpTile, Epi, true>;
+        const int g = grid_for(kern, kWarps, M.nblk);
+        return launch_k(kern, g, 0, s, view(M), M.rb, M.eb, M.nblk, x, epi, st, partials, NarrowCols{M.cd, M.cb});
+    }
+    auto kern = k_spmv_warp<kWarpTile, Epi, false>;
+    const int g = grid_for(kern, kWarps, M.nblk);
+    return launch_k(kern, g, 0, s, view(M), M.rb, M.eb, M.nblk, x, epi, st, partials, NarrowCols{});
+}
+
 // Solver SpMV: CSR-stream over the matrix's row blocks, exact row order, in the form and
 // row-block size the tuner chose. Every form gives the same bits.
 template <typename Epi>
 cudaError_t launch_spmv(const DevCsr &M, cudaStream_t s, const double *x, const Epi &epi, DState *st,
                         double *partials, int *fault = nullptr) {
+    if (M.form == kFormWarp) return spmv_warp(s, M, x, epi, st, partials);
     if (M.form == kFormBulk && fault) {
         if (M.tile == 1024) return spmv_pipe<1024>(s, M, x, epi, st, partials, fault);
         return spmv_pipe<2048>(s, M, x, epi, st, partials, fault);
@@ -242,7 +259,9 @@ int build_narrow(DevCsr &M, cudaStream_t s) {
 
 int set_tile(DevCsr &M, int tile, cudaStream_t s) {
     std::vector<int> rb;
-    build_row_blocks(M.hrp, tile - 1, kThreads, rb);   // k_spmv_rows reads aligned pairs
+    // k_spmv_rows reads aligned pairs (blocks of at most tile - 1 entries); a warp block has
+    // at most 32 rows, a CTA block kThreads.
+    build_row_blocks(M.hrp, tile - 1, M.form == kFormWarp ? 32 : kThreads, rb);
     M.tile = tile;
     M.nblk = (int)rb.size() - 1;
     std::vector<int> eb(rb.size());
@@ -273,6 +292,7 @@ static int autotune_tile(DevCsr &M, const double *x, double *y, cudaStream_t s, 
     const int only = !force ? -1
                             : (std::strcmp(force, "rows") == 0     ? kFormRows
                                : std::strcmp(force, "staged") == 0 ? kFormBulk
+                               : std::strcmp(force, "warp") == 0   ? kFormWarp
                                                                    : -1);
     std::vector<long> key = M.sig;
     key.push_back(only);
@@ -288,7 +308,8 @@ static int autotune_tile(DevCsr &M, const double *x, double *y, cudaStream_t s, 
     }
     // Candidates (row-block size, form).
     const std::pair<int, int> cands[] = {{512, kFormRows},  {1024, kFormRows}, {2048, kFormRows},
-                                         {4096, kFormRows},  {1024, kFormBulk}, {2048, kFormBulk}};
+                                         {4096, kFormRows},  {1024, kFormBulk}, {2048, kFormBulk},
+                                         {kWarpTile, kFormWarp}};
     cudaEvent_t e0, e1;
     FIIM_CUDA(cudaEventCreate(&e0));
     FIIM_CUDA(cudaEventCreate(&e1));
@@ -839,9 +860,16 @@ int Solver::create(int n_, const int *Ai, const int *Aj, const double *Av, const
             FIIM_TRY(autotune_tile(M, tm, t, stream, fault));
         } else {
             // Deterministic shape: the same launch shape, hence the same reduction trees and
-            // the same bits, in every process on the same GPU model.
-            M.form = kFormRows;
-            FIIM_TRY(set_tile(M, default_tile(M), stream));
+            // the same bits, in every process on the same GPU model. FIIM_SPMV=warp selects
+            // the warp-block form instead.
+            const char *form_env = std::getenv("FIIM_SPMV");
+            if (form_env && std::strcmp(form_env, "warp") == 0) {
+                M.form = kFormWarp;
+                FIIM_TRY(set_tile(M, kWarpTile, stream));
+            } else {
+                M.form = kFormRows;
+                FIIM_TRY(set_tile(M, default_tile(M), stream));
+            }
         }
     }
     {

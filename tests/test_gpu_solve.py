@@ -70,7 +70,8 @@ def test_prec_apply_matches_oracle(golden, cuda, name, prefix):
     ("poisson128_afiim", "", "afiim", {}), ("convdiff16_pdfiim", "", "pdfiim", {}),
     ("convdiff2d48_acifim", "", "acifim", {"mode": "C", "nr": 2}), ("poisson32_sym_pdfiim", "", "pdfiim",
                                                                      {"issym": True})])
-@pytest.mark.parametrize("form,cols", [("rows", "narrow"), ("rows", "wide"), ("staged", "wide")])
+@pytest.mark.parametrize("form,cols", [("rows", "narrow"), ("rows", "wide"), ("staged", "wide"), ("warp", "narrow"),
+                                       ("warp", "wide")])
 def test_solver_products_bit_identical(golden, monkeypatch, name, prefix, variant, kw, form, cols):
     """The solver's tuned CSR-stream kernels (streams through registers, with 16-bit or 32-bit
     column streams, or by bulk copies) reproduce the oracle's A x and M x exactly."""
@@ -87,7 +88,7 @@ def test_solver_products_bit_identical(golden, monkeypatch, name, prefix, varian
     S.close()
 
 
-@pytest.mark.parametrize("form", [None, "staged"])
+@pytest.mark.parametrize("form", [None, "staged", "warp"])
 @pytest.mark.parametrize("long_len", [0, 2046, 2047, 2048, 2500])
 def test_solver_spmv_random_rows(monkeypatch, long_len, form):
     """Random columns over the whole matrix, row blocks that start at odd entries, and a
@@ -280,7 +281,7 @@ def test_dropin_solve_matches_reference(golden, name, fprefix, rprefix, variant,
     assert true_relres(g, x) <= 10 * true_relres(g, g[rprefix + "x"]) + 1e-12
 
 
-@pytest.mark.parametrize("form", ["rows", "staged"])
+@pytest.mark.parametrize("form", ["rows", "staged", "warp"])
 def test_solver_forms_agree_on_convdiff64(monkeypatch, form):
     """A 64^3 solve takes the same iterations and (to rounding) the same x with either SpMV form."""
     monkeypatch.setenv("FIIM_SPMV", form)
@@ -462,3 +463,30 @@ def test_convdiff64_host_factors_match_oracle():
     tr = np.linalg.norm(b - sp.csr_matrix((A[2], A[1], A[0])) @ x) / np.linalg.norm(b)
     assert abs(tr - r["true_relres"]) <= 1e-3 * tr
     S.close()
+
+
+@pytest.mark.parametrize("long_len", [254, 255, 256, 257, 600])
+def test_solver_warp_form_rows_about_its_block_size(monkeypatch, long_len):
+    """The warp-block form (blocks of at most 32 rows and 255 entries): rows that fill a
+    block, one entry short of it, or need the long-row path. A x equals the oracle's bit
+    for bit."""
+    rng = np.random.default_rng(long_len)
+    n = 30000
+    lens = rng.integers(1, 12, n)
+    rows, cols = [], []
+    for i, k in enumerate(lens):
+        if i % 997 == 3:
+            k = long_len
+        rows.append(np.full(k, i))
+        cols.append(rng.choice(n, k, replace=False))
+    rows, cols = np.concatenate(rows), np.concatenate(cols)
+    M = sp.csr_matrix((rng.uniform(-1, 1, rows.size), (rows, cols)), shape=(n, n))
+    M.sort_indices()
+    A = (M.indptr.astype(np.int32), M.indices.astype(np.int32), M.data)
+    u = rng.standard_normal(n)
+    monkeypatch.setenv("FIIM_SPMV", "warp")
+    S = FB.Solver(A, identity_factors(n))
+    assert S.spmv_shape(0) == (256, 2)
+    y = S.apply(u, np.zeros(n), op="A")
+    S.close()
+    assert np.array_equal(y, O.csr_mv(A[0], A[1], A[2], u))
