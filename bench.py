@@ -943,10 +943,9 @@ def main():
     ap.add_argument("--no-small", action="store_true", help="skip the small plain case (Poisson 128^2)")
     ap.add_argument("--cpu-solves", type=int, default=3, help="timed full solves of the CPU baseline leg")
     # DRAM bytes per launch of the dominant kernel (H's SpMV) from an ncu capture of the
-    # 96^3 case (read + write = 0.842 x its algorithmic bytes: the column stream is stored as
-    # 16-bit offsets), scaled to the 128^3 launch by the units processed (entries and rows,
-    # which the traffic is proportional to).
-    ap.add_argument("--ncu-traffic", type=float, default=278.8e6,
+    # 128^3 workload (dram__bytes_read.sum + dram__bytes_write.sum, mean of three H launches:
+    # 0.817 x its algorithmic bytes, the column stream being stored as 16-bit offsets).
+    ap.add_argument("--ncu-traffic", type=float, default=270.7e6,
                     help="dram bytes per launch of the dominant kernel from an ncu capture")
     ap.add_argument("--dry-run", action="store_true",
                     help="no GPU: check the rank launcher and max-over-ranks timing over gloo (solves nothing)")
