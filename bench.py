@@ -471,7 +471,9 @@ def run_small(args, dev):
     x0 = 0, AFIIM factors with drop tolerance 0.1, FP64, rtol 1e-8, NMAX 1000). The factors
     are the ones the reference built for the committed fixture tests/golden/poisson128_afiim.npz
     (data only). The working set fits in L2: the solve is bound by launch and reduction latency,
-    not HBM bandwidth."""
+    not HBM bandwidth. The default path at this size is one thread-block cluster (the solve
+    vectors in the CTAs' shared memory); the WHILE graph and the cooperative launch are timed
+    beside it."""
     import torch
     import fiim_b200 as FB
     z = np.load(os.path.join(ROOT, "tests", "golden", "poisson128_afiim.npz"))
@@ -481,12 +483,15 @@ def run_small(args, dev):
     x = torch.zeros_like(b)
     def timed(persist):
         prev = os.environ.get("FIIM_PERSIST")
-        os.environ["FIIM_PERSIST"] = persist
+        if persist is None:
+            os.environ.pop("FIIM_PERSIST", None)
+        else:
+            os.environ["FIIM_PERSIST"] = persist
         try:
             S = FB.Solver(A, F, variant="afiim", memory="device")
         finally:
             if prev is None:
-                del os.environ["FIIM_PERSIST"]
+                os.environ.pop("FIIM_PERSIST", None)
             else:
                 os.environ["FIIM_PERSIST"] = prev
         mode = S.mode()
@@ -501,11 +506,13 @@ def run_small(args, dev):
         ms = sum(q["device_ms"] for q in rr) / len(rr)
         return {"solves_per_s": round(1000.0 / ms, 2), "ms_per_solve": round(ms, 4), "iterations": rr[-1]["iter"],
                 "us_per_iteration": round(1000.0 * ms / max(rr[-1]["iter"], 1), 2), "info": rr[-1]["info"],
-                "mode": {0: "WHILE graph", 1: "host-relaunched graph", 2: "one cooperative launch"}[mode]}
+                "mode": {0: "WHILE graph", 1: "host-relaunched graph", 2: "one cooperative launch",
+                         3: "one thread-block cluster"}[mode]}
     out = {"workload": "poisson2d_128 (n=16,384) AFIIM eps 0.1 (reference-built factors) FP64 BiCGSTAB",
            "reference_iterations": int(z["iter"]), "reference_iteration_envelope": [int(v) for v in z["iter_env"]],
            "bound": "latency (working set in L2)"}
-    out.update(timed("0"))
+    out.update(timed(None))                  # the default: one thread-block cluster at this size
+    out["while_graph"] = timed("0")
     out["one_cooperative_launch"] = timed("1")
     return out
 

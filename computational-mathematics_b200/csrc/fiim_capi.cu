@@ -298,7 +298,7 @@ int fiim_solver_mode(fiim_solver_t h) {
     if (!h) return fiim::set_error(FIIM_EARG, "bad handle");
     if (fiim_is_mixed(h)) return 1;
     auto *s = reinterpret_cast<fiim::Solver *>(h);
-    return s->persistent ? 2 : (s->use_cond ? 0 : 1);
+    return s->clustered ? 3 : s->persistent ? 2 : (s->use_cond ? 0 : 1);
 }
 
 int fiim_solver_set_wait_limit(fiim_solver_t h, int polls) {

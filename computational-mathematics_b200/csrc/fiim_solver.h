@@ -58,6 +58,11 @@ struct Solver : SolverBase {
     // Small systems: the whole solve as one cooperative launch (fiim_persist.cuh).
     bool persistent = false;
     int persist_grid = 0;
+    // Small systems: the whole solve in one thread-block cluster, vectors in shared memory
+    // (fiim_cluster.cuh).
+    bool clustered = false;
+    int cluster_rows = 0;
+    int launch_cluster();
     unsigned *pbar = nullptr;    // grid barrier words
     int wait_limit = 1 << 21;    // barrier polls (back-to-back acquire loads of the barrier word) before a solve gives up
     bool stall_next = false;     // test hook: the next solve's first barrier never completes

@@ -241,7 +241,8 @@ class Solver(_Handle):
         return t.value, f.value
 
     def mode(self) -> int:
-        """0 device-driven WHILE graph, 1 host-relaunched graph, 2 one cooperative launch."""
+        """0 device-driven WHILE graph, 1 host-relaunched graph, 2 one cooperative launch, 3 one
+        thread-block cluster (the default for systems of at most 32,768 rows)."""
         rc = lib().fiim_solver_mode(self._h)
         if rc < 0:
             _check(rc)

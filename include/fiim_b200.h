@@ -175,7 +175,9 @@ int fiim_solver_kernel_times_seq(fiim_solver_t s, int reps, int max_kernels, dou
  * body on the device (the default), 1 a one-iteration graph relaunched by the host
  * (FIIM_GRAPH=host; also what a mixed-precision solver reports), 2 the whole solve as one
  * cooperative launch with grid barriers between its phases (FIIM_PERSIST=1, systems of at
- * most 65,536 rows). */
+ * most 65,536 rows), 3 the whole solve in one thread-block cluster of 16 CTAs whose shared
+ * memory holds the solve vectors (the default for FP64 systems of at most 32,768 rows where
+ * the device can run it; FIIM_PERSIST=0 keeps the WHILE graph). */
 int fiim_solver_mode(fiim_solver_t s);
 
 /* Bound on each grid-barrier wait of a one-launch solve, in polls (back-to-back acquire loads
