@@ -205,6 +205,7 @@ void fiim_options_default(fiim_options *o) {
     o->max_refine = 50;
     o->verified = 0;
     o->max_restarts = 4;
+    o->reliable = 0.01;
 }
 
 int fiim_EPBiCGSTAB_afiim(int n, double *Av, int *Aj, int *Ai, double *b, double tol, int NMAX,

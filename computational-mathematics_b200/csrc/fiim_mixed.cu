@@ -1,4 +1,5 @@
-// Mixed-precision solve: FP64 iterative refinement around an FP32 inner BiCGSTAB.
+// Mixed-precision solve: an FP32 BiCGSTAB whose residual the FP64 b - A x replaces (reliable
+// updates, the default), or FP64 iterative refinement around an FP32 inner BiCGSTAB.
 //
 // Layout in HBM (one arena):
 //   A   : int32 rp/ci shared by an FP64 value array (outer residual) and an FP32 copy
@@ -8,10 +9,17 @@
 //   sc, tm: FP32.  Two DState blocks (inner, outer) and the reduction partials.
 // The FP64 factor values are staged through one scratch buffer at set-up and not kept.
 //
-// Solve: r64 = b - A x (FP64, true residual); while ||r64|| > tol ||b||: inner BiCGSTAB on
-// r64/||r64|| from e = 0 to inner_tol (one CUDA graph with a device-driven WHILE node, the
-// reference's control flow), x += ||r64|| e, r64 = b - A x. The host reads two scalars per
-// refinement step.
+// Reliable updates (opt.reliable = delta > 0): r64 = b - A x0 (FP64), sigma = ||r64||; one
+// FP32 BiCGSTAB on r64 / sigma from e = 0 (the reference's control flow, in one CUDA graph
+// with a device-driven WHILE node); its body ends in an IF node that, when the recurrence
+// residual has fallen below delta times its running maximum or has met the target, moves
+// sigma e into x and replaces r by (b - A x) / sigma (fiim_mixed.cuh, RState). The solve
+// stops when that FP64 residual meets tol ||b||; the host reads the scalars once per solve.
+//
+// Refinement (opt.reliable = 0): r64 = b - A x (FP64, true residual); while ||r64|| >
+// tol ||b||: inner BiCGSTAB on r64/||r64|| from e = 0 to inner_tol (the same graph without
+// the IF node), x += ||r64|| e, r64 = b - A x. The host reads two scalars per refinement
+// step.
 
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
@@ -98,6 +106,8 @@ struct MixedSolver : SolverBase {
     float *e = nullptr, *r = nullptr, *r0 = nullptr, *p = nullptr, *v = nullptr, *s = nullptr;
     float *t = nullptr, *pc = nullptr, *sc = nullptr, *tm = nullptr;
     DState *st = nullptr, *sto = nullptr, *hst = nullptr;
+    mx::RState *rs = nullptr, *hrs = nullptr;   // reliable updates (device, pinned host copy)
+    bool reliable = false;
     double *partials = nullptr;
     unsigned long long *d_count = nullptr, *h_count = nullptr;
     cudaGraph_t graph = nullptr;
@@ -111,7 +121,9 @@ struct MixedSolver : SolverBase {
         return spmv_f(M, is_g ? G32 : H32, stream, xx, epi, st, partials);
     }
 
-    int enqueue_inner(bool cond, cudaGraphConditionalHandle h) {
+    // cond: bit 0 = set the WHILE node's condition (hw), bit 1 = set the IF node's (hif,
+    // reliable updates); 0 outside a graph.
+    int enqueue_inner(int cond, cudaGraphConditionalHandle hw, cudaGraphConditionalHandle hif) {
         const long nn = n;
         FIIM_CUDA(spmv_gh(H, false, p, mx::EpiScaleF{tm, D32}));
         FIIM_CUDA(spmv_gh(G, true, tm, mx::EpiNormF{pc}));
@@ -120,10 +132,63 @@ struct MixedSolver : SolverBase {
         FIIM_CUDA(spmv_gh(H, false, s, mx::EpiScaleF{tm, D32}));
         FIIM_CUDA(spmv_gh(G, true, tm, mx::EpiStoreF{sc}));
         FIIM_CUDA(spmv_f(A, A32, stream, sc, mx::EpiOmegaF{t, s}, st, partials));
-        FIIM_CUDA(launch_k(mx::k_update_xr_f, sgrid(mx::k_update_xr_f, nn), 0, stream, nn, pc, sc, s, t, r0, e, r,
-                           st, partials));
-        FIIM_CUDA(launch_k(mx::k_update_p_f, sgrid(mx::k_update_p_f, nn), 0, stream, nn, r, v, p, st, h,
-                           cond ? 1 : 0));
+        if (reliable) {
+            auto kxr = mx::k_update_xr_f<mx::FinControlR>;
+            FIIM_CUDA(launch_k(kxr, sgrid(kxr, nn), 0, stream, nn, pc, sc, s, t, r0, e, r, st, partials,
+                               mx::FinControlR{rs}));
+            FIIM_CUDA(launch_k(mx::k_update_p_r, sgrid(mx::k_update_p_r, nn), 0, stream, nn, r, v, p, st,
+                               (const mx::RState *)rs, hw, hif, cond));
+            return FIIM_OK;
+        }
+        auto kxr = mx::k_update_xr_f<FinControl>;
+        FIIM_CUDA(launch_k(kxr, sgrid(kxr, nn), 0, stream, nn, pc, sc, s, t, r0, e, r, st, partials, FinControl{}));
+        FIIM_CUDA(launch_k(mx::k_update_p_f, sgrid(mx::k_update_p_f, nn), 0, stream, nn, r, v, p, st, hw,
+                           (cond & 1) ? 1 : 0));
+        return FIIM_OK;
+    }
+
+    // The replacement of reliable updates (the IF node's body): x += sigma e, e = 0, then
+    // r = (b - A x) / sigma with the FP64 A, p moved by the change in r, m1 = r0 . r.
+    int enqueue_replace() {
+        const long nn = n;
+        FIIM_CUDA(launch_k(mx::k_replace_x, sgrid(mx::k_replace_x, nn), 0, stream, nn, e, x,
+                           (const mx::RState *)rs));
+        FIIM_CUDA(spmv_64(A, stream, x, mx::EpiReplace{b, r, p, r0, rs}, st, partials));
+        return FIIM_OK;
+    }
+
+    // Captures one inner iteration into `into`; with reliable updates an IF node (hif) that
+    // runs the replacement follows the last kernel.
+    int capture_body(cudaGraph_t into, int cond, cudaGraphConditionalHandle hw, cudaGraphConditionalHandle hif) {
+        FIIM_CUDA(cudaStreamBeginCaptureToGraph(stream, into, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_inner(cond, hw, hif);
+        cudaGraph_t ifbody = nullptr;
+        if (rc == FIIM_OK && reliable) {
+            cudaStreamCaptureStatus cs;
+            const cudaGraphNode_t *deps = nullptr;
+            size_t nd = 0;
+            cudaGraphNodeParams ip = {};
+            ip.type = cudaGraphNodeTypeConditional;
+            ip.conditional.handle = hif;
+            ip.conditional.type = cudaGraphCondTypeIf;
+            ip.conditional.size = 1;
+            cudaGraphNode_t ifn;
+            cudaError_t ce = cudaStreamGetCaptureInfo(stream, &cs, nullptr, nullptr, &deps, &nd);
+            if (ce == cudaSuccess) ce = cudaGraphAddNode(&ifn, into, deps, nd, &ip);
+            if (ce == cudaSuccess) ce = cudaStreamUpdateCaptureDependencies(stream, &ifn, 1, cudaStreamSetCaptureDependencies);
+            if (ce == cudaSuccess) ifbody = ip.conditional.phGraph_out[0];
+            else rc = set_error(FIIM_ECUDA, cudaGetErrorString(ce));
+        }
+        cudaGraph_t captured = nullptr;
+        const cudaError_t ec = cudaStreamEndCapture(stream, &captured);
+        if (rc != FIIM_OK) return rc;
+        FIIM_CUDA(ec);
+        if (!ifbody) return FIIM_OK;
+        FIIM_CUDA(cudaStreamBeginCaptureToGraph(stream, ifbody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        rc = enqueue_replace();
+        const cudaError_t ec2 = cudaStreamEndCapture(stream, &captured);
+        if (rc != FIIM_OK) return rc;
+        FIIM_CUDA(ec2);
         return FIIM_OK;
     }
 
@@ -133,27 +198,29 @@ struct MixedSolver : SolverBase {
         hd.done = 1;
         *hst = hd;
         FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
-        FIIM_TRY(enqueue_inner(false, cudaGraphConditionalHandle{}));
+        FIIM_TRY(enqueue_inner(0, cudaGraphConditionalHandle{}, cudaGraphConditionalHandle{}));
+        if (reliable) FIIM_TRY(enqueue_replace());   // writes only this solver's scratch vectors
         FIIM_CUDA(cudaStreamSynchronize(stream));
         // FIIM_GRAPH=host: a graph of one inner iteration, relaunched by the host (the same
         // kernels and shapes; for profilers that replay graph kernel nodes one by one).
         const char *mode_env = std::getenv("FIIM_GRAPH");
         if (mode_env && std::strcmp(mode_env, "host") == 0) {
-            FIIM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-            const int rc = enqueue_inner(false, cudaGraphConditionalHandle{});
             cudaGraph_t g1 = nullptr;
-            const cudaError_t ec = cudaStreamEndCapture(stream, &g1);
-            if (rc != FIIM_OK) return rc;
-            FIIM_CUDA(ec);
-            FIIM_CUDA(cudaGraphInstantiate(&exec, g1, 0));
+            FIIM_CUDA(cudaGraphCreate(&g1, 0));
             graph = g1;
+            cudaGraphConditionalHandle hif{};
+            if (reliable) FIIM_CUDA(cudaGraphConditionalHandleCreate(&hif, g1, 0, cudaGraphCondAssignDefault));
+            FIIM_TRY(capture_body(g1, reliable ? 2 : 0, cudaGraphConditionalHandle{}, hif));
+            FIIM_CUDA(cudaGraphInstantiate(&exec, g1, 0));
             host_loop = true;
             return FIIM_OK;
         }
         cudaGraph_t g = nullptr;
         FIIM_CUDA(cudaGraphCreate(&g, 0));
-        cudaGraphConditionalHandle h;
+        graph = g;
+        cudaGraphConditionalHandle h, hif{};
         FIIM_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+        if (reliable) FIIM_CUDA(cudaGraphConditionalHandleCreate(&hif, g, 0, cudaGraphCondAssignDefault));
         cudaGraphNodeParams cp = {};
         cp.type = cudaGraphNodeTypeConditional;
         cp.conditional.handle = h;
@@ -162,14 +229,8 @@ struct MixedSolver : SolverBase {
         cudaGraphNode_t node;
         FIIM_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
         cudaGraph_t body = cp.conditional.phGraph_out[0];
-        FIIM_CUDA(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        const int rc = enqueue_inner(true, h);
-        cudaGraph_t captured = nullptr;
-        const cudaError_t ec = cudaStreamEndCapture(stream, &captured);
-        if (rc != FIIM_OK) return rc;
-        FIIM_CUDA(ec);
+        FIIM_TRY(capture_body(body, reliable ? 3 : 1, h, hif));
         FIIM_CUDA(cudaGraphInstantiate(&exec, g, 0));
-        graph = g;
         return FIIM_OK;
     }
 
@@ -210,6 +271,9 @@ struct MixedSolver : SolverBase {
             return set_error(FIIM_EARG, "mixed precision applies the explicit product (mode 'E')");
         if (!(opt.inner_tol > 0.0) || opt.inner_nmax <= 0 || opt.max_refine <= 0)
             return set_error(FIIM_EARG, "inner_tol > 0, inner_nmax > 0 and max_refine > 0 are required");
+        if (!(opt.reliable >= 0.0 && opt.reliable < 1.0))
+            return set_error(FIIM_EARG, "reliable must be 0 (refinement) or a delta in (0, 1)");
+        reliable = opt.reliable > 0.0;
         FIIM_TRY(check_device(&device));
         FIIM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         FIIM_CUDA(cudaEventCreate(&ev0));
@@ -230,7 +294,8 @@ struct MixedSolver : SolverBase {
         bytes += csr_bytes(n, nG) + csr_bytes(n, nH);
         bytes += Arena::need(vsz * std::max<long>(nG, 1)) + Arena::need(vsz * std::max<long>(nH, 1));
         bytes += 3 * Arena::need(sizeof(double) * n) + 11 * Arena::need(sizeof(float) * n);
-        bytes += 2 * Arena::need(sizeof(DState)) + Arena::need(sizeof(double) * 4 * max_blocks) + 4096;
+        bytes += 2 * Arena::need(sizeof(DState)) + Arena::need(sizeof(mx::RState)) +
+                 Arena::need(sizeof(double) * 4 * max_blocks) + 4096;
         FIIM_TRY(arena.reserve(bytes));
         FIIM_TRY(carve_csr(arena, A, n, nA));
         FIIM_TRY(carve_csr(arena, G, n, nG));   // G.v / H.v: FP64 staging, dropped after conversion
@@ -251,14 +316,17 @@ struct MixedSolver : SolverBase {
             if (!(*pp = static_cast<float *>(arena.take(sizeof(float) * n)))) return set_error(FIIM_ENOMEM, "arena");
         st = static_cast<DState *>(arena.take(sizeof(DState)));
         sto = static_cast<DState *>(arena.take(sizeof(DState)));
+        rs = static_cast<mx::RState *>(arena.take(sizeof(mx::RState)));
         partials = static_cast<double *>(arena.take(sizeof(double) * 4 * max_blocks));
         d_count = static_cast<unsigned long long *>(arena.take(sizeof(unsigned long long)));
-        if (!A32 || !st || !sto || !partials || !d_count || (bf16 ? (!G16 || !H16) : (!G32 || !H32)))
+        if (!A32 || !st || !sto || !rs || !partials || !d_count || (bf16 ? (!G16 || !H16) : (!G32 || !H32)))
             return set_error(FIIM_ENOMEM, "arena exhausted");
-        FIIM_CUDA(cudaHostAlloc(&hst, 2 * sizeof(DState) + 64, cudaHostAllocDefault));
+        FIIM_CUDA(cudaHostAlloc(&hst, 2 * sizeof(DState) + 64 + sizeof(mx::RState), cudaHostAllocDefault));
         h_count = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(hst) + 2 * sizeof(DState) + 32);
+        hrs = reinterpret_cast<mx::RState *>(reinterpret_cast<char *>(hst) + 2 * sizeof(DState) + 64);
         FIIM_CUDA(cudaMemsetAsync(st, 0, sizeof(DState), stream));
         FIIM_CUDA(cudaMemsetAsync(sto, 0, sizeof(DState), stream));
+        FIIM_CUDA(cudaMemsetAsync(rs, 0, sizeof(mx::RState), stream));
 
         FIIM_TRY(upload_csr(A, nA, n, Ai, Aj, Av, 0, dev, stream, d_count, h_count));
         FIIM_TRY(upload_csr(G, nG, n, Gi, Gj, Gv, 1, dev, stream, d_count, h_count));
@@ -325,9 +393,61 @@ struct MixedSolver : SolverBase {
             nb = std::sqrt(hso->tt);
             return FIIM_OK;
         };
+        // The inner loop: the graph's WHILE node, or (FIIM_GRAPH=host) the host relaunching
+        // a one-iteration graph until the device reports done.
+        auto run_inner = [&]() -> int {
+            if (!host_loop) {
+                FIIM_CUDA(cudaGraphLaunch(exec, stream));
+                return FIIM_OK;
+            }
+            int launched = 0, chunk = 1;
+            for (;;) {
+                for (int q = 0; q < chunk; ++q) FIIM_CUDA(cudaGraphLaunch(exec, stream));
+                launched += chunk;
+                FIIM_CUDA(cudaMemcpyAsync(&hst->done, &st->done, sizeof(int), cudaMemcpyDeviceToHost, stream));
+                FIIM_CUDA(cudaStreamSynchronize(stream));
+                if (hst->done) return FIIM_OK;
+                if (launched > hst->nmax + 2) return set_error(FIIM_ETIMEOUT, "inner solve did not finish");
+                chunk = std::min(chunk * 2, 16);
+            }
+        };
         FIIM_TRY(residual());
         const double r_start = nr;
-        while (true) {
+        // Reliable updates: one inner solve over the whole iteration budget; its residual
+        // replacements (refine_steps) move the correction into x and verify the stop in FP64.
+        if (reliable) {
+            if (nr <= tol * nb) {
+                info = 0;
+            } else if (nmax > 0) {
+                *hst = hi;
+                hst->nmax = nmax;
+                hst->tol = tol * nb / nr;
+                *hrs = mx::RState{};
+                hrs->sigma = nr;
+                hrs->inv_sigma = 1.0 / nr;
+                hrs->goal = tol * nb;
+                hrs->delta = opt.reliable;
+                hrs->true_r = nr;
+                hrs->max_verify = opt.max_refine;
+                FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
+                FIIM_CUDA(cudaMemcpyAsync(rs, hrs, sizeof(mx::RState), cudaMemcpyHostToDevice, stream));
+                mx::k_inner_init<<<sgrid(mx::k_inner_init, n), kThreads, 0, stream>>>(n, r64, sto, r, r0, p, e, st,
+                                                                                       partials);
+                FIIM_CUDA(cudaGetLastError());
+                FIIM_TRY(run_inner());
+                mx::k_promote<<<sgrid(mx::k_promote, n), kThreads, 0, stream>>>(n, e, x, sto);
+                FIIM_CUDA(cudaGetLastError());
+                FIIM_CUDA(cudaMemcpyAsync(hst, st, sizeof(DState), cudaMemcpyDeviceToHost, stream));
+                FIIM_CUDA(cudaMemcpyAsync(hrs, rs, sizeof(mx::RState), cudaMemcpyDeviceToHost, stream));
+                FIIM_TRY(residual());
+                if (hst->info == -5) return set_error(FIIM_ETIMEOUT, "device loop guard tripped");
+                steps = hrs->replacements;
+                total_iters = hst->iter + ((hst->info == 1 || hst->info == 2) ? 1 : 0);
+                launches += 2 + hst->loops * 9 + hrs->replacements * 2;
+                info = (nr <= tol * nb) ? 0 : ((hst->info >= 1 && hst->info <= 3) ? hst->info : 3);
+            }
+        }
+        while (!reliable) {
             if (nr <= tol * nb) { info = 0; break; }
             if (steps >= opt.max_refine || total_iters >= nmax) { info = 3; break; }
             *hst = hi;
@@ -340,20 +460,7 @@ struct MixedSolver : SolverBase {
             FIIM_CUDA(cudaMemcpyAsync(st, hst, sizeof(DState), cudaMemcpyHostToDevice, stream));
             mx::k_inner_init<<<sgrid(mx::k_inner_init, n), kThreads, 0, stream>>>(n, r64, sto, r, r0, p, e, st, partials);
             FIIM_CUDA(cudaGetLastError());
-            if (!host_loop) {
-                FIIM_CUDA(cudaGraphLaunch(exec, stream));
-            } else {
-                int launched = 0, chunk = 1;
-                for (;;) {
-                    for (int q = 0; q < chunk; ++q) FIIM_CUDA(cudaGraphLaunch(exec, stream));
-                    launched += chunk;
-                    FIIM_CUDA(cudaMemcpyAsync(&hst->done, &st->done, sizeof(int), cudaMemcpyDeviceToHost, stream));
-                    FIIM_CUDA(cudaStreamSynchronize(stream));
-                    if (hst->done) break;
-                    if (launched > hst->nmax + 2) return set_error(FIIM_ETIMEOUT, "inner solve did not finish");
-                    chunk = std::min(chunk * 2, 16);
-                }
-            }
+            FIIM_TRY(run_inner());
             mx::k_promote<<<sgrid(mx::k_promote, n), kThreads, 0, stream>>>(n, e, x, sto);
             FIIM_CUDA(cudaGetLastError());
             FIIM_CUDA(cudaMemcpyAsync(hst, st, sizeof(DState), cudaMemcpyDeviceToHost, stream));

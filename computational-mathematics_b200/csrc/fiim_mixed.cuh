@@ -211,11 +211,12 @@ k_update_s_f(long n, const float *__restrict__ r, const float *__restrict__ v,
     grid_reduce<2>(red, partials, st, FinS{});
 }
 
+template <class Fin = FinControl>
 static __global__ void __launch_bounds__(kThreads)
 k_update_xr_f(long n, const float *__restrict__ pc, const float *__restrict__ sc,
               const float *__restrict__ s, const float *__restrict__ t,
               const float *__restrict__ r0, float *__restrict__ e, float *__restrict__ r,
-              DState *st, double *__restrict__ partials) {
+              DState *st, double *__restrict__ partials, Fin fin = Fin{}) {
     pdl_enter();
     if (st->done) return;
     const float a = (float)st->alpha, om = (float)st->omega;
@@ -227,7 +228,7 @@ k_update_xr_f(long n, const float *__restrict__ pc, const float *__restrict__ sc
         red[0] += (double)r0[i] * (double)ri;
     }
     pdl_release();
-    grid_reduce<1>(red, partials, st, FinControl{});
+    grid_reduce<1>(red, partials, st, fin);
 }
 
 static __global__ void __launch_bounds__(kThreads)
@@ -246,6 +247,136 @@ k_update_p_f(long n, const float *__restrict__ r, const float *__restrict__ v,
     const float b = (float)st->beta, c = (float)(-st->beta * st->omega);
     FIIM_FOR_ROWS(i, n) { p[i] = fmaf(c, v[i], fmaf(b, p[i], r[i])); }
 }
+
+// ---------------------------------------------------------------- reliable updates
+// Residual replacement (Sleijpen and van der Vorst, "Reliable updated residuals in hybrid
+// Bi-CG methods", Computing 56 (1996); in the mixed-precision form of Clark et al., "Solving
+// lattice QCD systems of equations using mixed precision solvers on GPUs", Comput. Phys.
+// Commun. 181 (2010)): ONE FP32 BiCGSTAB on (b - A x0) / sigma, sigma = ||b - A x0||, whose
+// recurrence residual r is replaced by the FP64 true residual whenever ||r|| has fallen
+// below delta times its largest value since the last replacement, and whenever the
+// recurrence meets the target. A replacement first moves the correction into the FP64
+// iterate (x += sigma e, e = 0), then computes b - A x with the FP64 A and sets
+//   r <- (b - A x) / sigma,   p <- p + (r_new - r_old),   m1 <- r0 . r_new,
+// so p is the direction the iteration would have formed from the new r, and the search
+// directions are kept (a refinement step starts the Krylov space again). The solve stops
+// only on the FP64 test ||b - A x|| <= tol ||b||, checked at a replacement.
+struct RState {
+    double sigma;      // scale of the FP32 vectors: ||b - A x0||
+    double inv_sigma;  // 1 / sigma
+    double goal;       // the FP64 target on ||b - A x||: tol ||b||
+    double delta;      // replace when ||r|| < delta * rmax
+    double rmax;       // largest recurrence ||r|| (scaled) since the last replacement
+    double true_r;     // ||b - A x|| at the last replacement
+    int update;        // replace at the end of this body
+    int verify;        // the recurrence met the target: the replacement decides the stop
+    int replacements, verifies, max_verify;
+};
+
+// FinControl's tests (AFIIM/src/bicgstab.cpp:201-277) with the recurrence's convergence
+// test turned into a request for a replacement (the FP64 residual decides the stop), and
+// the replacement trigger: ||r|| below delta times its running maximum.
+struct FinControlR {
+    RState *rs;
+    __device__ void finish(DState *st, const double *t) const {
+        const double a = st->alpha, om = st->omega;
+        if (fabs(a) * sqrt(st->pc2) < st->eps * sqrt(st->x2)) st->stag++;
+        else st->stag = 0;
+        const double prc = st->rc;
+        st->rc = sqrt(st->r2);
+        if (prc < st->rc) st->msteps++;
+        else st->msteps = 0;
+        if (st->msteps >= st->maxmsteps) { st->info = 1; st->done = 1; return; }
+        if (st->stag >= 3) { st->info = 2; st->done = 1; return; }
+        st->m2 = st->m1;
+        st->m1 = t[0];
+        st->beta = st->m1 * a / (om * st->m2);
+        st->iter++;
+        rs->rmax = fmax(rs->rmax, st->rc);
+        if (st->rc < st->tol * st->ro) {
+            rs->update = 1;
+            rs->verify = 1;
+        } else if (st->rc < rs->delta * rs->rmax) {
+            rs->update = 1;
+        }
+        if (st->iter >= st->nmax) { st->info = 3; st->done = 1; }
+    }
+};
+
+// p = r + beta (p - omega v), the last kernel of the body. cond bit 1: block 0 sets the IF
+// node's condition (a replacement follows); bit 0 (the device-driven loop): it also counts
+// the body, trips the guard (info -5) past nmax + 2 bodies and sets the WHILE node's
+// condition. cond = 0 outside a graph: no condition is set.
+static __global__ void __launch_bounds__(kThreads)
+k_update_p_r(long n, const float *__restrict__ r, const float *__restrict__ v, float *__restrict__ p,
+             DState *st, const RState *rs, cudaGraphConditionalHandle hw, cudaGraphConditionalHandle hif,
+             int cond) {
+    pdl_enter();
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (cond & 1) {   // inside the WHILE node's body
+            const int loops = ++st->loops;
+            if (!st->done && loops > st->nmax + 2) {
+                st->info = -5;
+                st->done = 1;
+            }
+            cudaGraphSetConditional(hw, st->done ? 0u : 1u);
+        }
+        if (cond & 2) cudaGraphSetConditional(hif, (!st->done && rs->update) ? 1u : 0u);   // the IF node follows
+    }
+    if (st->done) return;
+    const float b = (float)st->beta, c = (float)(-st->beta * st->omega);
+    FIIM_FOR_ROWS(i, n) { p[i] = fmaf(c, v[i], fmaf(b, p[i], r[i])); }
+}
+
+// Replacement, first half: x += sigma e (FP64), e = 0.
+static __global__ void __launch_bounds__(kThreads)
+k_replace_x(long n, float *__restrict__ e, double *__restrict__ x, const RState *rs) {
+    pdl_enter();
+    const double scale = rs->sigma;
+    FIIM_FOR_ROWS(i, n) {
+        x[i] += scale * (double)e[i];
+        e[i] = 0.f;
+    }
+}
+
+// Replacement, second half: the epilogue of the FP64 product A x. Per row, the true
+// residual b - A x (FP64), the new scaled FP32 residual, p moved by the change in r; sums
+// ||b - A x||^2 and r0 . r_new. The finish sets m1, restarts the running maximum, and at a
+// verification ends the solve when the FP64 target is met (or after max_verify attempts).
+struct EpiReplace {
+    FIIM_EPI(2, true, false);
+    const double *__restrict__ b;
+    float *r;
+    float *p;
+    const float *__restrict__ r0;
+    RState *rs;
+    __device__ void emit(long i, double s, double (&red)[NR]) const {
+        const double rt = b[i] - s;
+        const float rn = (float)(rt * rs->inv_sigma);
+        p[i] += rn - r[i];
+        r[i] = rn;
+        red[0] += rt * rt;
+        red[1] += (double)r0[i] * (double)rn;
+    }
+    __device__ void finish(DState *st, const double *t) const {
+        rs->true_r = sqrt(t[0]);
+        st->m1 = t[1];
+        rs->rmax = rs->true_r * rs->inv_sigma;
+        rs->update = 0;
+        rs->replacements++;
+        if (rs->verify) {
+            rs->verify = 0;
+            rs->verifies++;
+            if (rs->true_r <= rs->goal) {
+                st->info = 0;
+                st->done = 1;
+            } else if (rs->verifies >= rs->max_verify) {
+                st->info = 3;
+                st->done = 1;
+            }
+        }
+    }
+};
 
 // x += ||r64|| e (FP64): the refinement step.
 static __global__ void __launch_bounds__(kThreads)

@@ -65,7 +65,7 @@ class Options(C.Structure):
     _fields_ = [("variant", C.c_int), ("issym", C.c_int), ("precision", C.c_int), ("memory", C.c_int),
                 ("mode", C.c_char), ("nr", C.c_int), ("autotune", C.c_int), ("verbose", C.c_int),
                 ("inner_tol", C.c_double), ("inner_nmax", C.c_int), ("max_refine", C.c_int),
-                ("verified", C.c_int), ("max_restarts", C.c_int)]
+                ("verified", C.c_int), ("max_restarts", C.c_int), ("reliable", C.c_double)]
 
 
 class Result(C.Structure):
@@ -186,7 +186,8 @@ class Solver(_Handle):
     Arrays are numpy (memory='host') or torch CUDA tensors (memory='device')."""
 
     def __init__(self, A, F, variant="afiim", issym=False, precision="fp64", mode="E", nr=1,
-                 autotune=False, memory="host", verbose=0, inner_tol=1e-5, inner_nmax=1000, max_refine=50):
+                 autotune=False, memory="host", verbose=0, inner_tol=1e-5, inner_nmax=1000, max_refine=50,
+                 reliable=None):
         self._h = C.c_void_p(0)
         o = Options()
         lib().fiim_options_default(C.byref(o))
@@ -201,6 +202,8 @@ class Solver(_Handle):
         o.inner_tol = inner_tol
         o.inner_nmax = inner_nmax
         o.max_refine = max_refine
+        if reliable is not None:
+            o.reliable = reliable
         self.memory = memory
         conv = (lambda a, ints: a) if memory == "device" else (lambda a, ints: None if a is None else (_i(a) if ints else _d(a)))
         self._keep = []

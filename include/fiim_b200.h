@@ -114,9 +114,16 @@ typedef struct {
                        /* BiCGSTAB from its current x (masked, the others stay finished);   */
                        /* 0 (default): the recurrence test alone, as the reference stops    */
     int max_restarts;  /* verified: restart rounds cap (default 4)                         */
+    double reliable;   /* mixed: delta in (0, 1) (default 0.01) = one FP32 BiCGSTAB whose  */
+                       /* residual is replaced by the FP64 b - A x whenever it falls below  */
+                       /* delta times its largest value since the last replacement         */
+                       /* (reliable updates; the stop is the FP64 test, at most max_refine  */
+                       /* verifications; inner_tol and inner_nmax unused); 0 = refinement   */
+                       /* steps, each restarting the inner BiCGSTAB                        */
 } fiim_options;
 
-/* Defaults: FIIM_AFIIM, FP64, host memory, mode 'E', nr 1, autotune 0, verified 0. */
+/* Defaults: FIIM_AFIIM, FP64, host memory, mode 'E', nr 1, autotune 0, verified 0,
+ * reliable 0.01. */
 void fiim_options_default(fiim_options *opt);
 
 typedef struct {
@@ -124,7 +131,8 @@ typedef struct {
     double true_relres;   /* ||b - A x|| / ||b|| recomputed in FP64 after the solve              */
     int iter;             /* iterations (outer+inner total for mixed precision)                  */
     int info;             /* 0 converged, 1 diverged, 2 stagnated, 3 NMAX / non-finite alpha     */
-    int refine_steps;     /* mixed precision: outer refinement steps taken                       */
+    int refine_steps;     /* mixed precision: residual replacements (reliable updates) or outer  */
+                          /* refinement steps taken                                              */
     double device_ms;     /* device time of the solve, CUDA events on the solve stream           */
     int launches;         /* kernels this solve launched (graph nodes included)                  */
 } fiim_result;

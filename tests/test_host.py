@@ -92,6 +92,7 @@ int main(void) {
     fiim_options o;
     fiim_options_default(&o);
     if (o.variant != FIIM_AFIIM || o.precision != FIIM_FP64 || o.mode != 'E') return 1;
+    if (o.reliable != 0.01 || o.max_refine != 50 || o.verified != 0) return 1;
     long nnz = fiim_gen_poisson2d(8, 8, NULL, NULL, NULL);
     int *Ai = malloc(sizeof(int) * 65), *Aj = malloc(sizeof(int) * nnz);
     double *Av = malloc(sizeof(double) * nnz);
@@ -130,6 +131,15 @@ def test_c_program_builds_and_calls_the_library(tmp_path):
     A = FB.gen_poisson2d(8)
     F = FB.pdfiim_build(A, 0.05, 2, 2, 1)
     assert nnz == len(A[1]) and ng == len(F["Gj"]) and nh == len(F["Hj"])
+
+
+def test_options_layout_matches_the_header():
+    """The ctypes mirror of fiim_options reads the C defaults field for field."""
+    o = FB.Options()
+    FB.lib().fiim_options_default(C.byref(o))
+    assert (o.variant, o.precision, o.memory, o.mode, o.nr) == (FB._VARIANTS["afiim"], FB.FP64, FB.MEM_HOST, b"E", 1)
+    assert (o.inner_tol, o.inner_nmax, o.max_refine) == (1e-5, 1000, 50)
+    assert (o.verified, o.max_restarts, o.reliable) == (0, 4, 0.01)
 
 
 def test_bad_arguments_rejected_before_device():
