@@ -280,7 +280,7 @@ int fiim_solver_spmv_shape(fiim_solver_t h, int which, int *tile, int *form) {
     const fiim::DevCsr *m[] = {&s->A, &s->G, &s->H, &s->L, &s->U};
     if (which < 0 || which > 4) return fiim::set_error(FIIM_EARG, "which in 0..4 (A, G, H, L, U)");
     *tile = m[which]->tile;
-    *form = m[which]->form;
+    *form = m[which]->dia ? fiim::kFormDia : m[which]->form;
     return FIIM_OK;
 }
 

@@ -47,10 +47,11 @@ struct Arena {
     static size_t need(size_t bytes);
 };
 
-// Forms of the CSR-stream SpMV. Both give the same bits; they differ in how a row block's
-// streams reach shared memory: through registers, pipelined by one block (fiim_kernels.cuh),
-// or by bulk copies into two buffers (fiim_pipe.cuh).
-constexpr int kFormRows = 0, kFormBulk = 1, kFormWarp = 2;
+// Forms of the solver's SpMV. All give the same bits. The CSR-stream forms differ in how a
+// row block's streams reach shared memory: through registers, pipelined by one block
+// (kFormRows, fiim_kernels.cuh), by bulk copies into two buffers (kFormBulk, fiim_pipe.cuh),
+// or per warp (kFormWarp); kFormDia reads the sliced-diagonal copy of the values instead.
+constexpr int kFormRows = 0, kFormBulk = 1, kFormWarp = 2, kFormDia = 3;
 
 // A CSR matrix resident on the device. v holds FP64 values; v32 / v16 are optional
 // FP32 / BF16 copies for the mixed-precision inner solve.
@@ -70,6 +71,17 @@ struct DevCsr {
     int *wide = nullptr;         // device flag written by the narrow-stream builder
     int narrow = 0;              // 1: the CSR-stream SpMV reads cd / cb instead of ci
     int nblk = 0;
+    // Sliced-diagonal copy (kFormDia; fiim_kernels.cuh, k_spmv_dia), in its own allocation.
+    int dia = 0;                 // 1: built and current
+    int nsl = 0;                 // slices of 32 rows
+    int drs = 0;                 // ints per slice record (16 or 32): first diagonal, count, offsets
+    long ndiag = 0;              // diagonals over all slices (32 slots each)
+    int *drec = nullptr;         // nsl records
+    int *dmap = nullptr;         // nnz: the slot of each entry
+    int *dbad = nullptr;         // device flag of the structure check and value placement
+    double *dv = nullptr;        // 32 * ndiag values
+    void *dia_mem = nullptr;
+    size_t dia_bytes = 0;        // size of that allocation
     std::vector<int> hrp;        // row offsets on the host (row blocks, tuning key)
     bool rows_same = false;      // the last upload_csr found the same row offsets as before
     std::vector<long> sig;       // tuning-cache key: n, nnz, sampled row offsets
@@ -119,6 +131,14 @@ int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, con
 int set_tile(DevCsr &M, int tile, cudaStream_t s);
 // Builds the narrow column stream (cd, cb) of M's row blocks (eb) when every block allows it.
 int build_narrow(DevCsr &M, cudaStream_t s);
+// Builds the sliced-diagonal copy of M (M.dia = 1) when its rows are sorted by column, every
+// slice of 32 rows has at most kDiaMaxDiags diagonals and the copy moves fewer bytes than the
+// narrow CSR streams; otherwise M.dia = 0. refresh_dia, after new values (and possibly new
+// columns) were uploaded with the same row offsets, re-places the values when the columns
+// still fit the diagonals and rebuilds otherwise. release_dia frees the copy.
+int build_dia(DevCsr &M, cudaStream_t s);
+int refresh_dia(DevCsr &M, cudaStream_t s);
+void release_dia(DevCsr &M);
 void expand_sym_upper(int n, const int *rp, const int *ci, const double *v, HostCsr &out);
 void transpose_upper(int n, const int *rp, const int *ci, const double *v, HostCsr &out);
 

@@ -626,6 +626,81 @@ k_narrow_cols(const int *__restrict__ ci, const int *__restrict__ eb, int nblk, 
     }
 }
 
+// ---------------------------------------------------------------- sliced-diagonal SpMV
+// The sliced-diagonal form of a CSR matrix whose rows, 32 at a time, share a few diagonals:
+// slice s holds rows 32 s .. 32 s + 31 and the union of their entries' diagonals d = col -
+// row, ascending; each diagonal stores one value per row of the slice (v[32 k + lane], k
+// counted over all slices). A row's own entries keep their storage order (rows are sorted by
+// column), and a slot the row has no entry in holds kDiaPad, a NaN bit pattern that no entry
+// of the matrix holds (checked when the values are placed). Each slice has a record of rs
+// ints (16 or 32): its first diagonal k0, its count m and its m offsets, which a warp reads
+// in one coalesced load. Bytes per entry: 8 (FP64 value) and the padding, plus 2 or 4 per row
+// for the records, against 10 or 12 per entry and 4 per row for the CSR streams.
+constexpr unsigned long long kDiaPad = 0xFFF7D1A6B00C5A1DULL;
+constexpr int kDiaMaxDiags = 30;   // diagonals of one slice at most (record of 32 ints)
+constexpr int kDiaChunk = 8;       // diagonals in flight per thread
+
+struct DiaView {
+    const int *__restrict__ rec;      // nsl records of rs ints: k0, m, offsets
+    const double *__restrict__ v;     // 32 values per diagonal
+    int n, nsl, rs;
+};
+
+// One warp per slice, lane = row, grid-stride over slices; the next slice's record is loaded
+// while the current slice is summed. A thread sums its row in storage order exactly as the
+// CSR-stream kernels do (from 0.0, __dmul_rn then __dadd_rn, padding skipped), so every form
+// gives the same bits. The gathers of a chunk are issued with its value loads (padding slots
+// read a clamped column and are not used); lanes read consecutive values and, on a banded
+// matrix, consecutive x.
+template <typename Epi>
+static __global__ void __launch_bounds__(kThreads)
+k_spmv_dia(DiaView M, const double *__restrict__ x, Epi epi, DState *st, double *__restrict__ partials) {
+    pdl_enter();
+    if (Epi::GATED && st != nullptr && st->done) return;
+    double red[Epi::NR];
+#pragma unroll
+    for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
+    const int lane = (int)threadIdx.x & 31;
+    const int nw = (int)gridDim.x * kWarps;
+    const unsigned full = 0xffffffffu;
+    int sl = (int)blockIdx.x * kWarps + ((int)threadIdx.x >> 5);
+    int rec = (sl < M.nsl && lane < M.rs) ? __ldg(M.rec + (long)sl * M.rs + lane) : 0;
+    for (; sl < M.nsl; sl += nw) {
+        const int nxt = sl + nw;
+        const int rec_next = (nxt < M.nsl && lane < M.rs) ? __ldg(M.rec + (long)nxt * M.rs + lane) : 0;
+        const int row = (sl << 5) + lane;
+        const bool live = row < M.n;
+        double opnd = 0.0;
+        if constexpr (HasPre<Epi>::value) opnd = live ? epi.pre(row) : 0.0;
+        const int k0 = __shfl_sync(full, rec, 0), m = __shfl_sync(full, rec, 1);
+        double s = 0.0;
+        for (int k = 0; k < m; k += kDiaChunk) {
+            double a[kDiaChunk], xv[kDiaChunk];
+#pragma unroll
+            for (int u = 0; u < kDiaChunk; ++u) {
+                a[u] = 0.0;
+                xv[u] = 0.0;
+                const int d = __shfl_sync(full, rec, (2 + k + u) & 31);
+                if (k + u < m) {
+                    a[u] = ldm(M.v + ((long)(k0 + k + u) << 5) + lane);
+                    xv[u] = ldx(x + min(max(row + d, 0), M.n - 1));
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kDiaChunk; ++u)
+                if (k + u < m && (unsigned long long)__double_as_longlong(a[u]) != kDiaPad)
+                    s = __dadd_rn(s, __dmul_rn(a[u], xv[u]));
+        }
+        if (live) {
+            if constexpr (HasPre<Epi>::value) epi.emit_pre(row, s, opnd, red);
+            else epi.emit(row, s, red);
+        }
+        rec = rec_next;
+    }
+    pdl_release();
+    if constexpr (Epi::REDUCES) grid_reduce<Epi::NR>(red, partials, st, epi);
+}
+
 // ---------------------------------------------------------------- CSR-vector SpMV
 // For callers without set-up (the kernel-level C-ABI): VEC lanes per row, 32/VEC rows
 // per warp, grid-stride over row groups. Each lane rounds its product; the group then
@@ -820,6 +895,47 @@ static __global__ void k_count_outside(int n, const int *__restrict__ rp, const 
         }
     }
     if (c) atomicAdd(count, c);
+}
+
+// Sliced-diagonal values: every slot padding, then each entry e moved to its slot map[e]
+// (slots = 32 x diagonals); *bad is set when an entry holds the padding's bit pattern.
+template <typename T>
+static __global__ void __launch_bounds__(kThreads)
+k_dia_fill(long slots, T *__restrict__ dv, T pad) {
+    FIIM_FOR_ROWS(i, slots) { dv[i] = pad; }
+}
+template <typename TI, typename TO, typename Conv>
+static __global__ void __launch_bounds__(kThreads)
+k_dia_scatter(long nnz, const TI *__restrict__ v, const int *__restrict__ map, TO *__restrict__ dv, Conv conv,
+              int *bad) {
+    FIIM_FOR_ROWS(e, nnz) {
+        const TO o = conv(v[e]);
+        if (Conv::is_pad(o)) atomicExch(bad, 1);
+        dv[map[e]] = o;
+    }
+}
+struct DiaConv64 {
+    __device__ double operator()(double v) const { return v; }
+    __device__ static bool is_pad(double v) { return (unsigned long long)__double_as_longlong(v) == kDiaPad; }
+};
+
+// Whether new column indices (with unchanged row offsets) still fit the slices' diagonals:
+// entry e of row i must sit in slot map[e] = 32 k + i % 32 of a diagonal k of slice i / 32
+// (k0 <= k < k0 + m) whose offset is ci[e] - i. *bad is set otherwise. One thread per row.
+static __global__ void __launch_bounds__(kThreads)
+k_dia_check(int n, const int *__restrict__ rp, const int *__restrict__ ci, const int *__restrict__ map,
+            const int *__restrict__ rec, int rs, int *bad) {
+    FIIM_FOR_ROWS(i, (long)n) {
+        const int *r = rec + (i >> 5) * rs;
+        const int lane = (int)(i & 31), k0 = r[0], m = r[1];
+        for (int e = rp[i]; e < rp[i + 1]; ++e) {
+            const int slot = map[e], k = (slot >> 5) - k0;
+            if ((slot & 31) != lane || k < 0 || k >= m || r[2 + k] != ci[e] - (int)i) {
+                atomicExch(bad, 1);
+                break;
+            }
+        }
+    }
 }
 
 }  // namespace fiim

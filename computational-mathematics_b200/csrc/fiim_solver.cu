@@ -193,11 +193,22 @@ static cudaError_t spmv_warp(cudaStream_t s, const DevCsr &M, const double *x, c
     return launch_k(kern, g, 0, s, view(M), M.rb, M.eb, M.nblk, x, epi, st, partials, NarrowCols{});
 }
 
-// Solver SpMV: CSR-stream over the matrix's row blocks, exact row order, in the form and
-// row-block size the tuner chose. Every form gives the same bits.
+// Sliced-diagonal SpMV: kWarps slices per CTA.
+template <typename Epi>
+static cudaError_t spmv_dia(cudaStream_t s, const DevCsr &M, const double *x, const Epi &epi, DState *st,
+                            double *partials) {
+    auto kern = k_spmv_dia<Epi>;
+    const int g = grid_for(kern, kWarps, M.nsl);
+    return launch_k(kern, g, 0, s, DiaView{M.drec, M.dv, (int)M.n, M.nsl, M.drs}, x, epi, st, partials);
+}
+
+// Solver SpMV: the sliced-diagonal copy where the matrix has one, else CSR-stream over the
+// matrix's row blocks, in the form and row-block size the tuner chose. Every form gives the
+// same bits.
 template <typename Epi>
 cudaError_t launch_spmv(const DevCsr &M, cudaStream_t s, const double *x, const Epi &epi, DState *st,
                         double *partials, int *fault = nullptr) {
+    if (M.dia) return spmv_dia(s, M, x, epi, st, partials);
     if (M.form == kFormWarp) return spmv_warp(s, M, x, epi, st, partials);
     if (M.form == kFormBulk && fault) {
         if (M.tile == 1024) return spmv_pipe<1024>(s, M, x, epi, st, partials, fault);
@@ -256,6 +267,144 @@ int build_narrow(DevCsr &M, cudaStream_t s) {
         M.narrow = wide ? 0 : 1;
     }
     return FIIM_OK;
+}
+
+void release_dia(DevCsr &M) {
+    if (M.dia_mem) cudaFree(M.dia_mem);
+    M.dia_mem = nullptr;
+    M.dia_bytes = 0;
+    M.drec = M.dmap = M.dbad = nullptr;
+    M.dv = nullptr;
+    M.dia = 0;
+    M.nsl = 0;
+    M.drs = 0;
+    M.ndiag = 0;
+}
+
+// Padding in every slot, then each entry in its own; keeps the copy only if no entry holds
+// the padding's bit pattern.
+static int place_dia_values(DevCsr &M, cudaStream_t s) {
+    FIIM_CUDA(cudaMemsetAsync(M.dbad, 0, sizeof(int), s));
+    const long slots = 32 * M.ndiag;
+    double pad;
+    std::memcpy(&pad, &kDiaPad, sizeof pad);
+    k_dia_fill<double><<<stream_grid(k_dia_fill<double>, slots), kThreads, 0, s>>>(slots, M.dv, pad);
+    FIIM_CUDA(cudaGetLastError());
+    auto scat = k_dia_scatter<double, double, DiaConv64>;
+    scat<<<stream_grid(scat, M.nnz), kThreads, 0, s>>>(M.nnz, M.v, M.dmap, M.dv, DiaConv64{}, M.dbad);
+    FIIM_CUDA(cudaGetLastError());
+    int bad = 0;
+    FIIM_CUDA(cudaMemcpyAsync(&bad, M.dbad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FIIM_CUDA(cudaStreamSynchronize(s));
+    if (bad) release_dia(M);
+    else M.dia = 1;
+    return FIIM_OK;
+}
+
+int build_dia(DevCsr &M, cudaStream_t s) {
+    release_dia(M);
+    // FIIM_SPMV=rows / staged / warp keep a CSR-stream form; FIIM_DIA=0 never builds the copy.
+    const char *force = std::getenv("FIIM_SPMV"), *off_env = std::getenv("FIIM_DIA");
+    if ((force && std::strcmp(force, "dia") != 0) || (off_env && std::strcmp(off_env, "0") == 0)) return FIIM_OK;
+    const int n = (int)M.n;
+    const long nnz = M.nnz;
+    if (n <= 0 || nnz <= 0 || (long)M.hrp.size() != (long)n + 1) return FIIM_OK;
+    std::vector<int> ci(nnz);
+    FIIM_CUDA(cudaMemcpyAsync(ci.data(), M.ci, sizeof(int) * nnz, cudaMemcpyDeviceToHost, s));
+    FIIM_CUDA(cudaStreamSynchronize(s));
+    const int *rp = M.hrp.data();
+    const int nsl = (n + 31) / 32;
+    // The diagonals of a slice: its entries' col - row, sorted and distinct.
+    auto diagonals = [&](int sl, std::vector<int> &d, int &unsorted) {
+        d.clear();
+        const int r0 = sl * 32, r1 = std::min(n, r0 + 32);
+        for (int i = r0; i < r1; ++i)
+            for (int e = rp[i]; e < rp[i + 1]; ++e) {
+                if (e > rp[i] && ci[e] <= ci[e - 1]) unsorted = 1;
+                d.push_back(ci[e] - i);
+            }
+        std::sort(d.begin(), d.end());
+        d.erase(std::unique(d.begin(), d.end()), d.end());
+    };
+    std::vector<int> sp(nsl + 1, 0);
+    int fail = 0;
+#pragma omp parallel
+    {
+        std::vector<int> d;
+        int bad = 0;
+#pragma omp for schedule(dynamic, 256)
+        for (int sl = 0; sl < nsl; ++sl) {
+            diagonals(sl, d, bad);
+            sp[sl + 1] = (int)d.size();
+            if ((int)d.size() > kDiaMaxDiags) bad = 1;
+        }
+#pragma omp atomic
+        fail |= bad;
+    }
+    if (fail) return FIIM_OK;
+    int most = 0;
+    for (int sl = 0; sl < nsl; ++sl) {
+        most = std::max(most, sp[sl + 1]);
+        sp[sl + 1] += sp[sl];
+    }
+    const long ndiag = sp[nsl];
+    const int rs = most <= 14 ? 16 : 32;
+    // Kept only when it moves fewer bytes than the CSR streams it replaces.
+    const double dia_bytes = 8.0 * 32 * ndiag + 4.0 * rs * nsl;
+    const double csr_bytes_now = (double)nnz * (8 + (M.narrow ? 2 : 4)) + 4.0 * (n + 1);
+    if (!(dia_bytes < csr_bytes_now) || 32 * ndiag >= (1L << 31)) return FIIM_OK;
+    std::vector<int> rec((size_t)nsl * rs, 0), map(nnz);
+#pragma omp parallel
+    {
+        std::vector<int> d;
+        int unused = 0;
+#pragma omp for schedule(dynamic, 256)
+        for (int sl = 0; sl < nsl; ++sl) {
+            diagonals(sl, d, unused);
+            int *r = rec.data() + (size_t)sl * rs;
+            r[0] = sp[sl];
+            r[1] = (int)d.size();
+            std::copy(d.begin(), d.end(), r + 2);
+            const int r0 = sl * 32, r1 = std::min(n, r0 + 32);
+            for (int i = r0; i < r1; ++i)
+                for (int e = rp[i]; e < rp[i + 1]; ++e) {
+                    const int k = (int)(std::lower_bound(d.begin(), d.end(), ci[e] - i) - d.begin());
+                    map[e] = 32 * (sp[sl] + k) + (i & 31);
+                }
+        }
+    }
+    const size_t b_rec = Arena::need(sizeof(int) * rec.size()), b_map = Arena::need(sizeof(int) * nnz),
+                 b_bad = Arena::need(sizeof(int)), b_v = Arena::need(sizeof(double) * 32 * ndiag);
+    char *mem = nullptr;
+    if (cudaMalloc(&mem, b_rec + b_map + b_bad + b_v) != cudaSuccess) {
+        cudaGetLastError();
+        return FIIM_OK;   // no room for the copy: the CSR streams serve
+    }
+    M.dia_mem = mem;
+    M.dia_bytes = b_rec + b_map + b_bad + b_v;
+    M.drec = reinterpret_cast<int *>(mem);
+    M.dmap = reinterpret_cast<int *>(mem + b_rec);
+    M.dbad = reinterpret_cast<int *>(mem + b_rec + b_map);
+    M.dv = reinterpret_cast<double *>(mem + b_rec + b_map + b_bad);
+    M.nsl = nsl;
+    M.drs = rs;
+    M.ndiag = ndiag;
+    FIIM_CUDA(cudaMemcpyAsync(M.drec, rec.data(), sizeof(int) * rec.size(), cudaMemcpyHostToDevice, s));
+    FIIM_CUDA(cudaMemcpyAsync(M.dmap, map.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, s));
+    return place_dia_values(M, s);   // synchronizes before the host arrays go
+}
+
+int refresh_dia(DevCsr &M, cudaStream_t s) {
+    if (!M.dia) return FIIM_OK;
+    FIIM_CUDA(cudaMemsetAsync(M.dbad, 0, sizeof(int), s));
+    k_dia_check<<<stream_grid(k_dia_check, M.n), kThreads, 0, s>>>((int)M.n, M.rp, M.ci, M.dmap, M.drec, M.drs,
+                                                                   M.dbad);
+    FIIM_CUDA(cudaGetLastError());
+    int bad = 0;
+    FIIM_CUDA(cudaMemcpyAsync(&bad, M.dbad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    FIIM_CUDA(cudaStreamSynchronize(s));
+    if (bad) return build_dia(M, s);
+    return place_dia_values(M, s);
 }
 
 int set_tile(DevCsr &M, int tile, cudaStream_t s) {
@@ -872,6 +1021,7 @@ int Solver::create(int n_, const int *Ai, const int *Aj, const double *Av, const
                 FIIM_TRY(set_tile(M, default_tile(M), stream));
             }
         }
+        FIIM_TRY(build_dia(M, stream));   // serves the products where the matrix allows it
     }
     {
         // FIIM_PERSIST=1: systems of at most kPersistMaxN rows solve as one cooperative launch.
@@ -946,15 +1096,23 @@ int Solver::reload(const int *Ai, const int *Aj, const double *Av, const int *Gi
         FIIM_TRY(upload_all(mats, caps, rps, cis, vs, fills, dev, combined ? 5 : 3, n, stream, d_count, h_count,
                              &stager));
     }
-    // Row blocks follow the new row offsets (rebuilt only where they changed); the graph
-    // bakes in each block count.
+    // Row blocks follow the new row offsets (rebuilt only where they changed); the narrow
+    // column stream follows the new column indices (rebuilt for every matrix: the same row
+    // offsets may hold other columns). The graph bakes in each block count and stream width.
     bool regraph = false;
     DevCsr *mats[] = {&A, &G, &H, &L, &U};
     for (int k = 0; k < (combined ? 5 : 3); ++k) {
-        if (mats[k]->rows_same && mats[k]->nblk > 0) continue;
-        const int old = mats[k]->nblk;
-        FIIM_TRY(set_tile(*mats[k], mats[k]->tile, stream));
-        regraph |= (mats[k]->nblk != old);
+        DevCsr &M = *mats[k];
+        const int old = M.nblk, was_narrow = M.narrow, was_dia = M.dia;
+        const void *was_mem = M.dia_mem;   // a rebuilt copy has new addresses
+        if (M.rows_same && M.nblk > 0) {
+            FIIM_TRY(build_narrow(M, stream));
+            FIIM_TRY(refresh_dia(M, stream));
+        } else {
+            FIIM_TRY(set_tile(M, M.tile, stream));
+            FIIM_TRY(build_dia(M, stream));
+        }
+        regraph |= (M.nblk != old) || (M.narrow != was_narrow) || (M.dia != was_dia) || (M.dia_mem != was_mem);
     }
     if (regraph) FIIM_TRY(build_graph());
     return FIIM_OK;
@@ -1130,6 +1288,7 @@ void Solver::destroy() {
     if (hst) cudaFreeHost(hst);
     hst = nullptr;
     stager.release();
+    for (DevCsr *M : {&A, &G, &H, &L, &U}) release_dia(*M);
     arena.release();
 }
 

@@ -68,7 +68,9 @@ struct Solver : SolverBase {
     bool stall_next = false;     // test hook: the next solve's first barrier never completes
     int launch_persistent();
     void destroy();
-    size_t device_bytes() const { return arena.cap; }
+    size_t device_bytes() const {   // the arena and the sliced-diagonal copies
+        return arena.cap + A.dia_bytes + G.dia_bytes + H.dia_bytes + L.dia_bytes + U.dia_bytes;
+    }
 
     int enqueue_prec(const double *in, double *out, bool norm);
     int enqueue_iteration(bool cond, cudaGraphConditionalHandle h);

@@ -88,6 +88,129 @@ def test_solver_products_bit_identical(golden, monkeypatch, name, prefix, varian
     S.close()
 
 
+def dia_bytes(rp, ci):
+    """Bytes of the sliced-diagonal copy of a CSR matrix (slices of 32 rows, 8 bytes per slot
+    of each slice's diagonals, a record of 16 or 32 ints per slice), or None when a row is
+    unsorted or a slice has more than 30 diagonals."""
+    n = len(rp) - 1
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    if np.any((np.diff(ci) <= 0) & (np.diff(rows) == 0)):
+        return None
+    d = ci.astype(np.int64) - rows
+    key = np.unique((rows // 32) * (4 * n) + (d + 2 * n))
+    per = np.bincount(key // (4 * n), minlength=(n + 31) // 32)
+    if per.max() > 30:
+        return None
+    nd = int(per.sum())
+    return 8.0 * 32 * nd + 4.0 * (16 if per.max() <= 14 else 32) * len(per)
+
+
+@pytest.mark.parametrize("name,prefix,variant", [("sherman2", "afiim9e-6_", "afiim"), ("poisson128_afiim", "", "afiim"),
+                                                 ("convdiff16_pdfiim", "", "pdfiim"),
+                                                 ("convdiff2d48_acifim", "", "acifim")])
+def test_dia_form_products_bit_identical(golden, name, prefix, variant):
+    """By default the solver reads the sliced-diagonal copy of each matrix whose rows allow it
+    (form 3) and the CSR streams otherwise; A x and M x equal the oracle's bit for bit."""
+    g = golden(name)
+    F = sub(g, prefix)
+    A = (g["Ai"], g["Aj"], g["Av"])
+    S = FB.Solver(A, F, variant=variant)
+    n = len(g["b"])
+    for which, (rp, ci) in enumerate([(A[0], A[1]), (F["Gi"], F["Gj"]), (F["Hi"], F["Hj"])]):
+        db = dia_bytes(rp, ci)
+        nnz = len(ci)
+        form = S.spmv_shape(which)[1]
+        if db is None or db >= nnz * 12 + 4 * (n + 1):
+            assert form != 3
+        elif db < nnz * 10 + 4 * (n + 1):
+            assert form == 3
+    assert np.array_equal(S.apply(F["u"], np.zeros(n), op="A"), F["Au"])
+    assert np.array_equal(S.apply(F["u"], np.zeros(n), op="M"), F["Mu"])
+    S.close()
+
+
+def test_dia_form_on_the_headline_structure():
+    """The 3D convection-diffusion matrix and its PDFIIM factors take the sliced-diagonal form;
+    A x and M x equal the CSR streams' (FIIM_SPMV=rows) bit for bit. The solves differ only
+    through the fused dot products, whose summation tree follows the launch shape."""
+    A = FB.gen_convdiff3d(48, 0.5)
+    n = len(A[0]) - 1
+    F = FB.pdfiim_build(A, 0.05, 2, 2, 1, -1, "I", "B")
+    b = FB.rand_normal(n, 5)
+    u = FB.rand_normal(n, 6)
+    out = {}
+    for form in (None, "rows"):
+        env = os.environ.pop("FIIM_SPMV", None)
+        if form:
+            os.environ["FIIM_SPMV"] = form
+        try:
+            S = FB.Solver(A, F, variant="pdfiim")
+            forms = [S.spmv_shape(w)[1] for w in range(3)]
+            x = np.zeros(n)
+            r = S.solve(b, x, tol=1e-10, nmax=500)
+            out[form] = (forms, S.apply(u, np.zeros(n), op="A"), S.apply(u, np.zeros(n), op="M"), x, r["iter"])
+            S.close()
+        finally:
+            os.environ.pop("FIIM_SPMV", None)
+            if env is not None:
+                os.environ["FIIM_SPMV"] = env
+    assert out[None][0] == [3, 3, 3] and 3 not in out["rows"][0]
+    for k in (1, 2):
+        assert np.array_equal(out[None][k], out["rows"][k])
+    assert abs(out[None][4] - out["rows"][4]) <= 2
+    assert np.linalg.norm(out[None][3] - out["rows"][3]) <= 1e-7 * np.linalg.norm(out["rows"][3])
+
+
+def test_dia_form_refused_for_unsorted_rows_and_the_padding_pattern():
+    """Rows not sorted by column, and an entry holding the padding's bit pattern, keep the CSR
+    streams; the products stay the oracle's."""
+    A = FB.gen_convdiff3d(40, 0.5)
+    n = len(A[0]) - 1
+    F = identity_factors(n)
+    u = FB.rand_normal(n, 9)
+    Av = A[2].copy()
+    Aj = A[1].copy()
+    e = A[0][(5 * 40 + 5) * 40 + 5]          # the first entry of an interior row (7 entries)
+    Aj[[e, e + 1]] = Aj[[e + 1, e]]
+    Av[[e, e + 1]] = Av[[e + 1, e]]
+    S = FB.Solver((A[0], Aj, Av), F)
+    assert S.spmv_shape(0)[1] != 3
+    assert np.array_equal(S.apply(u, np.zeros(n), op="A"), O.csr_mv(A[0], Aj, Av, u))
+    S.close()
+    Av = A[2].copy()
+    Av[500] = np.frombuffer(np.uint64(0xFFF7D1A6B00C5A1D).tobytes(), dtype=np.float64)[0]
+    S = FB.Solver((A[0], A[1], Av), F)
+    assert S.spmv_shape(0)[1] != 3
+    y = S.apply(u, np.zeros(n), op="A")
+    ref = O.csr_mv(A[0], A[1], Av, u)
+    assert np.array_equal(np.isnan(y), np.isnan(ref)) and np.array_equal(y[~np.isnan(y)], ref[~np.isnan(ref)])
+    S.close()
+
+
+def test_dropin_reload_replaces_diagonal_values():
+    """A drop-in call with new values in the same structure re-places them in the existing
+    sliced-diagonal copy: the result equals a fresh solver's bit for bit."""
+    A = FB.gen_convdiff3d(40, 0.5)
+    n = len(A[0]) - 1
+    F = FB.pdfiim_build(A, 0.05, 2, 2, 1, -1, "I", "B")
+    G, H = (F["Gi"], F["Gj"], F["Gv"]), (F["Hi"], F["Hj"], F["Hv"])
+    b = FB.rand_normal(n, 13)
+    prev = FB.dropin_cache(True)
+    try:
+        for scale in (1.0, 1.25):
+            AA = (A[0], A[1], A[2] * scale)
+            x = np.zeros(n)
+            r = FB.EPBiCGSTAB_pdfiim(AA, b, 1e-10, 500, G, F["IDv"], H, x)
+            S = FB.Solver(AA, F, variant="pdfiim")
+            assert S.spmv_shape(0)[1] == 3
+            y = np.zeros(n)
+            r1 = S.solve(b, y, tol=1e-10, nmax=500)
+            S.close()
+            assert np.array_equal(x, y) and r[1] == r1["iter"]
+    finally:
+        FB.dropin_cache(prev)
+
+
 @pytest.mark.parametrize("form", [None, "staged", "warp"])
 @pytest.mark.parametrize("long_len", [0, 2046, 2047, 2048, 2500])
 def test_solver_spmv_random_rows(monkeypatch, long_len, form):
@@ -281,7 +404,7 @@ def test_dropin_solve_matches_reference(golden, name, fprefix, rprefix, variant,
     assert true_relres(g, x) <= 10 * true_relres(g, g[rprefix + "x"]) + 1e-12
 
 
-@pytest.mark.parametrize("form", ["rows", "staged", "warp"])
+@pytest.mark.parametrize("form", ["rows", "staged", "warp", "dia"])
 def test_solver_forms_agree_on_convdiff64(monkeypatch, form):
     """A 64^3 solve takes the same iterations and (to rounding) the same x with either SpMV form."""
     monkeypatch.setenv("FIIM_SPMV", form)
@@ -328,6 +451,32 @@ def test_dropin_reload_follows_row_structure():
             S = FB.Solver(AA, F, variant="pdfiim")
             y = np.zeros(n)
             r1 = S.solve(b, y, tol=1e-10, nmax=500)
+            S.close()
+            assert np.array_equal(x, y) and r[1] == r1["iter"]
+    finally:
+        FB.dropin_cache(prev)
+
+
+def test_dropin_reload_follows_column_indices():
+    """A drop-in call with the same row offsets as the previous one but other column indices
+    rebuilds the narrow column stream: its result equals a fresh solver's bit for bit. The
+    system (64,000 rows) takes the graph path, whose products read that stream."""
+    A = FB.gen_convdiff3d(40, 0.5)
+    n = len(A[0]) - 1
+    A2 = (A[0].copy(), ((A[1].astype(np.int64) + 977) % n).astype(np.int32), A[2].copy())
+    assert np.array_equal(A2[0], A[0]) and not np.array_equal(A2[1], A[1])
+    F = identity_factors(n)
+    G, H = (F["Gi"], F["Gj"], F["Gv"]), (F["Hi"], F["Hj"], F["Hv"])
+    b = FB.rand_normal(n, 11)
+    prev = FB.dropin_cache(False)
+    try:
+        for AA in (A, A2, A):
+            x = np.zeros(n)
+            r = FB.EPBiCGSTAB_pdfiim(AA, b, 1e-14, 25, G, F["IDv"], H, x)
+            S = FB.Solver(AA, F, variant="pdfiim")
+            assert S.mode() in (0, 1)
+            y = np.zeros(n)
+            r1 = S.solve(b, y, tol=1e-14, nmax=25)
             S.close()
             assert np.array_equal(x, y) and r[1] == r1["iter"]
     finally:
