@@ -798,6 +798,13 @@ def run_ours(args):
     h_ms = sum(h_seq) / len(h_seq) - ev_cost
     achieved = h_bytes / (h_ms / 1000.0) / 1e9
     h_alone = next(m for k, m, _ in ktimes if k == "H_spmv_scale")
+    # The bytes H's product reads in the form it is served in (the formula above counts 4-byte
+    # column indices and row offsets; the sliced-diagonal form reads neither), and the
+    # iteration's bytes on the same count.
+    form_names = {0: "CSR stream", 1: "CSR stream (bulk copies)", 2: "CSR stream (warp blocks)", 3: "sliced-diagonal"}
+    nvb = 8.0 * n
+    h_form = S.matrix_bytes(2) + 3 * nvb
+    it_form = 2 * sum(S.matrix_bytes(w) for w in range(3)) + 32 * nvb
     roofline = {"bound": "hbm", "kernel": "H_spmv_scale", "achieved": round(achieved, 1), "peak": peak,
                 "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "traffic": args.ncu_traffic, "algorithmic_bytes_per_launch": h_bytes, "launch_ms": round(h_ms, 5),
@@ -807,7 +814,13 @@ def run_ours(args):
                           "frac": round(h_bytes / (h_alone / 1000) / 1e9 / peak, 4)},
                 "per_kernel": [{"kernel": k, "ms": round(m, 5), "gbs": round(by / (m / 1000) / 1e9, 1)}
                                for k, m, by in ktimes],
-                "per_kernel_in_sequence": [{"kernel": k, "ms": round(m, 5)} for k, m, _ in seq]}
+                "per_kernel_in_sequence": [{"kernel": k, "ms": round(m, 5)} for k, m, _ in seq],
+                "form": form_names.get(S.spmv_shape(2)[1], "?"),
+                "form_bytes_per_launch": h_form,
+                "achieved_on_form_bytes": round(h_form / (h_ms / 1000) / 1e9, 1),
+                "frac_on_form_bytes": round(h_form / (h_ms / 1000) / 1e9 / peak, 4),
+                "iteration_form_bytes": it_form,
+                "hbm_frac_on_form_bytes": round(sum(iters) * it_form / (dev_ms / 1000.0) / 1e9 / peak, 4)}
     # FP64 to the mixed leg's target (1e-10), the reference x for its error
     x_ref10 = None
     if not args.no_mixed:
@@ -957,7 +970,7 @@ def main():
     # DRAM bytes per launch of the dominant kernel (H's SpMV) from an ncu capture of the
     # 128^3 workload (dram__bytes_read.sum + dram__bytes_write.sum, mean of three H launches:
     # 0.817 x its algorithmic bytes, the column stream being stored as 16-bit offsets).
-    ap.add_argument("--ncu-traffic", type=float, default=270.7e6,
+    ap.add_argument("--ncu-traffic", type=float, default=221.8e6,
                     help="dram bytes per launch of the dominant kernel from an ncu capture")
     ap.add_argument("--dry-run", action="store_true",
                     help="no GPU: check the rank launcher and max-over-ranks timing over gloo (solves nothing)")

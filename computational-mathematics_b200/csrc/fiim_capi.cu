@@ -328,6 +328,16 @@ double fiim_solver_iteration_bytes(fiim_solver_t h) {
     return reinterpret_cast<fiim::Solver *>(h)->iteration_bytes();
 }
 
+double fiim_solver_matrix_bytes(fiim_solver_t h, int which) {
+    if (!h || fiim_is_mixed(h) || which < 0 || which > 4) return -1.0;
+    auto *s = reinterpret_cast<fiim::Solver *>(h);
+    const fiim::DevCsr *m[] = {&s->A, &s->G, &s->H, &s->L, &s->U};
+    const fiim::DevCsr &M = *m[which];
+    if (M.dia) return 32.0 * M.dvbytes * (double)M.ndiag + 4.0 * M.drs * M.nsl;
+    return (double)M.nnz * (8 + (M.narrow ? 2 : 4)) + 4.0 * (M.n + 1) + (M.narrow ? 4.0 * M.nblk : 0.0) +
+           8.0 * (M.nblk + 1);
+}
+
 int fiim_solver_destroy(fiim_solver_t h) {
     if (!h) return FIIM_OK;
     if (fiim_is_mixed(h)) return fiim_mixed_destroy(h);

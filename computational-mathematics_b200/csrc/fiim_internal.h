@@ -79,9 +79,13 @@ struct DevCsr {
     int *drec = nullptr;         // nsl records
     int *dmap = nullptr;         // nnz: the slot of each entry
     int *dbad = nullptr;         // device flag of the structure check and value placement
-    double *dv = nullptr;        // 32 * ndiag values
+    void *dvals = nullptr;       // 32 * ndiag values of dvbytes bytes each (FP64, FP32 or BF16)
+    int dvbytes = 0;
     void *dia_mem = nullptr;
     size_t dia_bytes = 0;        // size of that allocation
+    bool dia_tried = false;      // the copy was considered for the columns hashed in dia_cols
+    unsigned long long dia_cols = 0;
+    unsigned long long *dhash = nullptr;   // device scratch of the column hash (in the arena)
     std::vector<int> hrp;        // row offsets on the host (row blocks, tuning key)
     bool rows_same = false;      // the last upload_csr found the same row offsets as before
     std::vector<long> sig;       // tuning-cache key: n, nnz, sampled row offsets
@@ -131,11 +135,22 @@ int upload_csr(DevCsr &M, long nnz_cap, int n, const int *rp, const int *ci, con
 int set_tile(DevCsr &M, int tile, cudaStream_t s);
 // Builds the narrow column stream (cd, cb) of M's row blocks (eb) when every block allows it.
 int build_narrow(DevCsr &M, cudaStream_t s);
-// Builds the sliced-diagonal copy of M (M.dia = 1) when its rows are sorted by column, every
-// slice of 32 rows has at most kDiaMaxDiags diagonals and the copy moves fewer bytes than the
-// narrow CSR streams; otherwise M.dia = 0. refresh_dia, after new values (and possibly new
-// columns) were uploaded with the same row offsets, re-places the values when the columns
-// still fit the diagonals and rebuilds otherwise. release_dia frees the copy.
+// The sliced-diagonal copy of M (fiim_kernels.cuh, k_spmv_dia). build_dia_structure lays it
+// out (slice records, the slot of every entry) for values of vbytes bytes (8, 4 or 2) when
+// M's rows are sorted by column, every slice of 32 rows has at most kDiaMaxDiags diagonals
+// and the copy moves fewer bytes than the CSR streams (M.dia_mem stays null otherwise);
+// place_dia moves the nnz values `vals` (device, that width) into it and sets M.dia = 1,
+// unless an entry holds the padding pattern (then the copy is released). dia_fits tells
+// whether M's current columns (same row offsets) still sit in the laid-out slots.
+// build_dia / refresh_dia do this for the FP64 values M.v: refresh_dia, after new values (and
+// possibly new columns) with the same row offsets, re-places the values when the columns
+// still fit and rebuilds otherwise. release_dia frees the copy; dia_wanted is false under
+// FIIM_DIA=0 or FIIM_SPMV=rows / staged / warp.
+bool dia_wanted();
+
+int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes);
+int place_dia(DevCsr &M, const void *vals, cudaStream_t s);
+int dia_fits(DevCsr &M, cudaStream_t s, bool *fits);
 int build_dia(DevCsr &M, cudaStream_t s);
 int refresh_dia(DevCsr &M, cudaStream_t s);
 void release_dia(DevCsr &M);

@@ -636,66 +636,116 @@ k_narrow_cols(const int *__restrict__ ci, const int *__restrict__ eb, int nblk, 
 // ints (16 or 32): its first diagonal k0, its count m and its m offsets, which a warp reads
 // in one coalesced load. Bytes per entry: 8 (FP64 value) and the padding, plus 2 or 4 per row
 // for the records, against 10 or 12 per entry and 4 per row for the CSR streams.
-constexpr unsigned long long kDiaPad = 0xFFF7D1A6B00C5A1DULL;
+constexpr unsigned long long kDiaPad = 0xFFF7D1A6B00C5A1DULL;   // FP64 padding; FP32 and BF16 below
+constexpr unsigned kDiaPad32 = 0xFFD1A6B5u;
+constexpr unsigned short kDiaPad16 = 0xFFD1u;
 constexpr int kDiaMaxDiags = 30;   // diagonals of one slice at most (record of 32 ints)
 constexpr int kDiaChunk = 8;       // diagonals in flight per thread
 
+template <typename V = double>
 struct DiaView {
     const int *__restrict__ rec;      // nsl records of rs ints: k0, m, offsets
-    const double *__restrict__ v;     // 32 values per diagonal
+    const V *__restrict__ v;          // 32 values per diagonal
     int n, nsl, rs;
 };
 
-// One warp per slice, lane = row, grid-stride over slices; the next slice's record is loaded
-// while the current slice is summed. A thread sums its row in storage order exactly as the
-// CSR-stream kernels do (from 0.0, __dmul_rn then __dadd_rn, padding skipped), so every form
-// gives the same bits. The gathers of a chunk are issued with its value loads (padding slots
-// read a clamped column and are not used); lanes read consecutive values and, on a banded
-// matrix, consecutive x.
-template <typename Epi>
+// Loads of a stored value (FP64, FP32 or BF16) with its padding test, and the products and
+// sums of the accumulation type (FP64 or FP32), each rounded separately as in the CSR-stream
+// kernels.
+template <typename V>
+struct DiaLoad;
+template <>
+struct DiaLoad<double> {
+    static __device__ __forceinline__ double get(const double *p) { return ldm(p); }
+    static __device__ __forceinline__ bool pad(double a) {
+        return (unsigned long long)__double_as_longlong(a) == kDiaPad;
+    }
+};
+template <>
+struct DiaLoad<float> {
+    static __device__ __forceinline__ float get(const float *p) { return ldm(p); }
+    static __device__ __forceinline__ bool pad(float a) { return __float_as_uint(a) == kDiaPad32; }
+};
+template <>
+struct DiaLoad<__nv_bfloat16> {   // widened by a shift, so the padding keeps its pattern
+    static __device__ __forceinline__ float get(const __nv_bfloat16 *p) { return ldm(p); }
+    static __device__ __forceinline__ bool pad(float a) { return __float_as_uint(a) == ((unsigned)kDiaPad16 << 16); }
+};
+__device__ __forceinline__ double dia_fma(double s, double a, double x) { return __dadd_rn(s, __dmul_rn(a, x)); }
+__device__ __forceinline__ float dia_fma(float s, float a, float x) { return __fadd_rn(s, __fmul_rn(a, x)); }
+
+// One warp per P adjacent slices, lane = row of each, grid-stride; the next trip's records
+// are loaded while the current slices are summed, and a chunk's loads of all P slices are
+// issued before any of them is summed. P = 1 serves: two slices per trip took about 100
+// registers a thread and measured slower (H's FP64 product at 128^3: 78.9 against 42.9 us). A thread sums its row in storage order
+// exactly as the CSR-stream kernels do (from 0, products then sums each rounded, padding
+// skipped), so every form gives the same bits. Padding slots gather a clamped column and do
+// not use it; lanes read consecutive values and, on a banded matrix, consecutive x.
+template <typename V, typename T, int P, typename Epi>
 static __global__ void __launch_bounds__(kThreads)
-k_spmv_dia(DiaView M, const double *__restrict__ x, Epi epi, DState *st, double *__restrict__ partials) {
+k_spmv_dia(DiaView<V> M, const T *__restrict__ x, Epi epi, DState *st, double *__restrict__ partials) {
     pdl_enter();
     if (Epi::GATED && st != nullptr && st->done) return;
     double red[Epi::NR];
 #pragma unroll
     for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
     const int lane = (int)threadIdx.x & 31;
+    const int ntrip = (M.nsl + P - 1) / P;
     const int nw = (int)gridDim.x * kWarps;
     const unsigned full = 0xffffffffu;
-    int sl = (int)blockIdx.x * kWarps + ((int)threadIdx.x >> 5);
-    int rec = (sl < M.nsl && lane < M.rs) ? __ldg(M.rec + (long)sl * M.rs + lane) : 0;
-    for (; sl < M.nsl; sl += nw) {
-        const int nxt = sl + nw;
-        const int rec_next = (nxt < M.nsl && lane < M.rs) ? __ldg(M.rec + (long)nxt * M.rs + lane) : 0;
-        const int row = (sl << 5) + lane;
-        const bool live = row < M.n;
-        double opnd = 0.0;
-        if constexpr (HasPre<Epi>::value) opnd = live ? epi.pre(row) : 0.0;
-        const int k0 = __shfl_sync(full, rec, 0), m = __shfl_sync(full, rec, 1);
-        double s = 0.0;
-        for (int k = 0; k < m; k += kDiaChunk) {
-            double a[kDiaChunk], xv[kDiaChunk];
+    auto load_rec = [&](int trip, int q) {
+        const int sl = trip * P + q;
+        return (trip < ntrip && sl < M.nsl && lane < M.rs) ? __ldg(M.rec + (long)sl * M.rs + lane) : 0;
+    };
+    int tr = (int)blockIdx.x * kWarps + ((int)threadIdx.x >> 5);
+    int rec[P];
 #pragma unroll
-            for (int u = 0; u < kDiaChunk; ++u) {
-                a[u] = 0.0;
-                xv[u] = 0.0;
-                const int d = __shfl_sync(full, rec, (2 + k + u) & 31);
-                if (k + u < m) {
-                    a[u] = ldm(M.v + ((long)(k0 + k + u) << 5) + lane);
-                    xv[u] = ldx(x + min(max(row + d, 0), M.n - 1));
+    for (int q = 0; q < P; ++q) rec[q] = load_rec(tr, q);
+    for (; tr < ntrip; tr += nw) {
+        int rec_next[P];
+#pragma unroll
+        for (int q = 0; q < P; ++q) rec_next[q] = load_rec(tr + nw, q);
+        int k0[P], m[P], row[P];
+        T opnd[P], s[P];
+        int mm = 0;
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+            row[q] = ((tr * P + q) << 5) + lane;
+            k0[q] = __shfl_sync(full, rec[q], 0);
+            m[q] = __shfl_sync(full, rec[q], 1);   // 0 for a slice past the last
+            mm = max(mm, m[q]);
+            opnd[q] = T(0);
+            if constexpr (HasPre<Epi>::value) opnd[q] = row[q] < M.n ? epi.pre(row[q]) : T(0);
+            s[q] = T(0);
+        }
+        for (int k = 0; k < mm; k += kDiaChunk) {
+            T a[P][kDiaChunk], xv[P][kDiaChunk];
+#pragma unroll
+            for (int q = 0; q < P; ++q)
+#pragma unroll
+                for (int u = 0; u < kDiaChunk; ++u) {
+                    a[q][u] = T(0);
+                    xv[q][u] = T(0);
+                    const int d = __shfl_sync(full, rec[q], (2 + k + u) & 31);
+                    if (k + u < m[q]) {
+                        a[q][u] = DiaLoad<V>::get(M.v + ((long)(k0[q] + k + u) << 5) + lane);
+                        xv[q][u] = ldx(x + min(max(row[q] + d, 0), M.n - 1));
+                    }
                 }
-            }
 #pragma unroll
-            for (int u = 0; u < kDiaChunk; ++u)
-                if (k + u < m && (unsigned long long)__double_as_longlong(a[u]) != kDiaPad)
-                    s = __dadd_rn(s, __dmul_rn(a[u], xv[u]));
+            for (int q = 0; q < P; ++q)
+#pragma unroll
+                for (int u = 0; u < kDiaChunk; ++u)
+                    if (k + u < m[q] && !DiaLoad<V>::pad(a[q][u])) s[q] = dia_fma(s[q], a[q][u], xv[q][u]);
         }
-        if (live) {
-            if constexpr (HasPre<Epi>::value) epi.emit_pre(row, s, opnd, red);
-            else epi.emit(row, s, red);
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+            if (row[q] < M.n) {
+                if constexpr (HasPre<Epi>::value) epi.emit_pre(row[q], s[q], opnd[q], red);
+                else epi.emit(row[q], s[q], red);
+            }
+            rec[q] = rec_next[q];
         }
-        rec = rec_next;
     }
     pdl_release();
     if constexpr (Epi::REDUCES) grid_reduce<Epi::NR>(red, partials, st, epi);
@@ -897,27 +947,23 @@ static __global__ void k_count_outside(int n, const int *__restrict__ rp, const 
     if (c) atomicAdd(count, c);
 }
 
-// Sliced-diagonal values: every slot padding, then each entry e moved to its slot map[e]
-// (slots = 32 x diagonals); *bad is set when an entry holds the padding's bit pattern.
-template <typename T>
+// Sliced-diagonal values, moved as bit patterns B of the value's width (8, 4 or 2 bytes):
+// every slot padding, then each entry e to its slot map[e]; *bad is set when an entry holds
+// the padding's pattern.
+template <typename B>
 static __global__ void __launch_bounds__(kThreads)
-k_dia_fill(long slots, T *__restrict__ dv, T pad) {
+k_dia_fill(long slots, B *__restrict__ dv, B pad) {
     FIIM_FOR_ROWS(i, slots) { dv[i] = pad; }
 }
-template <typename TI, typename TO, typename Conv>
+template <typename B>
 static __global__ void __launch_bounds__(kThreads)
-k_dia_scatter(long nnz, const TI *__restrict__ v, const int *__restrict__ map, TO *__restrict__ dv, Conv conv,
-              int *bad) {
+k_dia_scatter(long nnz, const B *__restrict__ v, const int *__restrict__ map, B *__restrict__ dv, B pad, int *bad) {
     FIIM_FOR_ROWS(e, nnz) {
-        const TO o = conv(v[e]);
-        if (Conv::is_pad(o)) atomicExch(bad, 1);
+        const B o = v[e];
+        if (o == pad) atomicExch(bad, 1);
         dv[map[e]] = o;
     }
 }
-struct DiaConv64 {
-    __device__ double operator()(double v) const { return v; }
-    __device__ static bool is_pad(double v) { return (unsigned long long)__double_as_longlong(v) == kDiaPad; }
-};
 
 // Whether new column indices (with unchanged row offsets) still fit the slices' diagonals:
 // entry e of row i must sit in slot map[e] = 32 k + i % 32 of a diagonal k of slice i / 32
@@ -936,6 +982,23 @@ k_dia_check(int n, const int *__restrict__ rp, const int *__restrict__ ci, const
             }
         }
     }
+}
+
+// Order-sensitive hash of a column stream: the wrapping sum over entries of the splitmix64
+// finalizer (Steele, Lea and Flood, OOPSLA 2014) of (position, column), so the sum's order
+// does not matter. Tells whether a matrix's columns changed since a set-up decision.
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+static __global__ void __launch_bounds__(kThreads)
+k_col_hash(long nnz, const int *__restrict__ ci, unsigned long long *out) {
+    unsigned long long h = 0;
+    FIIM_FOR_ROWS(e, nnz) { h += mix64(((unsigned long long)e << 32) | (unsigned)ci[e]); }
+    for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, h);
 }
 
 }  // namespace fiim

@@ -60,6 +60,11 @@ cudaError_t rows_f(cudaStream_t s, const DevCsr &M, const V *vals, const float *
 template <typename V, typename Epi>
 cudaError_t spmv_f(const DevCsr &M, const V *vals, cudaStream_t s, const float *x, const Epi &epi,
                    DState *st, double *partials) {
+    if (M.dia && M.dvbytes == (int)sizeof(V)) {   // the sliced-diagonal copy of these values
+        const DiaView<V> view{M.drec, static_cast<const V *>(M.dvals), (int)M.n, M.nsl, M.drs};
+        auto kern = k_spmv_dia<V, float, 1, Epi>;
+        return launch_k(kern, grid_for(kern, kWarps, M.nsl), 0, s, view, x, epi, st, partials);
+    }
     switch (M.tile) {
         case 1024: return rows_f<1024>(s, M, vals, x, epi, st, partials);
         case 4096: return rows_f<4096>(s, M, vals, x, epi, st, partials);
@@ -362,6 +367,15 @@ struct MixedSolver : SolverBase {
             FIIM_TRY(set_tile(G, 2048, stream));
             FIIM_TRY(set_tile(H, 2048, stream));
         }
+        // Sliced-diagonal copies of the inner products' values where the matrices allow them
+        // (A's FP64 residual product keeps the CSR streams).
+        const int vb = bf16 ? 2 : 4;
+        FIIM_TRY(build_dia_structure(A, stream, 4));
+        FIIM_TRY(place_dia(A, A32, stream));
+        FIIM_TRY(build_dia_structure(G, stream, vb));
+        FIIM_TRY(place_dia(G, bf16 ? (const void *)G16 : (const void *)G32, stream));
+        FIIM_TRY(build_dia_structure(H, stream, vb));
+        FIIM_TRY(place_dia(H, bf16 ? (const void *)H16 : (const void *)H32, stream));
         return build_graph();
     }
 
@@ -507,6 +521,7 @@ struct MixedSolver : SolverBase {
         ev0 = ev1 = nullptr;
         stream = nullptr;
         hst = nullptr;
+        for (DevCsr *M : {&A, &G, &H}) release_dia(*M);
         arena.release();
     }
 };
@@ -537,7 +552,8 @@ int fiim_mixed_solve(fiim_solver_t h, const double *b, double *x, double tol, in
 }
 
 int64_t fiim_mixed_device_bytes(fiim_solver_t h) {
-    return (int64_t) reinterpret_cast<fiim::MixedSolver *>(h)->arena.cap;
+    const auto *s = reinterpret_cast<fiim::MixedSolver *>(h);
+    return (int64_t)(s->arena.cap + s->A.dia_bytes + s->G.dia_bytes + s->H.dia_bytes);
 }
 
 int fiim_mixed_destroy(fiim_solver_t h) {

@@ -24,6 +24,7 @@
 #include <iostream>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -193,13 +194,13 @@ static cudaError_t spmv_warp(cudaStream_t s, const DevCsr &M, const double *x, c
     return launch_k(kern, g, 0, s, view(M), M.rb, M.eb, M.nblk, x, epi, st, partials, NarrowCols{});
 }
 
-// Sliced-diagonal SpMV: kWarps slices per CTA.
+// Sliced-diagonal SpMV: kWarps warps per CTA, one slice per warp trip.
 template <typename Epi>
 static cudaError_t spmv_dia(cudaStream_t s, const DevCsr &M, const double *x, const Epi &epi, DState *st,
                             double *partials) {
-    auto kern = k_spmv_dia<Epi>;
-    const int g = grid_for(kern, kWarps, M.nsl);
-    return launch_k(kern, g, 0, s, DiaView{M.drec, M.dv, (int)M.n, M.nsl, M.drs}, x, epi, st, partials);
+    const DiaView<double> view{M.drec, static_cast<const double *>(M.dvals), (int)M.n, M.nsl, M.drs};
+    auto kern = k_spmv_dia<double, double, 1, Epi>;
+    return launch_k(kern, grid_for(kern, kWarps, M.nsl), 0, s, view, x, epi, st, partials);
 }
 
 // Solver SpMV: the sliced-diagonal copy where the matrix has one, else CSR-stream over the
@@ -274,41 +275,66 @@ void release_dia(DevCsr &M) {
     M.dia_mem = nullptr;
     M.dia_bytes = 0;
     M.drec = M.dmap = M.dbad = nullptr;
-    M.dv = nullptr;
+    M.dvals = nullptr;
+    M.dvbytes = 0;
     M.dia = 0;
     M.nsl = 0;
     M.drs = 0;
     M.ndiag = 0;
 }
 
-// Padding in every slot, then each entry in its own; keeps the copy only if no entry holds
-// the padding's bit pattern.
-static int place_dia_values(DevCsr &M, cudaStream_t s) {
-    FIIM_CUDA(cudaMemsetAsync(M.dbad, 0, sizeof(int), s));
+bool dia_wanted() {
+    // FIIM_SPMV=rows / staged / warp keep a CSR-stream form; FIIM_DIA=0 never builds the copy.
+    const char *force = std::getenv("FIIM_SPMV"), *off_env = std::getenv("FIIM_DIA");
+    return !((force && std::strcmp(force, "dia") != 0) || (off_env && std::strcmp(off_env, "0") == 0));
+}
+
+template <typename B>
+static int place_bits(DevCsr &M, const void *vals, B pad, cudaStream_t s) {
     const long slots = 32 * M.ndiag;
-    double pad;
-    std::memcpy(&pad, &kDiaPad, sizeof pad);
-    k_dia_fill<double><<<stream_grid(k_dia_fill<double>, slots), kThreads, 0, s>>>(slots, M.dv, pad);
+    B *dv = static_cast<B *>(M.dvals);
+    k_dia_fill<B><<<stream_grid(k_dia_fill<B>, slots), kThreads, 0, s>>>(slots, dv, pad);
     FIIM_CUDA(cudaGetLastError());
-    auto scat = k_dia_scatter<double, double, DiaConv64>;
-    scat<<<stream_grid(scat, M.nnz), kThreads, 0, s>>>(M.nnz, M.v, M.dmap, M.dv, DiaConv64{}, M.dbad);
+    k_dia_scatter<B><<<stream_grid(k_dia_scatter<B>, M.nnz), kThreads, 0, s>>>(M.nnz, static_cast<const B *>(vals),
+                                                                               M.dmap, dv, pad, M.dbad);
     FIIM_CUDA(cudaGetLastError());
+    return FIIM_OK;
+}
+
+int place_dia(DevCsr &M, const void *vals, cudaStream_t s) {
+    if (!M.dia_mem) return FIIM_OK;
+    FIIM_CUDA(cudaMemsetAsync(M.dbad, 0, sizeof(int), s));
+    if (M.dvbytes == 8) FIIM_TRY(place_bits<unsigned long long>(M, vals, kDiaPad, s));
+    else if (M.dvbytes == 4) FIIM_TRY(place_bits<unsigned>(M, vals, kDiaPad32, s));
+    else FIIM_TRY(place_bits<unsigned short>(M, vals, kDiaPad16, s));
     int bad = 0;
     FIIM_CUDA(cudaMemcpyAsync(&bad, M.dbad, sizeof(int), cudaMemcpyDeviceToHost, s));
     FIIM_CUDA(cudaStreamSynchronize(s));
-    if (bad) release_dia(M);
+    if (bad) release_dia(M);   // an entry holds the padding pattern: the CSR streams serve
     else M.dia = 1;
     return FIIM_OK;
 }
 
-int build_dia(DevCsr &M, cudaStream_t s) {
+static int col_hash(DevCsr &M, cudaStream_t s, unsigned long long *h) {
+    *h = 0;
+    if (M.nnz <= 0 || !M.dhash) return FIIM_OK;
+    FIIM_CUDA(cudaMemsetAsync(M.dhash, 0, sizeof(unsigned long long), s));
+    k_col_hash<<<stream_grid(k_col_hash, M.nnz), kThreads, 0, s>>>(M.nnz, M.ci, M.dhash);
+    FIIM_CUDA(cudaGetLastError());
+    FIIM_CUDA(cudaMemcpyAsync(h, M.dhash, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    FIIM_CUDA(cudaStreamSynchronize(s));
+    return FIIM_OK;
+}
+
+int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes) {
     release_dia(M);
-    // FIIM_SPMV=rows / staged / warp keep a CSR-stream form; FIIM_DIA=0 never builds the copy.
-    const char *force = std::getenv("FIIM_SPMV"), *off_env = std::getenv("FIIM_DIA");
-    if ((force && std::strcmp(force, "dia") != 0) || (off_env && std::strcmp(off_env, "0") == 0)) return FIIM_OK;
+    M.dia_tried = false;
+    if (!dia_wanted()) return FIIM_OK;
     const int n = (int)M.n;
     const long nnz = M.nnz;
     if (n <= 0 || nnz <= 0 || (long)M.hrp.size() != (long)n + 1) return FIIM_OK;
+    FIIM_TRY(col_hash(M, s, &M.dia_cols));
+    M.dia_tried = true;
     std::vector<int> ci(nnz);
     FIIM_CUDA(cudaMemcpyAsync(ci.data(), M.ci, sizeof(int) * nnz, cudaMemcpyDeviceToHost, s));
     FIIM_CUDA(cudaStreamSynchronize(s));
@@ -350,8 +376,8 @@ int build_dia(DevCsr &M, cudaStream_t s) {
     const long ndiag = sp[nsl];
     const int rs = most <= 14 ? 16 : 32;
     // Kept only when it moves fewer bytes than the CSR streams it replaces.
-    const double dia_bytes = 8.0 * 32 * ndiag + 4.0 * rs * nsl;
-    const double csr_bytes_now = (double)nnz * (8 + (M.narrow ? 2 : 4)) + 4.0 * (n + 1);
+    const double dia_bytes = (double)vbytes * 32 * ndiag + 4.0 * rs * nsl;
+    const double csr_bytes_now = (double)nnz * (vbytes + (M.narrow ? 2 : 4)) + 4.0 * (n + 1);
     if (!(dia_bytes < csr_bytes_now) || 32 * ndiag >= (1L << 31)) return FIIM_OK;
     std::vector<int> rec((size_t)nsl * rs, 0), map(nnz);
 #pragma omp parallel
@@ -374,7 +400,7 @@ int build_dia(DevCsr &M, cudaStream_t s) {
         }
     }
     const size_t b_rec = Arena::need(sizeof(int) * rec.size()), b_map = Arena::need(sizeof(int) * nnz),
-                 b_bad = Arena::need(sizeof(int)), b_v = Arena::need(sizeof(double) * 32 * ndiag);
+                 b_bad = Arena::need(sizeof(int)), b_v = Arena::need((size_t)vbytes * 32 * ndiag);
     char *mem = nullptr;
     if (cudaMalloc(&mem, b_rec + b_map + b_bad + b_v) != cudaSuccess) {
         cudaGetLastError();
@@ -385,17 +411,20 @@ int build_dia(DevCsr &M, cudaStream_t s) {
     M.drec = reinterpret_cast<int *>(mem);
     M.dmap = reinterpret_cast<int *>(mem + b_rec);
     M.dbad = reinterpret_cast<int *>(mem + b_rec + b_map);
-    M.dv = reinterpret_cast<double *>(mem + b_rec + b_map + b_bad);
+    M.dvals = mem + b_rec + b_map + b_bad;
+    M.dvbytes = vbytes;
     M.nsl = nsl;
     M.drs = rs;
     M.ndiag = ndiag;
     FIIM_CUDA(cudaMemcpyAsync(M.drec, rec.data(), sizeof(int) * rec.size(), cudaMemcpyHostToDevice, s));
     FIIM_CUDA(cudaMemcpyAsync(M.dmap, map.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, s));
-    return place_dia_values(M, s);   // synchronizes before the host arrays go
+    FIIM_CUDA(cudaStreamSynchronize(s));   // before the host arrays go
+    return FIIM_OK;
 }
 
-int refresh_dia(DevCsr &M, cudaStream_t s) {
-    if (!M.dia) return FIIM_OK;
+int dia_fits(DevCsr &M, cudaStream_t s, bool *fits) {
+    *fits = false;
+    if (!M.dia_mem) return FIIM_OK;
     FIIM_CUDA(cudaMemsetAsync(M.dbad, 0, sizeof(int), s));
     k_dia_check<<<stream_grid(k_dia_check, M.n), kThreads, 0, s>>>((int)M.n, M.rp, M.ci, M.dmap, M.drec, M.drs,
                                                                    M.dbad);
@@ -403,8 +432,27 @@ int refresh_dia(DevCsr &M, cudaStream_t s) {
     int bad = 0;
     FIIM_CUDA(cudaMemcpyAsync(&bad, M.dbad, sizeof(int), cudaMemcpyDeviceToHost, s));
     FIIM_CUDA(cudaStreamSynchronize(s));
-    if (bad) return build_dia(M, s);
-    return place_dia_values(M, s);
+    *fits = !bad;
+    return FIIM_OK;
+}
+
+int build_dia(DevCsr &M, cudaStream_t s) {
+    FIIM_TRY(build_dia_structure(M, s, 8));
+    return place_dia(M, M.v, s);
+}
+
+int refresh_dia(DevCsr &M, cudaStream_t s) {
+    if (!dia_wanted()) return FIIM_OK;
+    if (!M.dia) {   // not built for the previous columns: decide again only if they changed
+        unsigned long long h = 0;
+        FIIM_TRY(col_hash(M, s, &h));
+        if (M.dia_tried && h == M.dia_cols) return FIIM_OK;
+        return build_dia(M, s);
+    }
+    bool fits = false;
+    FIIM_TRY(dia_fits(M, s, &fits));
+    if (!fits) return build_dia(M, s);
+    return place_dia(M, M.v, s);
 }
 
 int set_tile(DevCsr &M, int tile, cudaStream_t s) {
@@ -743,17 +791,18 @@ int carve_csr(Arena &ar, DevCsr &M, long n, long nnz) {
     M.rp = static_cast<int *>(ar.take(sizeof(int) * (n + 1)));
     M.ci = static_cast<int *>(ar.take(sizeof(int) * std::max<long>(nnz, 1) + kStreamSlack));
     M.v = static_cast<double *>(ar.take(sizeof(double) * std::max<long>(nnz, 1) + kStreamSlack));
-    M.rb = static_cast<int *>(ar.take(sizeof(int) * (3 * (n + 1) + 1)));   // at most one block per row
+    M.rb = static_cast<int *>(ar.take(sizeof(int) * (3 * (n + 1) + 6)));   // at most one block per row
     M.cd = static_cast<short *>(ar.take(sizeof(short) * std::max<long>(nnz, 1) + kStreamSlack));
     if (!M.rp || !M.ci || !M.v || !M.rb || !M.cd) return set_error(FIIM_ENOMEM, "arena exhausted");
     M.eb = M.rb + (n + 1);
     M.cb = M.rb + 2 * (n + 1);
     M.wide = M.rb + 3 * (n + 1);
+    M.dhash = reinterpret_cast<unsigned long long *>(M.rb + ((3 * (n + 1) + 3) & ~1L));   // 8-byte aligned
     return FIIM_OK;
 }
 
 size_t csr_bytes(long n, long nnz) {
-    return Arena::need(sizeof(int) * (n + 1)) + Arena::need(sizeof(int) * (3 * (n + 1) + 1)) +
+    return Arena::need(sizeof(int) * (n + 1)) + Arena::need(sizeof(int) * (3 * (n + 1) + 6)) +
            Arena::need(sizeof(short) * std::max<long>(nnz, 1) + kStreamSlack) +
            Arena::need(sizeof(int) * std::max<long>(nnz, 1) + kStreamSlack) +
            Arena::need(sizeof(double) * std::max<long>(nnz, 1) + kStreamSlack);
@@ -1103,8 +1152,13 @@ int Solver::reload(const int *Ai, const int *Aj, const double *Av, const int *Gi
     DevCsr *mats[] = {&A, &G, &H, &L, &U};
     for (int k = 0; k < (combined ? 5 : 3); ++k) {
         DevCsr &M = *mats[k];
-        const int old = M.nblk, was_narrow = M.narrow, was_dia = M.dia;
-        const void *was_mem = M.dia_mem;   // a rebuilt copy has new addresses
+        const int old = M.nblk, was_narrow = M.narrow;
+        // Everything of the sliced-diagonal copy that a captured launch holds: a rebuilt copy
+        // may reuse the freed allocation's address with another layout inside it.
+        auto dia_args = [](const DevCsr &D) {
+            return std::make_tuple(D.dia, D.drec, D.dvals, D.nsl, D.drs);
+        };
+        const auto was_dia = dia_args(M);
         if (M.rows_same && M.nblk > 0) {
             FIIM_TRY(build_narrow(M, stream));
             FIIM_TRY(refresh_dia(M, stream));
@@ -1112,7 +1166,7 @@ int Solver::reload(const int *Ai, const int *Aj, const double *Av, const int *Gi
             FIIM_TRY(set_tile(M, M.tile, stream));
             FIIM_TRY(build_dia(M, stream));
         }
-        regraph |= (M.nblk != old) || (M.narrow != was_narrow) || (M.dia != was_dia) || (M.dia_mem != was_mem);
+        regraph |= (M.nblk != old) || (M.narrow != was_narrow) || (dia_args(M) != was_dia);
     }
     if (regraph) FIIM_TRY(build_graph());
     return FIIM_OK;

@@ -42,7 +42,7 @@ EXPORTS = (
     "fiim_last_error", "fiim_dropin_cache", "fiim_options_default", "fiim_EPBiCGSTAB_afiim", "fiim_EPBiCGSTAB_pdfiim",
     "fiim_PBiCGSTAB_acifim", "fiim_solver_create", "fiim_solver_solve", "fiim_solver_device_bytes",
     "fiim_solver_spmv_shape", "fiim_solver_apply", "fiim_solver_kernel_times", "fiim_solver_kernel_times_seq", "fiim_solver_mode",
-    "fiim_solver_set_wait_limit", "fiim_solver_test_stall", "fiim_solver_iteration_bytes",
+    "fiim_solver_set_wait_limit", "fiim_solver_test_stall", "fiim_solver_iteration_bytes", "fiim_solver_matrix_bytes",
     "fiim_solver_destroy", "fiim_batch_create", "fiim_batch_solve", "fiim_batch_destroy",
     "fiim_block_create", "fiim_block_solve", "fiim_block_apply", "fiim_block_spmm_shape", "fiim_block_destroy",
     "fiim_spmv", "fiim_prec_apply", "fiim_prec_apply_noalloc",
@@ -92,6 +92,7 @@ def lib() -> C.CDLL:
             getattr(L, name).restype = C.c_long
         L.fiim_gen_zipf_mean.restype = C.c_double
         L.fiim_solver_iteration_bytes.restype = C.c_double
+        L.fiim_solver_matrix_bytes.restype = C.c_double
         _lib = L
     return _lib
 
@@ -237,8 +238,8 @@ class Solver(_Handle):
         return int(lib().fiim_solver_device_bytes(self._h))
 
     def spmv_shape(self, which: int):
-        """(row-block size, form) of matrix `which` (0 A, 1 G, 2 H): form 0 streams through
-        registers, form 1 by bulk copies."""
+        """(row-block size, form) of matrix `which` (0 A, 1 G, 2 H): form 0 CSR streams through
+        registers, 1 by bulk copies, 2 one warp per row block, 3 the sliced-diagonal copy."""
         t, f = C.c_int(0), C.c_int(0)
         _check(lib().fiim_solver_spmv_shape(self._h, C.c_int(which), C.byref(t), C.byref(f)))
         return t.value, f.value
@@ -289,6 +290,10 @@ class Solver(_Handle):
 
     def iteration_bytes(self) -> float:
         return float(lib().fiim_solver_iteration_bytes(self._h))
+
+    def matrix_bytes(self, which: int) -> float:
+        """Bytes one product with matrix `which` reads from it in the form it is served in."""
+        return float(lib().fiim_solver_matrix_bytes(self._h, C.c_int(which)))
 
     def close(self):
         if self._h and self._h.value:

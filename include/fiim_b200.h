@@ -204,6 +204,13 @@ int fiim_solver_test_stall(fiim_solver_t s);
  * S(M) = 12 nnz(M) + 4 (n + 1). */
 double fiim_solver_iteration_bytes(fiim_solver_t s);
 
+/* Bytes that one product with matrix `which` (0 A, 1 G, 2 H, 3 L, 4 U) reads from the
+ * matrix in the form it is served in (fiim_solver_spmv_shape): 256 per diagonal of a slice
+ * plus the slice records for the sliced-diagonal copy; the values, the column stream (2 or 4
+ * bytes an entry), the row offsets and the row-block bounds for the CSR streams. -1 for a bad
+ * handle or index. */
+double fiim_solver_matrix_bytes(fiim_solver_t s, int which);
+
 int fiim_solver_destroy(fiim_solver_t s);
 
 /* ===========================================================================
