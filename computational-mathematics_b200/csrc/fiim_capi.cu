@@ -333,7 +333,7 @@ double fiim_solver_matrix_bytes(fiim_solver_t h, int which) {
     auto *s = reinterpret_cast<fiim::Solver *>(h);
     const fiim::DevCsr *m[] = {&s->A, &s->G, &s->H, &s->L, &s->U};
     const fiim::DevCsr &M = *m[which];
-    if (M.dia) return 32.0 * M.dvbytes * (double)M.ndiag + 4.0 * M.drs * M.nsl;
+    if (M.dia) return (double)M.dsh * M.dvbytes * (double)M.ndiag + 4.0 * M.drs * M.nsl;
     return (double)M.nnz * (8 + (M.narrow ? 2 : 4)) + 4.0 * (M.n + 1) + (M.narrow ? 4.0 * M.nblk : 0.0) +
            8.0 * (M.nblk + 1);
 }

@@ -73,13 +73,14 @@ struct DevCsr {
     int nblk = 0;
     // Sliced-diagonal copy (kFormDia; fiim_kernels.cuh, k_spmv_dia), in its own allocation.
     int dia = 0;                 // 1: built and current
-    int nsl = 0;                 // slices of 32 rows
+    int nsl = 0;                 // slices of dsh rows
+    int dsh = 0;                 // rows a slice: 32 R, R = 8 / dvbytes rows a lane
     int drs = 0;                 // ints per slice record (16 or 32): first diagonal, count, offsets
-    long ndiag = 0;              // diagonals over all slices (32 slots each)
+    long ndiag = 0;              // diagonals over all slices (dsh slots each)
     int *drec = nullptr;         // nsl records
     int *dmap = nullptr;         // nnz: the slot of each entry
     int *dbad = nullptr;         // device flag of the structure check and value placement
-    void *dvals = nullptr;       // 32 * ndiag values of dvbytes bytes each (FP64, FP32 or BF16)
+    void *dvals = nullptr;       // dsh * ndiag values of dvbytes bytes each (FP64, FP32 or BF16)
     int dvbytes = 0;
     void *dia_mem = nullptr;
     size_t dia_bytes = 0;        // size of that allocation
@@ -137,8 +138,9 @@ int set_tile(DevCsr &M, int tile, cudaStream_t s);
 int build_narrow(DevCsr &M, cudaStream_t s);
 // The sliced-diagonal copy of M (fiim_kernels.cuh, k_spmv_dia). build_dia_structure lays it
 // out (slice records, the slot of every entry) for values of vbytes bytes (8, 4 or 2) when
-// M's rows are sorted by column, every slice of 32 rows has at most kDiaMaxDiags diagonals
-// and the copy moves fewer bytes than the CSR streams (M.dia_mem stays null otherwise);
+// M's rows are sorted by column, every slice (32 R rows, R = 8 / vbytes) has at most
+// kDiaMaxDiags diagonals and the copy moves fewer bytes than the CSR streams (M.dia_mem
+// stays null otherwise);
 // place_dia moves the nnz values `vals` (device, that width) into it and sets M.dia = 1,
 // unless an entry holds the padding pattern (then the copy is released). dia_fits tells
 // whether M's current columns (same row offsets) still sit in the laid-out slots.

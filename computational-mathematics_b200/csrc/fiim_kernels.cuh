@@ -627,125 +627,165 @@ k_narrow_cols(const int *__restrict__ ci, const int *__restrict__ eb, int nblk, 
 }
 
 // ---------------------------------------------------------------- sliced-diagonal SpMV
-// The sliced-diagonal form of a CSR matrix whose rows, 32 at a time, share a few diagonals:
-// slice s holds rows 32 s .. 32 s + 31 and the union of their entries' diagonals d = col -
-// row, ascending; each diagonal stores one value per row of the slice (v[32 k + lane], k
-// counted over all slices). A row's own entries keep their storage order (rows are sorted by
-// column), and a slot the row has no entry in holds kDiaPad, a NaN bit pattern that no entry
-// of the matrix holds (checked when the values are placed). Each slice has a record of rs
-// ints (16 or 32): its first diagonal k0, its count m and its m offsets, which a warp reads
-// in one coalesced load. Bytes per entry: 8 (FP64 value) and the padding, plus 2 or 4 per row
-// for the records, against 10 or 12 per entry and 4 per row for the CSR streams.
+// The sliced-diagonal form of a CSR matrix whose rows, a slice of 32 R at a time, share a few
+// diagonals (R rows a lane: 1 for FP64 values, 2 for FP32, 4 for BF16, so that a lane's values
+// of one diagonal are one 8-byte word). Slice s holds rows 32 R s .. 32 R s + 32 R - 1 and the
+// union of their entries' diagonals d = col - row, ascending; each diagonal stores one value
+// per row of the slice (v[32 R k + row - 32 R s], k counted over all slices). A row's own
+// entries keep their storage order (rows are sorted by column), and a slot the row has no
+// entry in holds the padding pattern (kDiaPad, kDiaPad32, kDiaPad16: NaN bit patterns no
+// entry of the matrix holds, checked when the values are placed). Each slice has a record of
+// rs ints (16 or 32): its first diagonal k0, its count m (with kDiaClamp when a diagonal
+// reaches outside the matrix from one of its rows) and its m offsets, which a warp reads in
+// one coalesced load. Bytes per entry: the value's width and the padding, plus 2 or 4 per
+// R rows for the records, against the width plus 2 or 4 per entry and 4 per row for the CSR
+// streams.
 constexpr unsigned long long kDiaPad = 0xFFF7D1A6B00C5A1DULL;   // FP64 padding; FP32 and BF16 below
 constexpr unsigned kDiaPad32 = 0xFFD1A6B5u;
 constexpr unsigned short kDiaPad16 = 0xFFD1u;
 constexpr int kDiaMaxDiags = 30;   // diagonals of one slice at most (record of 32 ints)
-constexpr int kDiaChunk = 8;       // diagonals in flight per thread
+constexpr int kDiaCountMask = 0xffff, kDiaClamp = 1 << 30;   // record[1]: count | clamp flag
+constexpr int kDiaChunk = 8;       // diagonals in flight per thread (4 for BF16's 4 rows a lane)
 
 template <typename V = double>
 struct DiaView {
     const int *__restrict__ rec;      // nsl records of rs ints: k0, m, offsets
-    const V *__restrict__ v;          // 32 values per diagonal
+    const V *__restrict__ v;          // 32 R values per diagonal
     int n, nsl, rs;
 };
 
-// Loads of a stored value (FP64, FP32 or BF16) with its padding test, and the products and
-// sums of the accumulation type (FP64 or FP32), each rounded separately as in the CSR-stream
-// kernels.
+// A lane's R values of one diagonal (one 8-byte load, streamed) and the padding test; BF16 is
+// widened by a shift or a mask, so the padding keeps its pattern in the upper half.
 template <typename V>
 struct DiaLoad;
 template <>
-struct DiaLoad<double> {
-    static __device__ __forceinline__ double get(const double *p) { return ldm(p); }
-    static __device__ __forceinline__ bool pad(double a) {
-        return (unsigned long long)__double_as_longlong(a) == kDiaPad;
-    }
+struct DiaLoad<double> {   // the upper word decides: no entry of a served matrix shares it
+    static constexpr int R = 1;
+    static __device__ __forceinline__ void get(const double *p, double (&a)[1]) { a[0] = ldm(p); }
+    static __device__ __forceinline__ bool pad(double a) { return __double2hiint(a) == (int)(kDiaPad >> 32); }
 };
 template <>
 struct DiaLoad<float> {
-    static __device__ __forceinline__ float get(const float *p) { return ldm(p); }
+    static constexpr int R = 2;
+    static __device__ __forceinline__ void get(const float *p, float (&a)[2]) {
+        const float2 w = __ldcs(reinterpret_cast<const float2 *>(p));
+        a[0] = w.x;
+        a[1] = w.y;
+    }
     static __device__ __forceinline__ bool pad(float a) { return __float_as_uint(a) == kDiaPad32; }
 };
 template <>
-struct DiaLoad<__nv_bfloat16> {   // widened by a shift, so the padding keeps its pattern
-    static __device__ __forceinline__ float get(const __nv_bfloat16 *p) { return ldm(p); }
+struct DiaLoad<__nv_bfloat16> {
+    static constexpr int R = 4;
+    static __device__ __forceinline__ void get(const __nv_bfloat16 *p, float (&a)[4]) {
+        const uint2 w = __ldcs(reinterpret_cast<const uint2 *>(p));
+        a[0] = __uint_as_float(w.x << 16);
+        a[1] = __uint_as_float(w.x & 0xffff0000u);
+        a[2] = __uint_as_float(w.y << 16);
+        a[3] = __uint_as_float(w.y & 0xffff0000u);
+    }
     static __device__ __forceinline__ bool pad(float a) { return __float_as_uint(a) == ((unsigned)kDiaPad16 << 16); }
 };
 __device__ __forceinline__ double dia_fma(double s, double a, double x) { return __dadd_rn(s, __dmul_rn(a, x)); }
 __device__ __forceinline__ float dia_fma(float s, float a, float x) { return __fadd_rn(s, __fmul_rn(a, x)); }
 
-// One warp per P adjacent slices, lane = row of each, grid-stride; the next trip's records
-// are loaded while the current slices are summed, and a chunk's loads of all P slices are
-// issued before any of them is summed. P = 1 serves: two slices per trip took about 100
-// registers a thread and measured slower (H's FP64 product at 128^3: 78.9 against 42.9 us). A thread sums its row in storage order
-// exactly as the CSR-stream kernels do (from 0, products then sums each rounded, padding
-// skipped), so every form gives the same bits. Padding slots gather a clamped column and do
-// not use it; lanes read consecutive values and, on a banded matrix, consecutive x.
-template <typename V, typename T, int P, typename Epi>
+// A lane's R gathered x of one diagonal d for its rows row0 .. row0 + R - 1 (row0 a multiple
+// of R). A slice whose diagonals all stay inside the matrix (no kDiaClamp flag) reads without
+// clamping, FP32 pairs as one 8-byte load when d is even; otherwise each column is clamped to
+// [0, n) (padding slots may point outside; their x is never used).
+template <bool CLAMP, int R, typename T>
+__device__ __forceinline__ void dia_gather(const T *__restrict__ x, int row0, int d, int n, T (&xv)[R]) {
+    if constexpr (!CLAMP && R >= 2 && sizeof(T) == 4) {
+        if ((d & 1) == 0) {
+#pragma unroll
+            for (int j = 0; j < R; j += 2) {
+                const float2 w = __ldg(reinterpret_cast<const float2 *>(x + row0 + d + j));
+                xv[j] = w.x;
+                xv[j + 1] = w.y;
+            }
+            return;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        const int c = row0 + j + d;
+        xv[j] = ldx(x + (CLAMP ? min(max(c, 0), n - 1) : c));
+    }
+}
+
+// One warp per slice, R rows a lane, grid-stride; the next slice's record is loaded while the
+// current one is summed, and a chunk's value loads and gathers are all issued before any is
+// summed. A thread sums each of its rows in storage order exactly as the CSR-stream kernels
+// do (from 0, products then sums each rounded, padding skipped), so every form gives the same
+// bits. Lanes read consecutive values and, on a banded matrix, consecutive x. Two slices per
+// warp trip took about 100 registers a thread and measured slower (H's FP64 product at 128^3:
+// 78.9 against 42.9 us). The kernels are bound by instruction issue (63 % issue active at 48 %
+// warps active), so with 2 or 4 rows a lane a slice that needs no clamping takes a path
+// without it, with paired FP32 gathers; for FP64 that path lost its loads' overlap (long-
+// scoreboard stalls 15.4 against 7.2 an issue, H's product 67.0 against 47.7 us under ncu),
+// so FP64 always clamps.
+template <typename V, typename T, typename Epi>
 static __global__ void __launch_bounds__(kThreads)
 k_spmv_dia(DiaView<V> M, const T *__restrict__ x, Epi epi, DState *st, double *__restrict__ partials) {
+    constexpr int R = DiaLoad<V>::R, SH = 32 * R;
+    constexpr int C = R >= 4 ? kDiaChunk / 2 : kDiaChunk;   // about 32 values in flight a thread
     pdl_enter();
     if (Epi::GATED && st != nullptr && st->done) return;
     double red[Epi::NR];
 #pragma unroll
     for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
     const int lane = (int)threadIdx.x & 31;
-    const int ntrip = (M.nsl + P - 1) / P;
     const int nw = (int)gridDim.x * kWarps;
     const unsigned full = 0xffffffffu;
-    auto load_rec = [&](int trip, int q) {
-        const int sl = trip * P + q;
-        return (trip < ntrip && sl < M.nsl && lane < M.rs) ? __ldg(M.rec + (long)sl * M.rs + lane) : 0;
-    };
-    int tr = (int)blockIdx.x * kWarps + ((int)threadIdx.x >> 5);
-    int rec[P];
+    int sl = (int)blockIdx.x * kWarps + ((int)threadIdx.x >> 5);
+    int rec = (sl < M.nsl && lane < M.rs) ? __ldg(M.rec + (long)sl * M.rs + lane) : 0;
+    for (; sl < M.nsl; sl += nw) {
+        const int nxt = sl + nw;
+        const int rec_next = (nxt < M.nsl && lane < M.rs) ? __ldg(M.rec + (long)nxt * M.rs + lane) : 0;
+        const int row0 = sl * SH + R * lane;
+        T opnd[R], s[R];
 #pragma unroll
-    for (int q = 0; q < P; ++q) rec[q] = load_rec(tr, q);
-    for (; tr < ntrip; tr += nw) {
-        int rec_next[P];
-#pragma unroll
-        for (int q = 0; q < P; ++q) rec_next[q] = load_rec(tr + nw, q);
-        int k0[P], m[P], row[P];
-        T opnd[P], s[P];
-        int mm = 0;
-#pragma unroll
-        for (int q = 0; q < P; ++q) {
-            row[q] = ((tr * P + q) << 5) + lane;
-            k0[q] = __shfl_sync(full, rec[q], 0);
-            m[q] = __shfl_sync(full, rec[q], 1);   // 0 for a slice past the last
-            mm = max(mm, m[q]);
-            opnd[q] = T(0);
-            if constexpr (HasPre<Epi>::value) opnd[q] = row[q] < M.n ? epi.pre(row[q]) : T(0);
-            s[q] = T(0);
+        for (int j = 0; j < R; ++j) {
+            opnd[j] = T(0);
+            if constexpr (HasPre<Epi>::value) opnd[j] = row0 + j < M.n ? epi.pre(row0 + j) : T(0);
+            s[j] = T(0);
         }
-        for (int k = 0; k < mm; k += kDiaChunk) {
-            T a[P][kDiaChunk], xv[P][kDiaChunk];
+        const int k0 = __shfl_sync(full, rec, 0), mf = __shfl_sync(full, rec, 1);
+        const int m = mf & kDiaCountMask;
+        auto sum = [&](auto clamp) {
+            constexpr bool CL = decltype(clamp)::value;
+            for (int k = 0; k < m; k += C) {
+                T a[C][R], xv[C][R];
 #pragma unroll
-            for (int q = 0; q < P; ++q)
+                for (int u = 0; u < C; ++u) {
+                    const int d = __shfl_sync(full, rec, (2 + k + u) & 31);
 #pragma unroll
-                for (int u = 0; u < kDiaChunk; ++u) {
-                    a[q][u] = T(0);
-                    xv[q][u] = T(0);
-                    const int d = __shfl_sync(full, rec[q], (2 + k + u) & 31);
-                    if (k + u < m[q]) {
-                        a[q][u] = DiaLoad<V>::get(M.v + ((long)(k0[q] + k + u) << 5) + lane);
-                        xv[q][u] = ldx(x + min(max(row[q] + d, 0), M.n - 1));
+                    for (int j = 0; j < R; ++j) {
+                        a[u][j] = T(0);
+                        xv[u][j] = T(0);
+                    }
+                    if (k + u < m) {
+                        DiaLoad<V>::get(M.v + (long)(k0 + k + u) * SH + R * lane, a[u]);
+                        dia_gather<CL, R>(x, row0, d, M.n, xv[u]);
                     }
                 }
 #pragma unroll
-            for (int q = 0; q < P; ++q)
+                for (int u = 0; u < C; ++u)
 #pragma unroll
-                for (int u = 0; u < kDiaChunk; ++u)
-                    if (k + u < m[q] && !DiaLoad<V>::pad(a[q][u])) s[q] = dia_fma(s[q], a[q][u], xv[q][u]);
-        }
-#pragma unroll
-        for (int q = 0; q < P; ++q) {
-            if (row[q] < M.n) {
-                if constexpr (HasPre<Epi>::value) epi.emit_pre(row[q], s[q], opnd[q], red);
-                else epi.emit(row[q], s[q], red);
+                    for (int j = 0; j < R; ++j)
+                        if (k + u < m && !DiaLoad<V>::pad(a[u][j])) s[j] = dia_fma(s[j], a[u][j], xv[u][j]);
             }
-            rec[q] = rec_next[q];
+        };
+        if (R == 1 || (mf & kDiaClamp)) sum(std::true_type{});
+        else sum(std::false_type{});
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            if (row0 + j < M.n) {
+                if constexpr (HasPre<Epi>::value) epi.emit_pre(row0 + j, s[j], opnd[j], red);
+                else epi.emit(row0 + j, s[j], red);
+            }
         }
+        rec = rec_next;
     }
     pdl_release();
     if constexpr (Epi::REDUCES) grid_reduce<Epi::NR>(red, partials, st, epi);
@@ -956,27 +996,33 @@ k_dia_fill(long slots, B *__restrict__ dv, B pad) {
     FIIM_FOR_ROWS(i, slots) { dv[i] = pad; }
 }
 template <typename B>
+__device__ __forceinline__ bool dia_is_pad(B o, B pad) {   // the kernel's test (upper word of FP64)
+    if constexpr (sizeof(B) == 8) return (o >> 32) == (pad >> 32);
+    else return o == pad;
+}
+template <typename B>
 static __global__ void __launch_bounds__(kThreads)
 k_dia_scatter(long nnz, const B *__restrict__ v, const int *__restrict__ map, B *__restrict__ dv, B pad, int *bad) {
     FIIM_FOR_ROWS(e, nnz) {
         const B o = v[e];
-        if (o == pad) atomicExch(bad, 1);
+        if (dia_is_pad(o, pad)) atomicExch(bad, 1);
         dv[map[e]] = o;
     }
 }
 
 // Whether new column indices (with unchanged row offsets) still fit the slices' diagonals:
-// entry e of row i must sit in slot map[e] = 32 k + i % 32 of a diagonal k of slice i / 32
-// (k0 <= k < k0 + m) whose offset is ci[e] - i. *bad is set otherwise. One thread per row.
+// entry e of row i must sit in slot map[e] = sh k + i % sh of a diagonal k of slice i / sh
+// (k0 <= k < k0 + m) whose offset is ci[e] - i; sh = 32 R rows a slice. *bad is set
+// otherwise. One thread per row.
 static __global__ void __launch_bounds__(kThreads)
 k_dia_check(int n, const int *__restrict__ rp, const int *__restrict__ ci, const int *__restrict__ map,
-            const int *__restrict__ rec, int rs, int *bad) {
+            const int *__restrict__ rec, int rs, int sh, int *bad) {
     FIIM_FOR_ROWS(i, (long)n) {
-        const int *r = rec + (i >> 5) * rs;
-        const int lane = (int)(i & 31), k0 = r[0], m = r[1];
+        const int *r = rec + (i / sh) * rs;
+        const int lane = (int)(i % sh), k0 = r[0], m = r[1] & kDiaCountMask;
         for (int e = rp[i]; e < rp[i + 1]; ++e) {
-            const int slot = map[e], k = (slot >> 5) - k0;
-            if ((slot & 31) != lane || k < 0 || k >= m || r[2 + k] != ci[e] - (int)i) {
+            const int slot = map[e], k = slot / sh - k0;
+            if (slot % sh != lane || k < 0 || k >= m || r[2 + k] != ci[e] - (int)i) {
                 atomicExch(bad, 1);
                 break;
             }

@@ -199,7 +199,7 @@ template <typename Epi>
 static cudaError_t spmv_dia(cudaStream_t s, const DevCsr &M, const double *x, const Epi &epi, DState *st,
                             double *partials) {
     const DiaView<double> view{M.drec, static_cast<const double *>(M.dvals), (int)M.n, M.nsl, M.drs};
-    auto kern = k_spmv_dia<double, double, 1, Epi>;
+    auto kern = k_spmv_dia<double, double, Epi>;
     return launch_k(kern, grid_for(kern, kWarps, M.nsl), 0, s, view, x, epi, st, partials);
 }
 
@@ -277,6 +277,7 @@ void release_dia(DevCsr &M) {
     M.drec = M.dmap = M.dbad = nullptr;
     M.dvals = nullptr;
     M.dvbytes = 0;
+    M.dsh = 0;
     M.dia = 0;
     M.nsl = 0;
     M.drs = 0;
@@ -291,7 +292,7 @@ bool dia_wanted() {
 
 template <typename B>
 static int place_bits(DevCsr &M, const void *vals, B pad, cudaStream_t s) {
-    const long slots = 32 * M.ndiag;
+    const long slots = (long)M.dsh * M.ndiag;
     B *dv = static_cast<B *>(M.dvals);
     k_dia_fill<B><<<stream_grid(k_dia_fill<B>, slots), kThreads, 0, s>>>(slots, dv, pad);
     FIIM_CUDA(cudaGetLastError());
@@ -339,11 +340,12 @@ int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes) {
     FIIM_CUDA(cudaMemcpyAsync(ci.data(), M.ci, sizeof(int) * nnz, cudaMemcpyDeviceToHost, s));
     FIIM_CUDA(cudaStreamSynchronize(s));
     const int *rp = M.hrp.data();
-    const int nsl = (n + 31) / 32;
+    const int R = 8 / vbytes, sh = 32 * R;   // rows a lane, rows a slice
+    const int nsl = (n + sh - 1) / sh;
     // The diagonals of a slice: its entries' col - row, sorted and distinct.
     auto diagonals = [&](int sl, std::vector<int> &d, int &unsorted) {
         d.clear();
-        const int r0 = sl * 32, r1 = std::min(n, r0 + 32);
+        const int r0 = sl * sh, r1 = std::min(n, r0 + sh);
         for (int i = r0; i < r1; ++i)
             for (int e = rp[i]; e < rp[i + 1]; ++e) {
                 if (e > rp[i] && ci[e] <= ci[e - 1]) unsorted = 1;
@@ -376,9 +378,9 @@ int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes) {
     const long ndiag = sp[nsl];
     const int rs = most <= 14 ? 16 : 32;
     // Kept only when it moves fewer bytes than the CSR streams it replaces.
-    const double dia_bytes = (double)vbytes * 32 * ndiag + 4.0 * rs * nsl;
+    const double dia_bytes = (double)vbytes * sh * ndiag + 4.0 * rs * nsl;
     const double csr_bytes_now = (double)nnz * (vbytes + (M.narrow ? 2 : 4)) + 4.0 * (n + 1);
-    if (!(dia_bytes < csr_bytes_now) || 32 * ndiag >= (1L << 31)) return FIIM_OK;
+    if (!(dia_bytes < csr_bytes_now) || (long)sh * ndiag >= (1L << 31)) return FIIM_OK;
     std::vector<int> rec((size_t)nsl * rs, 0), map(nnz);
 #pragma omp parallel
     {
@@ -388,19 +390,22 @@ int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes) {
         for (int sl = 0; sl < nsl; ++sl) {
             diagonals(sl, d, unused);
             int *r = rec.data() + (size_t)sl * rs;
+            const int r0 = sl * sh, r1 = std::min(n, r0 + sh);
+            // Every slot of the slice (rows r0 .. r0 + sh - 1, padding included) gathers a column
+            // r + d: the slice is flagged when one of them falls outside [0, n).
+            const bool outside = !d.empty() && ((long)r0 + d.front() < 0 || (long)r0 + sh - 1 + d.back() > n - 1);
             r[0] = sp[sl];
-            r[1] = (int)d.size();
+            r[1] = (int)d.size() | (outside ? kDiaClamp : 0);
             std::copy(d.begin(), d.end(), r + 2);
-            const int r0 = sl * 32, r1 = std::min(n, r0 + 32);
             for (int i = r0; i < r1; ++i)
                 for (int e = rp[i]; e < rp[i + 1]; ++e) {
                     const int k = (int)(std::lower_bound(d.begin(), d.end(), ci[e] - i) - d.begin());
-                    map[e] = 32 * (sp[sl] + k) + (i & 31);
+                    map[e] = sh * (sp[sl] + k) + (i - r0);
                 }
         }
     }
     const size_t b_rec = Arena::need(sizeof(int) * rec.size()), b_map = Arena::need(sizeof(int) * nnz),
-                 b_bad = Arena::need(sizeof(int)), b_v = Arena::need((size_t)vbytes * 32 * ndiag);
+                 b_bad = Arena::need(sizeof(int)), b_v = Arena::need((size_t)vbytes * sh * ndiag);
     char *mem = nullptr;
     if (cudaMalloc(&mem, b_rec + b_map + b_bad + b_v) != cudaSuccess) {
         cudaGetLastError();
@@ -413,6 +418,7 @@ int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes) {
     M.dbad = reinterpret_cast<int *>(mem + b_rec + b_map);
     M.dvals = mem + b_rec + b_map + b_bad;
     M.dvbytes = vbytes;
+    M.dsh = sh;
     M.nsl = nsl;
     M.drs = rs;
     M.ndiag = ndiag;
@@ -427,7 +433,7 @@ int dia_fits(DevCsr &M, cudaStream_t s, bool *fits) {
     if (!M.dia_mem) return FIIM_OK;
     FIIM_CUDA(cudaMemsetAsync(M.dbad, 0, sizeof(int), s));
     k_dia_check<<<stream_grid(k_dia_check, M.n), kThreads, 0, s>>>((int)M.n, M.rp, M.ci, M.dmap, M.drec, M.drs,
-                                                                   M.dbad);
+                                                                   M.dsh, M.dbad);
     FIIM_CUDA(cudaGetLastError());
     int bad = 0;
     FIIM_CUDA(cudaMemcpyAsync(&bad, M.dbad, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1156,7 +1162,7 @@ int Solver::reload(const int *Ai, const int *Aj, const double *Av, const int *Gi
         // Everything of the sliced-diagonal copy that a captured launch holds: a rebuilt copy
         // may reuse the freed allocation's address with another layout inside it.
         auto dia_args = [](const DevCsr &D) {
-            return std::make_tuple(D.dia, D.drec, D.dvals, D.nsl, D.drs);
+            return std::make_tuple(D.dia, D.drec, D.dvals, D.nsl, D.drs, D.dsh);
         };
         const auto was_dia = dia_args(M);
         if (M.rows_same && M.nblk > 0) {
