@@ -74,7 +74,7 @@ struct DevCsr {
     // Sliced-diagonal copy (kFormDia; fiim_kernels.cuh, k_spmv_dia), in its own allocation.
     int dia = 0;                 // 1: built and current
     int nsl = 0;                 // slices of dsh rows
-    int dsh = 0;                 // rows a slice: 32 R, R = 8 / dvbytes rows a lane
+    int dsh = 0;                 // rows a slice: 32 R, R rows a lane (dia_rows_per_lane)
     int drs = 0;                 // ints per slice record (16 or 32): first diagonal, count, offsets
     long ndiag = 0;              // diagonals over all slices (dsh slots each)
     int *drec = nullptr;         // nsl records
@@ -138,7 +138,7 @@ int set_tile(DevCsr &M, int tile, cudaStream_t s);
 int build_narrow(DevCsr &M, cudaStream_t s);
 // The sliced-diagonal copy of M (fiim_kernels.cuh, k_spmv_dia). build_dia_structure lays it
 // out (slice records, the slot of every entry) for values of vbytes bytes (8, 4 or 2) when
-// M's rows are sorted by column, every slice (32 R rows, R = 8 / vbytes) has at most
+// M's rows are sorted by column, every slice (32 R rows, R = dia_rows_per_lane) has at most
 // kDiaMaxDiags diagonals and the copy moves fewer bytes than the CSR streams (M.dia_mem
 // stays null otherwise);
 // place_dia moves the nnz values `vals` (device, that width) into it and sets M.dia = 1,
@@ -149,6 +149,10 @@ int build_narrow(DevCsr &M, cudaStream_t s);
 // still fit and rebuilds otherwise. release_dia frees the copy; dia_wanted is false under
 // FIIM_DIA=0 or FIIM_SPMV=rows / staged / warp.
 bool dia_wanted();
+// Rows a lane of the sliced-diagonal copy for values of vbytes bytes: 2 for FP32, 4 for BF16;
+// for FP64 0, which lets build_dia_structure choose 1 or 2 by the matrix (FIIM_DIA_R=1 or 2
+// forces one).
+int dia_rows_per_lane(int vbytes);
 
 int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes);
 int place_dia(DevCsr &M, const void *vals, cudaStream_t s);

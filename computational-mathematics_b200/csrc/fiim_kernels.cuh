@@ -645,7 +645,6 @@ constexpr unsigned kDiaPad32 = 0xFFD1A6B5u;
 constexpr unsigned short kDiaPad16 = 0xFFD1u;
 constexpr int kDiaMaxDiags = 30;   // diagonals of one slice at most (record of 32 ints)
 constexpr int kDiaCountMask = 0xffff, kDiaClamp = 1 << 30;   // record[1]: count | clamp flag
-constexpr int kDiaChunk = 8;       // diagonals in flight per thread (4 for BF16's 4 rows a lane)
 
 template <typename V = double>
 struct DiaView {
@@ -654,19 +653,26 @@ struct DiaView {
     int n, nsl, rs;
 };
 
-// A lane's R values of one diagonal (one 8-byte load, streamed) and the padding test; BF16 is
-// widened by a shift or a mask, so the padding keeps its pattern in the upper half.
-template <typename V>
+// A lane's R values of one diagonal (one load of R values, streamed) and the padding test;
+// BF16 is widened by a shift or a mask, so the padding keeps its pattern in the upper half.
+// R is 1 or 2 for FP64, 2 for FP32, 4 for BF16.
+template <typename V, int R>
 struct DiaLoad;
-template <>
-struct DiaLoad<double> {   // the upper word decides: no entry of a served matrix shares it
-    static constexpr int R = 1;
-    static __device__ __forceinline__ void get(const double *p, double (&a)[1]) { a[0] = ldm(p); }
+template <int R>
+struct DiaLoad<double, R> {   // the upper word decides: no entry of a served matrix shares it
+    static __device__ __forceinline__ void get(const double *p, double (&a)[R]) {
+        if constexpr (R == 2) {
+            const double2 w = __ldcs(reinterpret_cast<const double2 *>(p));
+            a[0] = w.x;
+            a[1] = w.y;
+        } else {
+            a[0] = ldm(p);
+        }
+    }
     static __device__ __forceinline__ bool pad(double a) { return __double2hiint(a) == (int)(kDiaPad >> 32); }
 };
 template <>
-struct DiaLoad<float> {
-    static constexpr int R = 2;
+struct DiaLoad<float, 2> {
     static __device__ __forceinline__ void get(const float *p, float (&a)[2]) {
         const float2 w = __ldcs(reinterpret_cast<const float2 *>(p));
         a[0] = w.x;
@@ -675,8 +681,7 @@ struct DiaLoad<float> {
     static __device__ __forceinline__ bool pad(float a) { return __float_as_uint(a) == kDiaPad32; }
 };
 template <>
-struct DiaLoad<__nv_bfloat16> {
-    static constexpr int R = 4;
+struct DiaLoad<__nv_bfloat16, 4> {
     static __device__ __forceinline__ void get(const __nv_bfloat16 *p, float (&a)[4]) {
         const uint2 w = __ldcs(reinterpret_cast<const uint2 *>(p));
         a[0] = __uint_as_float(w.x << 16);
@@ -695,11 +700,12 @@ __device__ __forceinline__ float dia_fma(float s, float a, float x) { return __f
 // [0, n) (padding slots may point outside; their x is never used).
 template <bool CLAMP, int R, typename T>
 __device__ __forceinline__ void dia_gather(const T *__restrict__ x, int row0, int d, int n, T (&xv)[R]) {
-    if constexpr (!CLAMP && R >= 2 && sizeof(T) == 4) {
+    if constexpr (!CLAMP && R >= 2) {
         if ((d & 1) == 0) {
+            using T2 = std::conditional_t<sizeof(T) == 8, double2, float2>;
 #pragma unroll
             for (int j = 0; j < R; j += 2) {
-                const float2 w = __ldg(reinterpret_cast<const float2 *>(x + row0 + d + j));
+                const T2 w = __ldg(reinterpret_cast<const T2 *>(x + row0 + d + j));
                 xv[j] = w.x;
                 xv[j + 1] = w.y;
             }
@@ -724,11 +730,11 @@ __device__ __forceinline__ void dia_gather(const T *__restrict__ x, int row0, in
 // without it, with paired FP32 gathers; for FP64 that path lost its loads' overlap (long-
 // scoreboard stalls 15.4 against 7.2 an issue, H's product 67.0 against 47.7 us under ncu),
 // so FP64 always clamps.
-template <typename V, typename T, typename Epi>
+template <typename V, typename T, int R, typename Epi>
 static __global__ void __launch_bounds__(kThreads)
 k_spmv_dia(DiaView<V> M, const T *__restrict__ x, Epi epi, DState *st, double *__restrict__ partials) {
-    constexpr int R = DiaLoad<V>::R, SH = 32 * R;
-    constexpr int C = R >= 4 ? kDiaChunk / 2 : kDiaChunk;   // about 32 values in flight a thread
+    constexpr int SH = 32 * R;
+    constexpr int C = 64 / (R * (int)sizeof(T));   // diagonals a chunk: 64 bytes of values a thread
     pdl_enter();
     if (Epi::GATED && st != nullptr && st->done) return;
     double red[Epi::NR];
@@ -765,7 +771,7 @@ k_spmv_dia(DiaView<V> M, const T *__restrict__ x, Epi epi, DState *st, double *_
                         xv[u][j] = T(0);
                     }
                     if (k + u < m) {
-                        DiaLoad<V>::get(M.v + (long)(k0 + k + u) * SH + R * lane, a[u]);
+                        DiaLoad<V, R>::get(M.v + (long)(k0 + k + u) * SH + R * lane, a[u]);
                         dia_gather<CL, R>(x, row0, d, M.n, xv[u]);
                     }
                 }
@@ -773,7 +779,7 @@ k_spmv_dia(DiaView<V> M, const T *__restrict__ x, Epi epi, DState *st, double *_
                 for (int u = 0; u < C; ++u)
 #pragma unroll
                     for (int j = 0; j < R; ++j)
-                        if (k + u < m && !DiaLoad<V>::pad(a[u][j])) s[j] = dia_fma(s[j], a[u][j], xv[u][j]);
+                        if (k + u < m && !DiaLoad<V, R>::pad(a[u][j])) s[j] = dia_fma(s[j], a[u][j], xv[u][j]);
             }
         };
         if (R == 1 || (mf & kDiaClamp)) sum(std::true_type{});

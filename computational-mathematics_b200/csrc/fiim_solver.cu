@@ -199,7 +199,11 @@ template <typename Epi>
 static cudaError_t spmv_dia(cudaStream_t s, const DevCsr &M, const double *x, const Epi &epi, DState *st,
                             double *partials) {
     const DiaView<double> view{M.drec, static_cast<const double *>(M.dvals), (int)M.n, M.nsl, M.drs};
-    auto kern = k_spmv_dia<double, double, Epi>;
+    if (M.dsh == 64) {
+        auto kern = k_spmv_dia<double, double, 2, Epi>;
+        return launch_k(kern, grid_for(kern, kWarps, M.nsl), 0, s, view, x, epi, st, partials);
+    }
+    auto kern = k_spmv_dia<double, double, 1, Epi>;
     return launch_k(kern, grid_for(kern, kWarps, M.nsl), 0, s, view, x, epi, st, partials);
 }
 
@@ -327,6 +331,14 @@ static int col_hash(DevCsr &M, cudaStream_t s, unsigned long long *h) {
     return FIIM_OK;
 }
 
+int dia_rows_per_lane(int vbytes) {
+    if (vbytes == 8) {
+        const char *e = std::getenv("FIIM_DIA_R");
+        return (e && (e[0] == '1' || e[0] == '2') && e[1] == 0) ? e[0] - '0' : 0;   // 0: by the matrix
+    }
+    return vbytes == 4 ? 2 : 4;
+}
+
 int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes) {
     release_dia(M);
     M.dia_tried = false;
@@ -340,9 +352,8 @@ int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes) {
     FIIM_CUDA(cudaMemcpyAsync(ci.data(), M.ci, sizeof(int) * nnz, cudaMemcpyDeviceToHost, s));
     FIIM_CUDA(cudaStreamSynchronize(s));
     const int *rp = M.hrp.data();
-    const int R = 8 / vbytes, sh = 32 * R;   // rows a lane, rows a slice
-    const int nsl = (n + sh - 1) / sh;
-    // The diagonals of a slice: its entries' col - row, sorted and distinct.
+    // The diagonals of a slice of sh rows: its entries' col - row, sorted and distinct.
+    int sh = 0, nsl = 0;
     auto diagonals = [&](int sl, std::vector<int> &d, int &unsorted) {
         d.clear();
         const int r0 = sl * sh, r1 = std::min(n, r0 + sh);
@@ -354,22 +365,45 @@ int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes) {
         std::sort(d.begin(), d.end());
         d.erase(std::unique(d.begin(), d.end()), d.end());
     };
-    std::vector<int> sp(nsl + 1, 0);
-    int fail = 0;
+    // Diagonals per slice for R rows a lane (sp[sl + 1]); false when a row is unsorted or a
+    // slice has more than kDiaMaxDiags.
+    std::vector<int> sp;
+    auto count = [&](int R) -> bool {
+        sh = 32 * R;
+        nsl = (n + sh - 1) / sh;
+        sp.assign(nsl + 1, 0);
+        int fail = 0;
 #pragma omp parallel
-    {
-        std::vector<int> d;
-        int bad = 0;
+        {
+            std::vector<int> d;
+            int bad = 0;
 #pragma omp for schedule(dynamic, 256)
-        for (int sl = 0; sl < nsl; ++sl) {
-            diagonals(sl, d, bad);
-            sp[sl + 1] = (int)d.size();
-            if ((int)d.size() > kDiaMaxDiags) bad = 1;
-        }
+            for (int sl = 0; sl < nsl; ++sl) {
+                diagonals(sl, d, bad);
+                sp[sl + 1] = (int)d.size();
+                if ((int)d.size() > kDiaMaxDiags) bad = 1;
+            }
 #pragma omp atomic
-        fail |= bad;
+            fail |= bad;
+        }
+        return !fail;
+    };
+    // FP64 takes two rows a lane when its 32-row slices average more diagonals than one chunk
+    // of the kernel holds (H at 128^3: 11 diagonals, 32.9 against 41.6 us a product; A and G,
+    // 7 diagonals, were slower with two).
+    int R = dia_rows_per_lane(vbytes);
+    if (R == 0) {
+        if (!count(1)) return FIIM_OK;
+        long nd1 = 0;
+        for (int sl = 0; sl < nsl; ++sl) nd1 += sp[sl + 1];
+        R = 1;
+        if (nd1 > 8L * nsl) {
+            if (count(2)) R = 2;
+            else if (!count(1)) return FIIM_OK;
+        }
+    } else if (!count(R)) {
+        return FIIM_OK;
     }
-    if (fail) return FIIM_OK;
     int most = 0;
     for (int sl = 0; sl < nsl; ++sl) {
         most = std::max(most, sp[sl + 1]);
