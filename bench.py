@@ -973,7 +973,7 @@ def main():
     # DRAM bytes per launch of the dominant kernel (H's SpMV) from an ncu capture of the
     # 128^3 workload (dram__bytes_read.sum + dram__bytes_write.sum, mean of three H launches:
     # 0.817 x its algorithmic bytes, the column stream being stored as 16-bit offsets).
-    ap.add_argument("--ncu-traffic", type=float, default=221.8e6,
+    ap.add_argument("--ncu-traffic", type=float, default=220.0e6,
                     help="dram bytes per launch of the dominant kernel from an ncu capture")
     ap.add_argument("--dry-run", action="store_true",
                     help="no GPU: check the rank launcher and max-over-ranks timing over gloo (solves nothing)")
