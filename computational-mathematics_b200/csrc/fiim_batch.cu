@@ -10,7 +10,8 @@
 //
 // Layout: CSR per matrix + row blocks aligned to systems (blk_sys, sys_blk); factor values
 // FP64, FP32 or BF16 (fiim_options.precision); A, D^-1 and all vectors FP64; per-system
-// state as arrays of nsys entries.
+// state as arrays of nsys entries. Each matrix whose rows allow it also has a sliced-diagonal
+// copy with slices inside the systems, which serves its products (FIIM_DIA=0: CSR streams).
 
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
@@ -38,6 +39,10 @@ struct BMat {
     int *flag = nullptr;                           // device: finished-system flag per row block
     float *v32 = nullptr;
     __nv_bfloat16 *v16 = nullptr;
+    // With a sliced-diagonal copy (M.dia): finished-system flag per slice and each system's
+    // first slice (device, one allocation).
+    int *sflag = nullptr, *sys_sl = nullptr;
+    void *sl_mem = nullptr;
 };
 
 // Row blocks per system: consecutive rows of one system, <= max_rows rows, <= tile entries.
@@ -94,6 +99,20 @@ struct BatchSolver : SolverBase {
 
     template <typename V, typename Epi>
     cudaError_t spmv(const BMat &B, const V *vals, const double *xx, const Epi &epi) {
+        if (B.M.dia) {   // its sliced-diagonal copy (values of V's width: 2 rows a lane for FP32)
+            const DiaView<V> view{B.M.drec, static_cast<const V *>(B.M.dvals), (int)B.M.n, B.M.nsl, B.M.drs};
+            if constexpr (sizeof(V) == 8) {
+                if (B.M.dsh == 64) {
+                    auto k2 = bt::k_bspmv_dia<V, 2, Epi>;
+                    return launch_k(k2, grid_for(k2, kWarps, B.M.nsl), 0, stream, view, B.sflag, xx, epi, bs, partials);
+                }
+                auto k1 = bt::k_bspmv_dia<V, 1, Epi>;
+                return launch_k(k1, grid_for(k1, kWarps, B.M.nsl), 0, stream, view, B.sflag, xx, epi, bs, partials);
+            } else {
+                auto kd = bt::k_bspmv_dia<V, sizeof(V) == 4 ? 2 : 4, Epi>;
+                return launch_k(kd, grid_for(kd, kWarps, B.M.nsl), 0, stream, view, B.sflag, xx, epi, bs, partials);
+            }
+        }
         auto kern = bt::k_bspmv<kTile, V, Epi, false>;
         const int g = sgrid(kern, B.M.nblk);
         if (B.M.narrow) {
@@ -111,11 +130,44 @@ struct BatchSolver : SolverBase {
         return spmv(B, B.M.v, xx, epi);
     }
 
-    // Second phase of a per-system reduction over matrix B's row blocks (bt::k_bfinish).
+    // Second phase of a per-system reduction (bt::k_bfinish) after a product with matrix B:
+    // over its slices when its sliced-diagonal copy served, else over its row blocks.
     template <int NR, bool GATED = true, class Fin>
     cudaError_t finish(const BMat &B, const Fin &fin) {
         const int g = (int)std::min<long>(nsys, 8L * num_sms());
-        return launch_k(bt::k_bfinish<NR, GATED, Fin>, g, 0, stream, B.sys_blk, nsys, partials, bs, fin);
+        if (B.M.dia) return launch_k(bt::k_bfinish<NR, GATED, Fin>, g, 0, stream, B.sys_sl, 1, nsys, partials, bs, fin);
+        return launch_k(bt::k_bfinish<NR, GATED, Fin>, g, 0, stream, B.sys_blk, kWarps, nsys, partials, bs, fin);
+    }
+    // ... after a vector update, which walks A's row blocks.
+    template <int NR, class Fin>
+    cudaError_t finish_rows(const Fin &fin) {
+        const int g = (int)std::min<long>(nsys, 8L * num_sms());
+        return launch_k(bt::k_bfinish<NR, true, Fin>, g, 0, stream, A.sys_blk, kWarps, nsys, partials, bs, fin);
+    }
+
+    // The sliced-diagonal copy of B (fiim_internal.h, build_dia_structure) with slices inside
+    // the systems, its values `vals` (device, the stored width vbytes), its slice flags and the
+    // systems' first slices; B keeps its CSR streams when the matrix does not allow it.
+    int build_copy(BMat &B, int m, int vbytes, const void *vals) {
+        FIIM_TRY(build_dia_structure(B.M, stream, vbytes, &sys_rows));
+        if (!B.M.dia_mem) return FIIM_OK;
+        FIIM_TRY(place_dia(B.M, vals, stream));
+        if (!B.M.dia) return FIIM_OK;
+        const size_t bf = Arena::need(sizeof(int) * std::max(B.M.nsl, 1)), bsl = Arena::need(sizeof(int) * (nsys + 1));
+        char *mem = nullptr;
+        if (cudaMalloc(&mem, bf + bsl) != cudaSuccess) {
+            cudaGetLastError();
+            release_dia(B.M);   // no room: the CSR streams serve
+            return FIIM_OK;
+        }
+        B.sl_mem = mem;
+        B.sflag = reinterpret_cast<int *>(mem);
+        B.sys_sl = reinterpret_cast<int *>(mem + bf);
+        FIIM_CUDA(cudaMemcpyAsync(B.sys_sl, B.M.hseg_sl.data(), sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice,
+                                  stream));
+        FIIM_CUDA(cudaStreamSynchronize(stream));
+        bs.bf[3 + m] = bt::BlockFlags{B.sflag, B.sys_sl};
+        return FIIM_OK;
     }
 
     int enqueue_iteration(bool cond, cudaGraphConditionalHandle h) {
@@ -127,14 +179,14 @@ struct BatchSolver : SolverBase {
         FIIM_CUDA(finish<1>(A, bt::BEpiAlpha{v, r0}));
         FIIM_CUDA(launch_k(bt::k_bupdate_s, sgrid(bt::k_bupdate_s, nb), 0, stream, A.M.rb, A.blk_sys, A.sys_blk,
                            nb, r, v, x, sv, bs, partials));
-        FIIM_CUDA(finish<2>(A, bt::BFinS{}));
+        FIIM_CUDA(finish_rows<2>(bt::BFinS{}));
         FIIM_CUDA(spmv_f(H, sv, bt::BEpiScale{tm, IDv}));
         FIIM_CUDA(spmv_f(G, tm, bt::BEpiStore{sc}));
         FIIM_CUDA(spmv(A, A.M.v, sc, bt::BEpiOmega{t, sv}));
         FIIM_CUDA(finish<2>(A, bt::BEpiOmega{t, sv}));
         FIIM_CUDA(launch_k(bt::k_bupdate_xr, sgrid(bt::k_bupdate_xr, nb), 0, stream, A.M.rb, A.blk_sys, A.sys_blk,
                            nb, pc, sc, sv, t, r0, x, r, bs, partials));
-        FIIM_CUDA(finish<1>(A, bt::BFinControl{}));
+        FIIM_CUDA(finish_rows<1>(bt::BFinControl{}));
         FIIM_CUDA(launch_k(bt::k_bupdate_p, sgrid(bt::k_bupdate_p, nb), 0, stream, A.M.rb, A.blk_sys, nb, r, v, p,
                            bs, h, cond ? 1 : 0));
         return FIIM_OK;
@@ -252,9 +304,16 @@ struct BatchSolver : SolverBase {
             FIIM_CUDA(cudaGetLastError());
         }
         for (int m = 0; m < 3; ++m) FIIM_TRY(set_blocks(*mats[m]));
-        // Per-warp partials of the largest block count (two values each).
-        const long maxblk = std::max({(long)A.M.nblk, (long)G.M.nblk, (long)H.M.nblk, 1L});
-        FIIM_CUDA(cudaMalloc(&partials, sizeof(double) * 2 * kWarps * maxblk));
+        // Sliced-diagonal copies where the matrices allow them: A in FP64, G and H in the
+        // factors' stored precision.
+        const int fvb = f16 ? 2 : (f32 ? 4 : 8);
+        FIIM_TRY(build_copy(A, 0, 8, A.M.v));
+        FIIM_TRY(build_copy(G, 1, fvb, f16 ? (const void *)G.v16 : f32 ? (const void *)G.v32 : (const void *)G.M.v));
+        FIIM_TRY(build_copy(H, 2, fvb, f16 ? (const void *)H.v16 : f32 ? (const void *)H.v32 : (const void *)H.M.v));
+        // Partials of the largest count: per warp of a row block, or per slice (two values each).
+        long maxq = std::max({(long)A.M.nblk, (long)G.M.nblk, (long)H.M.nblk, 1L}) * kWarps;
+        for (const BMat *B : {&A, &G, &H}) maxq = std::max(maxq, (long)B->M.nsl);
+        FIIM_CUDA(cudaMalloc(&partials, sizeof(double) * 2 * maxq));
         // per-system divergence windows (AFIIM/src/bicgstab.cpp:114, ACIFIM/src/bicgstab.cpp:132)
         std::vector<int> mm(nsys);
         for (int k = 0; k < nsys; ++k) {
@@ -282,8 +341,10 @@ struct BatchSolver : SolverBase {
         FIIM_CUDA(cudaMemcpyAsync(bs.g, hg, sizeof(bt::BGlobal), cudaMemcpyHostToDevice, stream));
         FIIM_CUDA(cudaMemsetAsync(bs.done, 0, sizeof(int) * nsys, stream));
         FIIM_CUDA(cudaMemsetAsync(bs.info, 0xff, sizeof(int) * nsys, stream));   // -1
-        for (const BMat *B : {&A, &G, &H})
+        for (const BMat *B : {&A, &G, &H}) {
             FIIM_CUDA(cudaMemsetAsync(B->flag, 0, sizeof(int) * std::max(B->M.nblk, 1), stream));
+            if (B->sflag) FIIM_CUDA(cudaMemsetAsync(B->sflag, 0, sizeof(int) * std::max(B->M.nsl, 1), stream));
+        }
         return FIIM_OK;
     }
 
@@ -292,8 +353,10 @@ struct BatchSolver : SolverBase {
         FIIM_TRY(reset_state(0.0, 0));
         std::vector<int> ones(nsys, 1);
         FIIM_CUDA(cudaMemcpyAsync(bs.done, ones.data(), sizeof(int) * nsys, cudaMemcpyHostToDevice, stream));
-        for (const BMat *B : {&A, &G, &H})   // nonzero: finished
+        for (const BMat *B : {&A, &G, &H}) {   // nonzero: finished
             FIIM_CUDA(cudaMemsetAsync(B->flag, 1, sizeof(int) * std::max(B->M.nblk, 1), stream));
+            if (B->sflag) FIIM_CUDA(cudaMemsetAsync(B->sflag, 1, sizeof(int) * std::max(B->M.nsl, 1), stream));
+        }
         FIIM_TRY(enqueue_iteration(false, cudaGraphConditionalHandle{}));
         FIIM_CUDA(cudaStreamSynchronize(stream));
         // FIIM_GRAPH=host: a graph of one loop iteration, relaunched by the host (the same
@@ -441,6 +504,12 @@ struct BatchSolver : SolverBase {
         if (hg) cudaFreeHost(hg);
         if (partials) cudaFree(partials);
         partials = nullptr;
+        for (BMat *B : {&A, &G, &H}) {
+            if (B->sl_mem) cudaFree(B->sl_mem);
+            B->sl_mem = nullptr;
+            B->sflag = B->sys_sl = nullptr;
+            release_dia(B->M);
+        }
         exec = nullptr;
         graph = nullptr;
         ev0 = ev1 = nullptr;

@@ -22,9 +22,9 @@ struct BGlobal {
     int loops_total;   // verified solves: loop bodies of the runs before the current one
 };
 
-// Finished-system flags per row block of one matrix (batched solve; NULL elsewhere):
-// flag[b] != 0 once the system of block b has left the loop, so a kernel can skip a block
-// with one load that needs no other.
+// Finished-system flags per row block (or per slice of a sliced-diagonal copy) of one matrix
+// (batched solve; NULL elsewhere): flag[b] != 0 once the system of block b has left the loop,
+// so a kernel can skip a block with one load that needs no other.
 struct BlockFlags {
     int *flag;
     const int *sys_blk;   // nsys + 1 block offsets per system
@@ -36,14 +36,14 @@ struct BState {
     int *iter, *stag, *msteps, *maxmsteps, *info, *done;
     unsigned int *ticket;   // per-system tickets (the block solver's last-CTA reductions)
     BGlobal *g;
-    BlockFlags bf[3];       // A, G, H row blocks (batched solve)
+    BlockFlags bf[6];       // A, G, H row blocks, then the slices of their sliced-diagonal copies
 };
 
 __device__ __forceinline__ void retire(BState &bs, int k, int info) {
     bs.info[k] = info;
     bs.done[k] = 1;
     atomicSub(&bs.g->active, 1);
-    for (int m = 0; m < 3; ++m)
+    for (int m = 0; m < 6; ++m)
         if (bs.bf[m].flag)
             for (int b = bs.bf[m].sys_blk[k]; b < bs.bf[m].sys_blk[k + 1]; ++b) bs.bf[m].flag[b] = 1;
 }
@@ -92,7 +92,7 @@ static __global__ void __launch_bounds__(kThreads) k_bverify(int nsys, BState bs
         if (!verify_misses(bs, k)) continue;
         bs.done[k] = 0;
         bs.info[k] = -1;
-        for (int m = 0; m < 3; ++m)
+        for (int m = 0; m < 6; ++m)
             if (bs.bf[m].flag)
                 for (int b = bs.bf[m].sys_blk[k]; b < bs.bf[m].sys_blk[k + 1]; ++b) bs.bf[m].flag[b] = 0;
         atomicAdd(&bs.g->active, 1);
@@ -226,16 +226,19 @@ __device__ __forceinline__ void warp_partials(double (&v)[NR], int blk, double *
 
 // One CTA per system (grid-stride over systems): thread t adds partials t, t + 256, ...
 // of the system, then the CTA's warp trees and the warp totals in warp order (a fixed
-// order). Systems whose loop has ended are left alone when GATED.
+// order). Systems whose loop has ended are left alone when GATED. A system's partials are
+// [sys_blk[k] qmul, sys_blk[k + 1] qmul): qmul = kWarps for row-block partials (one per warp
+// of a block), 1 for slice partials (one per slice).
 template <int NR, bool GATED, class Fin>
 static __global__ void __launch_bounds__(kThreads)
-k_bfinish(const int *__restrict__ sys_blk, int nsys, const double *__restrict__ partials, BState bs, Fin fin) {
+k_bfinish(const int *__restrict__ sys_blk, int qmul, int nsys, const double *__restrict__ partials, BState bs,
+          Fin fin) {
     pdl_enter();
     __shared__ double sm[kWarps][NR];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int k = blockIdx.x; k < nsys; k += gridDim.x) {
         if (GATED && bs.done[k]) continue;             // uniform in the CTA
-        const int q0 = __ldg(sys_blk + k) * kWarps, q1 = __ldg(sys_blk + k + 1) * kWarps;
+        const int q0 = __ldg(sys_blk + k) * qmul, q1 = __ldg(sys_blk + k + 1) * qmul;
         double acc[NR];
 #pragma unroll
         for (int j = 0; j < NR; ++j) acc[j] = 0.0;
@@ -365,6 +368,45 @@ k_bspmv(CsrView<V> M, const int *__restrict__ rb, const int *__restrict__ eb, co
             if (nxt < nblk) fetch(nxt);
         }
         if constexpr (Epi::REDUCES) warp_partials<Epi::NR>(red, blk, partials);
+    }
+    pdl_release();
+}
+
+// ---------------------------------------------------------------- batched sliced-diagonal SpMV
+// The single-system kernel's slices (dia_slice in fiim_kernels.cuh), which never straddle two
+// systems: one warp per slice, grid-stride, a finished system's slices skipped (sflag, set with
+// the system's done flag), and each slice's reductions stored as one partial (lane 0, after
+// the warp's tree) for the per-system finish (qmul = 1). Factor values stored in FP32 or BF16
+// are widened to FP64 at the rounded product, as in k_bspmv.
+template <typename V, int R, typename Epi>
+static __global__ void __launch_bounds__(kThreads)
+k_bspmv_dia(DiaView<V> M, const int *__restrict__ sflag, const double *__restrict__ x, Epi epi, BState bs,
+            double *__restrict__ partials) {
+    pdl_enter();
+    const int lane = (int)threadIdx.x & 31;
+    const int nw = (int)gridDim.x * kWarps;
+    int sl = (int)blockIdx.x * kWarps + ((int)threadIdx.x >> 5);
+    int rec = (sl < M.nsl && lane < M.rs) ? __ldg(M.rec + (long)sl * M.rs + lane) : 0;
+    for (; sl < M.nsl; sl += nw) {
+        const int nxt = sl + nw;
+        const int rec_next = (nxt < M.nsl && lane < M.rs) ? __ldg(M.rec + (long)nxt * M.rs + lane) : 0;
+        if (!(Epi::GATED && sflag[sl])) {   // uniform in the warp
+            double red[Epi::NR];
+#pragma unroll
+            for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
+            dia_slice<V, double, R>(M, x, epi, rec, lane, [&](int row, double s, double opnd) {
+                if constexpr (HasPre<Epi>::value) epi.emit_pre(row, s, opnd, red);
+                else epi.emit(row, s, red);
+            });
+            if constexpr (Epi::REDUCES) {
+#pragma unroll
+                for (int j = 0; j < Epi::NR; ++j) red[j] = warp_sum(red[j]);
+                if (lane == 0)
+#pragma unroll
+                    for (int j = 0; j < Epi::NR; ++j) partials[(size_t)sl * Epi::NR + j] = red[j];
+            }
+        }
+        rec = rec_next;
     }
     pdl_release();
 }

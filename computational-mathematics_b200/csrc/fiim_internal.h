@@ -87,6 +87,7 @@ struct DevCsr {
     bool dia_tried = false;      // the copy was considered for the columns hashed in dia_cols
     unsigned long long dia_cols = 0;
     unsigned long long *dhash = nullptr;   // device scratch of the column hash (in the arena)
+    std::vector<int> hseg_sl;    // first slice of each segment (host), segments + 1 entries
     std::vector<int> hrp;        // row offsets on the host (row blocks, tuning key)
     bool rows_same = false;      // the last upload_csr found the same row offsets as before
     std::vector<long> sig;       // tuning-cache key: n, nnz, sampled row offsets
@@ -137,7 +138,9 @@ int set_tile(DevCsr &M, int tile, cudaStream_t s);
 // Builds the narrow column stream (cd, cb) of M's row blocks (eb) when every block allows it.
 int build_narrow(DevCsr &M, cudaStream_t s);
 // The sliced-diagonal copy of M (fiim_kernels.cuh, k_spmv_dia). build_dia_structure lays it
-// out (slice records, the slot of every entry) for values of vbytes bytes (8, 4 or 2) when
+// out (slice records, the slot of every entry; slices never straddle a boundary of
+// `segments`, ascending row starts from 0 to n, one segment when null) for values of vbytes
+// bytes (8, 4 or 2) when
 // M's rows are sorted by column, every slice (32 R rows, R = dia_rows_per_lane) has at most
 // kDiaMaxDiags diagonals and the copy moves fewer bytes than the CSR streams (M.dia_mem
 // stays null otherwise);
@@ -154,7 +157,7 @@ bool dia_wanted();
 // forces one).
 int dia_rows_per_lane(int vbytes);
 
-int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes);
+int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes, const std::vector<int> *segments = nullptr);
 int place_dia(DevCsr &M, const void *vals, cudaStream_t s);
 int dia_fits(DevCsr &M, cudaStream_t s, bool *fits);
 int build_dia(DevCsr &M, cudaStream_t s);

@@ -627,28 +627,30 @@ k_narrow_cols(const int *__restrict__ ci, const int *__restrict__ eb, int nblk, 
 }
 
 // ---------------------------------------------------------------- sliced-diagonal SpMV
-// The sliced-diagonal form of a CSR matrix whose rows, a slice of 32 R at a time, share a few
-// diagonals (R rows a lane: 1 for FP64 values, 2 for FP32, 4 for BF16, so that a lane's values
-// of one diagonal are one 8-byte word). Slice s holds rows 32 R s .. 32 R s + 32 R - 1 and the
-// union of their entries' diagonals d = col - row, ascending; each diagonal stores one value
-// per row of the slice (v[32 R k + row - 32 R s], k counted over all slices). A row's own
-// entries keep their storage order (rows are sorted by column), and a slot the row has no
-// entry in holds the padding pattern (kDiaPad, kDiaPad32, kDiaPad16: NaN bit patterns no
-// entry of the matrix holds, checked when the values are placed). Each slice has a record of
-// rs ints (16 or 32): its first diagonal k0, its count m (with kDiaClamp when a diagonal
-// reaches outside the matrix from one of its rows) and its m offsets, which a warp reads in
-// one coalesced load. Bytes per entry: the value's width and the padding, plus 2 or 4 per
-// R rows for the records, against the width plus 2 or 4 per entry and 4 per row for the CSR
-// streams.
+// The sliced-diagonal form of a CSR matrix whose rows, a slice of up to 32 R at a time, share a
+// few diagonals (R rows a lane: 1 or 2 for FP64 values, 2 for FP32, 4 for BF16, so that a
+// lane's values of one diagonal are one load). Slices never straddle a segment boundary (the
+// systems of a batch; one segment for a single system), so a segment's last slice may hold
+// fewer rows. Slice s holds its rows' diagonals d = col - row, ascending; each diagonal stores
+// one value per row slot of the slice (v[32 R k + row - first row], k counted over all
+// slices). A row's own entries keep their storage order (rows are sorted by column), and a
+// slot the row has no entry in holds the padding pattern (kDiaPad, kDiaPad32, kDiaPad16: NaN
+// bit patterns no entry of the matrix holds, checked when the values are placed). Each slice
+// has a record of rs ints (16 or 32): its first diagonal k0, its count m (with kDiaClamp when
+// a slot's column falls outside the matrix), its first row, its row count and its m offsets,
+// which a warp reads in one coalesced load. Bytes per entry: the value's width and the
+// padding, plus 2 or 4 per R rows for the records, against the width plus 2 or 4 per entry
+// and 4 per row for the CSR streams.
 constexpr unsigned long long kDiaPad = 0xFFF7D1A6B00C5A1DULL;   // FP64 padding; FP32 and BF16 below
 constexpr unsigned kDiaPad32 = 0xFFD1A6B5u;
 constexpr unsigned short kDiaPad16 = 0xFFD1u;
-constexpr int kDiaMaxDiags = 30;   // diagonals of one slice at most (record of 32 ints)
+constexpr int kDiaRecHead = 4;     // record: k0, count | flags, first row, rows; then offsets
+constexpr int kDiaMaxDiags = 32 - kDiaRecHead;   // diagonals of one slice at most
 constexpr int kDiaCountMask = 0xffff, kDiaClamp = 1 << 30;   // record[1]: count | clamp flag
 
 template <typename V = double>
 struct DiaView {
-    const int *__restrict__ rec;      // nsl records of rs ints: k0, m, offsets
+    const int *__restrict__ rec;      // nsl records of rs ints: k0, m, first row, rows, offsets
     const V *__restrict__ v;          // 32 R values per diagonal
     int n, nsl, rs;
 };
@@ -660,6 +662,7 @@ template <typename V, int R>
 struct DiaLoad;
 template <int R>
 struct DiaLoad<double, R> {   // the upper word decides: no entry of a served matrix shares it
+    using E = double;
     static __device__ __forceinline__ void get(const double *p, double (&a)[R]) {
         if constexpr (R == 2) {
             const double2 w = __ldcs(reinterpret_cast<const double2 *>(p));
@@ -673,6 +676,7 @@ struct DiaLoad<double, R> {   // the upper word decides: no entry of a served ma
 };
 template <>
 struct DiaLoad<float, 2> {
+    using E = float;
     static __device__ __forceinline__ void get(const float *p, float (&a)[2]) {
         const float2 w = __ldcs(reinterpret_cast<const float2 *>(p));
         a[0] = w.x;
@@ -682,6 +686,7 @@ struct DiaLoad<float, 2> {
 };
 template <>
 struct DiaLoad<__nv_bfloat16, 4> {
+    using E = float;
     static __device__ __forceinline__ void get(const __nv_bfloat16 *p, float (&a)[4]) {
         const uint2 w = __ldcs(reinterpret_cast<const uint2 *>(p));
         a[0] = __uint_as_float(w.x << 16);
@@ -694,14 +699,16 @@ struct DiaLoad<__nv_bfloat16, 4> {
 __device__ __forceinline__ double dia_fma(double s, double a, double x) { return __dadd_rn(s, __dmul_rn(a, x)); }
 __device__ __forceinline__ float dia_fma(float s, float a, float x) { return __fadd_rn(s, __fmul_rn(a, x)); }
 
-// A lane's R gathered x of one diagonal d for its rows row0 .. row0 + R - 1 (row0 a multiple
-// of R). A slice whose diagonals all stay inside the matrix (no kDiaClamp flag) reads without
-// clamping, FP32 pairs as one 8-byte load when d is even; otherwise each column is clamped to
-// [0, n) (padding slots may point outside; their x is never used).
+// A lane's R gathered x of one diagonal d for its rows row0 .. row0 + R - 1 (row0 = the
+// slice's first row + R lane, R even when R > 1, so row0 + d has the same parity in every
+// lane). A slice whose slots all stay inside the matrix (no kDiaClamp flag) reads without
+// clamping, pairs as one load when row0 + d is even (the pair then starts on its own width);
+// otherwise each column is clamped to [0, n) (padding slots may point outside; their x is
+// never used).
 template <bool CLAMP, int R, typename T>
 __device__ __forceinline__ void dia_gather(const T *__restrict__ x, int row0, int d, int n, T (&xv)[R]) {
     if constexpr (!CLAMP && R >= 2) {
-        if ((d & 1) == 0) {
+        if (((row0 + d) & 1) == 0) {
             using T2 = std::conditional_t<sizeof(T) == 8, double2, float2>;
 #pragma unroll
             for (int j = 0; j < R; j += 2) {
@@ -730,11 +737,74 @@ __device__ __forceinline__ void dia_gather(const T *__restrict__ x, int row0, in
 // without it, with paired FP32 gathers; for FP64 that path lost its loads' overlap (long-
 // scoreboard stalls 15.4 against 7.2 an issue, H's product 67.0 against 47.7 us under ncu),
 // so FP64 always clamps.
+// One slice (record rec, its first ints held by lanes 0 .. rs - 1): sums each live row of the
+// lane and hands it to emit(row, sum, operand) (operand: the epilogue's pre(row) when it has
+// one). Values are loaded in their stored type E and widened to T (FP64 vectors over FP32
+// factors in the batched solve) at the product.
+template <typename V, typename T, int R, typename Epi, typename Emit>
+__device__ __forceinline__ void dia_slice(const DiaView<V> &M, const T *__restrict__ x, const Epi &epi, int rec,
+                                          int lane, Emit &&emit) {
+    using E = typename DiaLoad<V, R>::E;
+    constexpr int SH = 32 * R;
+    constexpr int C = 64 / (R * (int)sizeof(E));   // diagonals a chunk: 64 bytes of values a thread
+    const unsigned full = 0xffffffffu;
+    const int k0 = __shfl_sync(full, rec, 0), mf = __shfl_sync(full, rec, 1);
+    const int first = __shfl_sync(full, rec, 2), rows = __shfl_sync(full, rec, 3);
+    const int m = mf & kDiaCountMask;
+    const int row0 = first + R * lane;
+    T opnd[R], s[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+        opnd[j] = T(0);
+        if constexpr (HasPre<Epi>::value) opnd[j] = R * lane + j < rows ? epi.pre(row0 + j) : T(0);
+        s[j] = T(0);
+    }
+    auto sum = [&](auto clamp) {
+        constexpr bool CL = decltype(clamp)::value;
+        for (int k = 0; k < m; k += C) {
+            E a[C][R];
+            T xv[C][R];
+#pragma unroll
+            for (int u = 0; u < C; ++u) {
+                const int d = __shfl_sync(full, rec, (kDiaRecHead + k + u) & 31);
+#pragma unroll
+                for (int j = 0; j < R; ++j) {
+                    a[u][j] = E(0);
+                    xv[u][j] = T(0);
+                }
+                if (k + u < m) {
+                    DiaLoad<V, R>::get(M.v + (long)(k0 + k + u) * SH + R * lane, a[u]);
+                    dia_gather<CL, R>(x, row0, d, M.n, xv[u]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < C; ++u)
+#pragma unroll
+                for (int j = 0; j < R; ++j)
+                    if (k + u < m && !DiaLoad<V, R>::pad(a[u][j])) s[j] = dia_fma(s[j], T(a[u][j]), xv[u][j]);
+        }
+    };
+    if (R == 1 || (mf & kDiaClamp)) sum(std::true_type{});
+    else sum(std::false_type{});
+#pragma unroll
+    for (int j = 0; j < R; ++j)
+        if (R * lane + j < rows) emit(row0 + j, s[j], opnd[j]);
+}
+
+// One warp per slice, grid-stride; the next slice's record is loaded while the current one is
+// summed, and a chunk's value loads and gathers are all issued before any is summed. A thread
+// sums each of its rows in storage order exactly as the CSR-stream kernels do (from 0,
+// products then sums each rounded, padding skipped), so every form gives the same bits. Lanes
+// read consecutive values and, on a banded matrix, consecutive x. Two slices per warp trip
+// took about 100 registers a thread and measured slower (H's FP64 product at 128^3: 78.9
+// against 42.9 us). The kernels are bound by instruction issue (63 % issue active at 48 %
+// warps active), so with 2 or more rows a lane a slice that needs no clamping takes a path
+// without it, gathering pairs as one load; with one row a lane that path lost its loads'
+// overlap (long-scoreboard stalls 15.4 against 7.2 an issue, H's product 67.0 against 47.7 us
+// under ncu), so one row a lane always clamps.
 template <typename V, typename T, int R, typename Epi>
 static __global__ void __launch_bounds__(kThreads)
 k_spmv_dia(DiaView<V> M, const T *__restrict__ x, Epi epi, DState *st, double *__restrict__ partials) {
-    constexpr int SH = 32 * R;
-    constexpr int C = 64 / (R * (int)sizeof(T));   // diagonals a chunk: 64 bytes of values a thread
     pdl_enter();
     if (Epi::GATED && st != nullptr && st->done) return;
     double red[Epi::NR];
@@ -742,55 +812,15 @@ k_spmv_dia(DiaView<V> M, const T *__restrict__ x, Epi epi, DState *st, double *_
     for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
     const int lane = (int)threadIdx.x & 31;
     const int nw = (int)gridDim.x * kWarps;
-    const unsigned full = 0xffffffffu;
     int sl = (int)blockIdx.x * kWarps + ((int)threadIdx.x >> 5);
     int rec = (sl < M.nsl && lane < M.rs) ? __ldg(M.rec + (long)sl * M.rs + lane) : 0;
     for (; sl < M.nsl; sl += nw) {
         const int nxt = sl + nw;
         const int rec_next = (nxt < M.nsl && lane < M.rs) ? __ldg(M.rec + (long)nxt * M.rs + lane) : 0;
-        const int row0 = sl * SH + R * lane;
-        T opnd[R], s[R];
-#pragma unroll
-        for (int j = 0; j < R; ++j) {
-            opnd[j] = T(0);
-            if constexpr (HasPre<Epi>::value) opnd[j] = row0 + j < M.n ? epi.pre(row0 + j) : T(0);
-            s[j] = T(0);
-        }
-        const int k0 = __shfl_sync(full, rec, 0), mf = __shfl_sync(full, rec, 1);
-        const int m = mf & kDiaCountMask;
-        auto sum = [&](auto clamp) {
-            constexpr bool CL = decltype(clamp)::value;
-            for (int k = 0; k < m; k += C) {
-                T a[C][R], xv[C][R];
-#pragma unroll
-                for (int u = 0; u < C; ++u) {
-                    const int d = __shfl_sync(full, rec, (2 + k + u) & 31);
-#pragma unroll
-                    for (int j = 0; j < R; ++j) {
-                        a[u][j] = T(0);
-                        xv[u][j] = T(0);
-                    }
-                    if (k + u < m) {
-                        DiaLoad<V, R>::get(M.v + (long)(k0 + k + u) * SH + R * lane, a[u]);
-                        dia_gather<CL, R>(x, row0, d, M.n, xv[u]);
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < C; ++u)
-#pragma unroll
-                    for (int j = 0; j < R; ++j)
-                        if (k + u < m && !DiaLoad<V, R>::pad(a[u][j])) s[j] = dia_fma(s[j], a[u][j], xv[u][j]);
-            }
-        };
-        if (R == 1 || (mf & kDiaClamp)) sum(std::true_type{});
-        else sum(std::false_type{});
-#pragma unroll
-        for (int j = 0; j < R; ++j) {
-            if (row0 + j < M.n) {
-                if constexpr (HasPre<Epi>::value) epi.emit_pre(row0 + j, s[j], opnd[j], red);
-                else epi.emit(row0 + j, s[j], red);
-            }
-        }
+        dia_slice<V, T, R>(M, x, epi, rec, lane, [&](int row, T s, T opnd) {
+            if constexpr (HasPre<Epi>::value) epi.emit_pre(row, s, opnd, red);
+            else epi.emit(row, s, red);
+        });
         rec = rec_next;
     }
     pdl_release();
@@ -1017,20 +1047,24 @@ k_dia_scatter(long nnz, const B *__restrict__ v, const int *__restrict__ map, B 
 }
 
 // Whether new column indices (with unchanged row offsets) still fit the slices' diagonals:
-// entry e of row i must sit in slot map[e] = sh k + i % sh of a diagonal k of slice i / sh
-// (k0 <= k < k0 + m) whose offset is ci[e] - i; sh = 32 R rows a slice. *bad is set
-// otherwise. One thread per row.
+// entry e of row i of a slice must sit in slot map[e] = sh k + i - first of a diagonal k of
+// the slice (k0 <= k < k0 + m) whose offset is ci[e] - i; sh = 32 R row slots a slice. *bad
+// is set otherwise. One warp per slice, its lanes over the slice's rows.
 static __global__ void __launch_bounds__(kThreads)
-k_dia_check(int n, const int *__restrict__ rp, const int *__restrict__ ci, const int *__restrict__ map,
+k_dia_check(int nsl, const int *__restrict__ rp, const int *__restrict__ ci, const int *__restrict__ map,
             const int *__restrict__ rec, int rs, int sh, int *bad) {
-    FIIM_FOR_ROWS(i, (long)n) {
-        const int *r = rec + (i / sh) * rs;
-        const int lane = (int)(i % sh), k0 = r[0], m = r[1] & kDiaCountMask;
-        for (int e = rp[i]; e < rp[i + 1]; ++e) {
-            const int slot = map[e], k = slot / sh - k0;
-            if (slot % sh != lane || k < 0 || k >= m || r[2 + k] != ci[e] - (int)i) {
-                atomicExch(bad, 1);
-                break;
+    const int lane = (int)threadIdx.x & 31;
+    for (int sl = (int)blockIdx.x * kWarps + ((int)threadIdx.x >> 5); sl < nsl; sl += (int)gridDim.x * kWarps) {
+        const int *r = rec + (long)sl * rs;
+        const int k0 = r[0], m = r[1] & kDiaCountMask, first = r[2], rows = r[3];
+        for (int t = lane; t < rows; t += 32) {
+            const int i = first + t;
+            for (int e = rp[i]; e < rp[i + 1]; ++e) {
+                const int slot = map[e], k = slot / sh - k0;
+                if (slot % sh != t || k < 0 || k >= m || r[kDiaRecHead + k] != ci[e] - i) {
+                    atomicExch(bad, 1);
+                    break;
+                }
             }
         }
     }

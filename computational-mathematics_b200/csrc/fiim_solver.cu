@@ -339,24 +339,45 @@ int dia_rows_per_lane(int vbytes) {
     return vbytes == 4 ? 2 : 4;
 }
 
-int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes) {
+int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes, const std::vector<int> *segments) {
     release_dia(M);
     M.dia_tried = false;
+    M.hseg_sl.clear();
     if (!dia_wanted()) return FIIM_OK;
     const int n = (int)M.n;
     const long nnz = M.nnz;
     if (n <= 0 || nnz <= 0 || (long)M.hrp.size() != (long)n + 1) return FIIM_OK;
+    const std::vector<int> whole = {0, n};
+    const std::vector<int> &seg = segments ? *segments : whole;
+    if (seg.size() < 2 || seg.front() != 0 || seg.back() != n) return set_error(FIIM_EARG, "segments must cover the rows");
     FIIM_TRY(col_hash(M, s, &M.dia_cols));
     M.dia_tried = true;
     std::vector<int> ci(nnz);
     FIIM_CUDA(cudaMemcpyAsync(ci.data(), M.ci, sizeof(int) * nnz, cudaMemcpyDeviceToHost, s));
     FIIM_CUDA(cudaStreamSynchronize(s));
     const int *rp = M.hrp.data();
-    // The diagonals of a slice of sh rows: its entries' col - row, sorted and distinct.
+    // Slices of up to sh rows, never straddling a segment: first row, rows, and each segment's
+    // first slice.
     int sh = 0, nsl = 0;
+    std::vector<int> first, rows, seg_sl;
+    auto slices = [&](int R) {
+        sh = 32 * R;
+        first.clear();
+        rows.clear();
+        seg_sl.assign(1, 0);
+        for (size_t q = 0; q + 1 < seg.size(); ++q) {
+            for (int r = seg[q]; r < seg[q + 1]; r += sh) {
+                first.push_back(r);
+                rows.push_back(std::min(sh, seg[q + 1] - r));
+            }
+            seg_sl.push_back((int)first.size());
+        }
+        nsl = (int)first.size();
+    };
+    // The diagonals of a slice: its entries' col - row, sorted and distinct.
     auto diagonals = [&](int sl, std::vector<int> &d, int &unsorted) {
         d.clear();
-        const int r0 = sl * sh, r1 = std::min(n, r0 + sh);
+        const int r0 = first[sl], r1 = r0 + rows[sl];
         for (int i = r0; i < r1; ++i)
             for (int e = rp[i]; e < rp[i + 1]; ++e) {
                 if (e > rp[i] && ci[e] <= ci[e - 1]) unsorted = 1;
@@ -369,8 +390,7 @@ int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes) {
     // slice has more than kDiaMaxDiags.
     std::vector<int> sp;
     auto count = [&](int R) -> bool {
-        sh = 32 * R;
-        nsl = (n + sh - 1) / sh;
+        slices(R);
         sp.assign(nsl + 1, 0);
         int fail = 0;
 #pragma omp parallel
@@ -410,7 +430,7 @@ int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes) {
         sp[sl + 1] += sp[sl];
     }
     const long ndiag = sp[nsl];
-    const int rs = most <= 14 ? 16 : 32;
+    const int rs = most <= 16 - kDiaRecHead ? 16 : 32;
     // Kept only when it moves fewer bytes than the CSR streams it replaces.
     const double dia_bytes = (double)vbytes * sh * ndiag + 4.0 * rs * nsl;
     const double csr_bytes_now = (double)nnz * (vbytes + (M.narrow ? 2 : 4)) + 4.0 * (n + 1);
@@ -424,13 +444,15 @@ int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes) {
         for (int sl = 0; sl < nsl; ++sl) {
             diagonals(sl, d, unused);
             int *r = rec.data() + (size_t)sl * rs;
-            const int r0 = sl * sh, r1 = std::min(n, r0 + sh);
+            const int r0 = first[sl], r1 = r0 + rows[sl];
             // Every slot of the slice (rows r0 .. r0 + sh - 1, padding included) gathers a column
             // r + d: the slice is flagged when one of them falls outside [0, n).
             const bool outside = !d.empty() && ((long)r0 + d.front() < 0 || (long)r0 + sh - 1 + d.back() > n - 1);
             r[0] = sp[sl];
             r[1] = (int)d.size() | (outside ? kDiaClamp : 0);
-            std::copy(d.begin(), d.end(), r + 2);
+            r[2] = r0;
+            r[3] = rows[sl];
+            std::copy(d.begin(), d.end(), r + kDiaRecHead);
             for (int i = r0; i < r1; ++i)
                 for (int e = rp[i]; e < rp[i + 1]; ++e) {
                     const int k = (int)(std::lower_bound(d.begin(), d.end(), ci[e] - i) - d.begin());
@@ -456,6 +478,7 @@ int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes) {
     M.nsl = nsl;
     M.drs = rs;
     M.ndiag = ndiag;
+    M.hseg_sl = seg_sl;
     FIIM_CUDA(cudaMemcpyAsync(M.drec, rec.data(), sizeof(int) * rec.size(), cudaMemcpyHostToDevice, s));
     FIIM_CUDA(cudaMemcpyAsync(M.dmap, map.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, s));
     FIIM_CUDA(cudaStreamSynchronize(s));   // before the host arrays go
@@ -466,8 +489,8 @@ int dia_fits(DevCsr &M, cudaStream_t s, bool *fits) {
     *fits = false;
     if (!M.dia_mem) return FIIM_OK;
     FIIM_CUDA(cudaMemsetAsync(M.dbad, 0, sizeof(int), s));
-    k_dia_check<<<stream_grid(k_dia_check, M.n), kThreads, 0, s>>>((int)M.n, M.rp, M.ci, M.dmap, M.drec, M.drs,
-                                                                   M.dsh, M.dbad);
+    const int g = (int)std::min<long>((M.nsl + kWarps - 1) / kWarps, 16L * num_sms());
+    k_dia_check<<<std::max(g, 1), kThreads, 0, s>>>(M.nsl, M.rp, M.ci, M.dmap, M.drec, M.drs, M.dsh, M.dbad);
     FIIM_CUDA(cudaGetLastError());
     int bad = 0;
     FIIM_CUDA(cudaMemcpyAsync(&bad, M.dbad, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -157,7 +157,7 @@ int64_t fiim_solver_device_bytes(fiim_solver_t s);
 /* Row-block size (entries) and form of the SpMV for matrix `which` (0 A, 1 G, 2 H, 3 L,
    4 U). Forms: 0 CSR streams through registers, pipelined by one block; 1 bulk copies into
    two shared-memory buffers; 2 one warp per row block; 3 the sliced-diagonal copy (rows in
-   slices of 32 that share at most 30 diagonals; built when the rows are sorted by column and
+   slices of 32 that share at most 28 diagonals; built when the rows are sorted by column and
    it moves fewer bytes; FIIM_DIA=0 or FIIM_SPMV=rows/staged/warp keep the CSR streams). Every
    form gives the same bits. */
 int fiim_solver_spmv_shape(fiim_solver_t s, int which, int *tile, int *form);

@@ -88,6 +88,22 @@ def test_batch_pdfiim_convdiff(precision):
     check_batch(convdiff_systems(9, 7, "pdfiim"), "pdfiim", precision)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "bf16"])
+def test_batch_diagonal_copies_agree_with_csr_streams(monkeypatch, precision):
+    """The batch's products read sliced-diagonal copies (slices inside the systems) where the
+    matrices allow them; with FIIM_DIA=0 they read the CSR streams. Both stay inside the
+    oracle's envelopes, and they agree system by system to rounding (the products are the same
+    bits; the per-system dot products are summed over other partials)."""
+    systems = convdiff_systems(9, 7, "pdfiim")
+    out = {}
+    for dia in ("1", "0"):
+        monkeypatch.setenv("FIIM_DIA", dia)
+        out[dia] = check_batch(systems, "pdfiim", precision)
+    assert np.all(np.abs(out["1"]["iter"].astype(int) - out["0"]["iter"].astype(int)) <= 2)
+    assert np.array_equal(out["1"]["info"], out["0"]["info"])
+    assert np.all(out["1"]["true_relres"] <= 10 * out["0"]["true_relres"] + 1e-12)
+
+
 def test_batch_acifim_golden_and_guard(golden):
     """ACIFIM factors from the reference (sherman2, 2D convection-diffusion) batched with a
     system whose alpha is non-finite at once (ACIFIM/src/bicgstab.cpp:208-213)."""

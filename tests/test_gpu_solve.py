@@ -91,7 +91,7 @@ def test_solver_products_bit_identical(golden, monkeypatch, name, prefix, varian
 def dia_bytes(rp, ci):
     """Bytes of the sliced-diagonal copy of a CSR matrix (slices of 32 rows, 8 bytes per slot
     of each slice's diagonals, a record of 16 or 32 ints per slice), or None when a row is
-    unsorted or a slice has more than 30 diagonals."""
+    unsorted or a slice has more than 28 diagonals."""
     n = len(rp) - 1
     rows = np.repeat(np.arange(n), np.diff(rp))
     if np.any((np.diff(ci) <= 0) & (np.diff(rows) == 0)):
@@ -99,10 +99,10 @@ def dia_bytes(rp, ci):
     d = ci.astype(np.int64) - rows
     key = np.unique((rows // 32) * (4 * n) + (d + 2 * n))
     per = np.bincount(key // (4 * n), minlength=(n + 31) // 32)
-    if per.max() > 30:
+    if per.max() > 28:
         return None
     nd = int(per.sum())
-    return 8.0 * 32 * nd + 4.0 * (16 if per.max() <= 14 else 32) * len(per)
+    return 8.0 * 32 * nd + 4.0 * (16 if per.max() <= 12 else 32) * len(per)
 
 
 @pytest.mark.parametrize("name,prefix,variant", [("sherman2", "afiim9e-6_", "afiim"), ("poisson128_afiim", "", "afiim"),
