@@ -39,13 +39,13 @@ struct BState {
     BlockFlags bf[6];       // A, G, H row blocks, then the slices of their sliced-diagonal copies
 };
 
+// A system leaves the loop. Its row-block and slice flags are then set by the whole CTA of
+// the finish kernel that retired it (k_bfinish): a large system has thousands of slices, and
+// one thread setting them all cost up to ~45 us a launch.
 __device__ __forceinline__ void retire(BState &bs, int k, int info) {
     bs.info[k] = info;
     bs.done[k] = 1;
     atomicSub(&bs.g->active, 1);
-    for (int m = 0; m < 6; ++m)
-        if (bs.bf[m].flag)
-            for (int b = bs.bf[m].sys_blk[k]; b < bs.bf[m].sys_blk[k + 1]; ++b) bs.bf[m].flag[b] = 1;
 }
 
 // ---------------------------------------------------------------- per-system scalar steps
@@ -263,6 +263,11 @@ k_bfinish(const int *__restrict__ sys_blk, int qmul, int nsys, const double *__r
             fin.finish(bs, k, tot);
         }
         __syncthreads();
+        if (GATED && bs.done[k])   // retired just now (a finished system was skipped above)
+            for (int m = 0; m < 6; ++m)
+                if (bs.bf[m].flag)
+                    for (int b = bs.bf[m].sys_blk[k] + (int)threadIdx.x; b < bs.bf[m].sys_blk[k + 1]; b += kThreads)
+                        bs.bf[m].flag[b] = 1;
     }
 }
 
