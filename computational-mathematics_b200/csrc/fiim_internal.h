@@ -88,6 +88,7 @@ struct DevCsr {
     unsigned long long dia_cols = 0;
     unsigned long long *dhash = nullptr;   // device scratch of the column hash (in the arena)
     std::vector<int> hseg_sl;    // first slice of each segment (host), segments + 1 entries
+    bool dseg = false;           // built with several segments: only the batched kernel reads it
     std::vector<int> hrp;        // row offsets on the host (row blocks, tuning key)
     bool rows_same = false;      // the last upload_csr found the same row offsets as before
     std::vector<long> sig;       // tuning-cache key: n, nnz, sampled row offsets

@@ -637,15 +637,15 @@ k_narrow_cols(const int *__restrict__ ci, const int *__restrict__ eb, int nblk, 
 // slot the row has no entry in holds the padding pattern (kDiaPad, kDiaPad32, kDiaPad16: NaN
 // bit patterns no entry of the matrix holds, checked when the values are placed). Each slice
 // has a record of rs ints (16 or 32): its first diagonal k0, its count m (with kDiaClamp when
-// a slot's column falls outside the matrix), its first row, its row count and its m offsets,
-// which a warp reads in one coalesced load. Bytes per entry: the value's width and the
-// padding, plus 2 or 4 per R rows for the records, against the width plus 2 or 4 per entry
-// and 4 per row for the CSR streams.
+// a slot's column falls outside the matrix), its m offsets, and in its last two ints its first
+// row and its row count; a warp reads it in one coalesced load. Bytes per entry: the value's
+// width and the padding, plus 2 or 4 per R rows for the records, against the width plus 2 or
+// 4 per entry and 4 per row for the CSR streams.
 constexpr unsigned long long kDiaPad = 0xFFF7D1A6B00C5A1DULL;   // FP64 padding; FP32 and BF16 below
 constexpr unsigned kDiaPad32 = 0xFFD1A6B5u;
 constexpr unsigned short kDiaPad16 = 0xFFD1u;
-constexpr int kDiaRecHead = 4;     // record: k0, count | flags, first row, rows; then offsets
-constexpr int kDiaMaxDiags = 32 - kDiaRecHead;   // diagonals of one slice at most
+constexpr int kDiaRecHead = 2;     // record: k0, count | flags, offsets ..., first row, rows
+constexpr int kDiaMaxDiags = 32 - kDiaRecHead - 2;   // diagonals of one slice at most
 constexpr int kDiaCountMask = 0xffff, kDiaClamp = 1 << 30;   // record[1]: count | clamp flag
 
 template <typename V = double>
@@ -749,7 +749,7 @@ __device__ __forceinline__ void dia_slice(const DiaView<V> &M, const T *__restri
     constexpr int C = 64 / (R * (int)sizeof(E));   // diagonals a chunk: 64 bytes of values a thread
     const unsigned full = 0xffffffffu;
     const int k0 = __shfl_sync(full, rec, 0), mf = __shfl_sync(full, rec, 1);
-    const int first = __shfl_sync(full, rec, 2), rows = __shfl_sync(full, rec, 3);
+    const int first = __shfl_sync(full, rec, M.rs - 2), rows = __shfl_sync(full, rec, M.rs - 1);
     const int m = mf & kDiaCountMask;
     const int row0 = first + R * lane;
     T opnd[R], s[R];
@@ -791,20 +791,27 @@ __device__ __forceinline__ void dia_slice(const DiaView<V> &M, const T *__restri
         if (R * lane + j < rows) emit(row0 + j, s[j], opnd[j]);
 }
 
-// One warp per slice, grid-stride; the next slice's record is loaded while the current one is
-// summed, and a chunk's value loads and gathers are all issued before any is summed. A thread
-// sums each of its rows in storage order exactly as the CSR-stream kernels do (from 0,
-// products then sums each rounded, padding skipped), so every form gives the same bits. Lanes
-// read consecutive values and, on a banded matrix, consecutive x. Two slices per warp trip
-// took about 100 registers a thread and measured slower (H's FP64 product at 128^3: 78.9
-// against 42.9 us). The kernels are bound by instruction issue (63 % issue active at 48 %
-// warps active), so with 2 or more rows a lane a slice that needs no clamping takes a path
-// without it, gathering pairs as one load; with one row a lane that path lost its loads'
-// overlap (long-scoreboard stalls 15.4 against 7.2 an issue, H's product 67.0 against 47.7 us
-// under ncu), so one row a lane always clamps.
+// One warp per slice of a single system (one segment: slice s starts at row 32 R s, so its
+// rows follow from s and the matrix's n), grid-stride; the next slice's record is loaded while
+// the current one is summed, and a chunk's value loads and gathers are all issued before any
+// is summed. A thread sums each of its rows in storage order exactly as the CSR-stream kernels
+// do (from 0, products then sums each rounded, padding skipped), so every form gives the same
+// bits. Lanes read consecutive values and, on a banded matrix, consecutive x. This body is
+// dia_slice's with the slice's rows taken from s: reading them from the record, as dia_slice
+// must for the batch's segments, measured 5 % slower on the 128^3 FP64 solve (G's product with
+// its norm 28.9 against 24.7 us, A's with omega 30.5 against 27.3 us, the same box).
+// Two slices per warp trip took about 100 registers a thread and measured slower (H's FP64
+// product at 128^3: 78.9 against 42.9 us). The kernels are bound by instruction issue (63 %
+// issue active at 48 % warps active), so with 2 or more rows a lane a slice that needs no
+// clamping takes a path without it, gathering pairs as one load; with one row a lane that path
+// lost its loads' overlap (long-scoreboard stalls 15.4 against 7.2 an issue, H's product 67.0
+// against 47.7 us under ncu), so one row a lane always clamps.
 template <typename V, typename T, int R, typename Epi>
 static __global__ void __launch_bounds__(kThreads)
 k_spmv_dia(DiaView<V> M, const T *__restrict__ x, Epi epi, DState *st, double *__restrict__ partials) {
+    static_assert(std::is_same_v<typename DiaLoad<V, R>::E, T>, "one system: values load as T");
+    constexpr int SH = 32 * R;
+    constexpr int C = 64 / (R * (int)sizeof(T));   // diagonals a chunk: 64 bytes of values a thread
     pdl_enter();
     if (Epi::GATED && st != nullptr && st->done) return;
     double red[Epi::NR];
@@ -812,15 +819,55 @@ k_spmv_dia(DiaView<V> M, const T *__restrict__ x, Epi epi, DState *st, double *_
     for (int j = 0; j < Epi::NR; ++j) red[j] = 0.0;
     const int lane = (int)threadIdx.x & 31;
     const int nw = (int)gridDim.x * kWarps;
+    const unsigned full = 0xffffffffu;
     int sl = (int)blockIdx.x * kWarps + ((int)threadIdx.x >> 5);
     int rec = (sl < M.nsl && lane < M.rs) ? __ldg(M.rec + (long)sl * M.rs + lane) : 0;
     for (; sl < M.nsl; sl += nw) {
         const int nxt = sl + nw;
         const int rec_next = (nxt < M.nsl && lane < M.rs) ? __ldg(M.rec + (long)nxt * M.rs + lane) : 0;
-        dia_slice<V, T, R>(M, x, epi, rec, lane, [&](int row, T s, T opnd) {
-            if constexpr (HasPre<Epi>::value) epi.emit_pre(row, s, opnd, red);
-            else epi.emit(row, s, red);
-        });
+        const int row0 = sl * SH + R * lane;
+        T opnd[R], s[R];
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            opnd[j] = T(0);
+            if constexpr (HasPre<Epi>::value) opnd[j] = row0 + j < M.n ? epi.pre(row0 + j) : T(0);
+            s[j] = T(0);
+        }
+        const int k0 = __shfl_sync(full, rec, 0), mf = __shfl_sync(full, rec, 1);
+        const int m = mf & kDiaCountMask;
+        auto sum = [&](auto clamp) {
+            constexpr bool CL = decltype(clamp)::value;
+            for (int k = 0; k < m; k += C) {
+                T a[C][R], xv[C][R];
+#pragma unroll
+                for (int u = 0; u < C; ++u) {
+                    const int d = __shfl_sync(full, rec, (kDiaRecHead + k + u) & 31);
+#pragma unroll
+                    for (int j = 0; j < R; ++j) {
+                        a[u][j] = T(0);
+                        xv[u][j] = T(0);
+                    }
+                    if (k + u < m) {
+                        DiaLoad<V, R>::get(M.v + (long)(k0 + k + u) * SH + R * lane, a[u]);
+                        dia_gather<CL, R>(x, row0, d, M.n, xv[u]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < C; ++u)
+#pragma unroll
+                    for (int j = 0; j < R; ++j)
+                        if (k + u < m && !DiaLoad<V, R>::pad(a[u][j])) s[j] = dia_fma(s[j], a[u][j], xv[u][j]);
+            }
+        };
+        if (R == 1 || (mf & kDiaClamp)) sum(std::true_type{});
+        else sum(std::false_type{});
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            if (row0 + j < M.n) {
+                if constexpr (HasPre<Epi>::value) epi.emit_pre(row0 + j, s[j], opnd[j], red);
+                else epi.emit(row0 + j, s[j], red);
+            }
+        }
         rec = rec_next;
     }
     pdl_release();
@@ -1056,7 +1103,7 @@ k_dia_check(int nsl, const int *__restrict__ rp, const int *__restrict__ ci, con
     const int lane = (int)threadIdx.x & 31;
     for (int sl = (int)blockIdx.x * kWarps + ((int)threadIdx.x >> 5); sl < nsl; sl += (int)gridDim.x * kWarps) {
         const int *r = rec + (long)sl * rs;
-        const int k0 = r[0], m = r[1] & kDiaCountMask, first = r[2], rows = r[3];
+        const int k0 = r[0], m = r[1] & kDiaCountMask, first = r[rs - 2], rows = r[rs - 1];
         for (int t = lane; t < rows; t += 32) {
             const int i = first + t;
             for (int e = rp[i]; e < rp[i + 1]; ++e) {

@@ -61,6 +61,7 @@ template <typename V, typename Epi>
 cudaError_t spmv_f(const DevCsr &M, const V *vals, cudaStream_t s, const float *x, const Epi &epi,
                    DState *st, double *partials) {
     if (M.dia && M.dvbytes == (int)sizeof(V)) {   // the sliced-diagonal copy of these values
+        if (M.dseg) return cudaErrorInvalidValue;     // k_spmv_dia takes slices of one segment
         const DiaView<V> view{M.drec, static_cast<const V *>(M.dvals), (int)M.n, M.nsl, M.drs};
         auto kern = k_spmv_dia<V, float, sizeof(V) == 4 ? 2 : 4, Epi>;   // the rows a lane it was built for
         return launch_k(kern, grid_for(kern, kWarps, M.nsl), 0, s, view, x, epi, st, partials);

@@ -198,6 +198,7 @@ static cudaError_t spmv_warp(cudaStream_t s, const DevCsr &M, const double *x, c
 template <typename Epi>
 static cudaError_t spmv_dia(cudaStream_t s, const DevCsr &M, const double *x, const Epi &epi, DState *st,
                             double *partials) {
+    if (M.dseg) return cudaErrorInvalidValue;   // k_spmv_dia takes slices of one segment
     const DiaView<double> view{M.drec, static_cast<const double *>(M.dvals), (int)M.n, M.nsl, M.drs};
     if (M.dsh == 64) {
         auto kern = k_spmv_dia<double, double, 2, Epi>;
@@ -282,6 +283,7 @@ void release_dia(DevCsr &M) {
     M.dvals = nullptr;
     M.dvbytes = 0;
     M.dsh = 0;
+    M.dseg = false;
     M.dia = 0;
     M.nsl = 0;
     M.drs = 0;
@@ -430,7 +432,7 @@ int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes, const std::vector
         sp[sl + 1] += sp[sl];
     }
     const long ndiag = sp[nsl];
-    const int rs = most <= 16 - kDiaRecHead ? 16 : 32;
+    const int rs = most <= 16 - kDiaRecHead - 2 ? 16 : 32;
     // Kept only when it moves fewer bytes than the CSR streams it replaces.
     const double dia_bytes = (double)vbytes * sh * ndiag + 4.0 * rs * nsl;
     const double csr_bytes_now = (double)nnz * (vbytes + (M.narrow ? 2 : 4)) + 4.0 * (n + 1);
@@ -450,8 +452,8 @@ int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes, const std::vector
             const bool outside = !d.empty() && ((long)r0 + d.front() < 0 || (long)r0 + sh - 1 + d.back() > n - 1);
             r[0] = sp[sl];
             r[1] = (int)d.size() | (outside ? kDiaClamp : 0);
-            r[2] = r0;
-            r[3] = rows[sl];
+            r[rs - 2] = r0;
+            r[rs - 1] = rows[sl];
             std::copy(d.begin(), d.end(), r + kDiaRecHead);
             for (int i = r0; i < r1; ++i)
                 for (int e = rp[i]; e < rp[i + 1]; ++e) {
@@ -479,6 +481,7 @@ int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes, const std::vector
     M.drs = rs;
     M.ndiag = ndiag;
     M.hseg_sl = seg_sl;
+    M.dseg = seg.size() > 2;
     FIIM_CUDA(cudaMemcpyAsync(M.drec, rec.data(), sizeof(int) * rec.size(), cudaMemcpyHostToDevice, s));
     FIIM_CUDA(cudaMemcpyAsync(M.dmap, map.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, s));
     FIIM_CUDA(cudaStreamSynchronize(s));   // before the host arrays go
