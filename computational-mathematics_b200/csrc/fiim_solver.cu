@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -394,21 +395,20 @@ int build_dia_structure(DevCsr &M, cudaStream_t s, int vbytes, const std::vector
     auto count = [&](int R) -> bool {
         slices(R);
         sp.assign(nsl + 1, 0);
-        int fail = 0;
+        std::atomic<int> fail{0};   // a failed slice ends the analysis (random matrices fail at once)
 #pragma omp parallel
         {
             std::vector<int> d;
-            int bad = 0;
 #pragma omp for schedule(dynamic, 256)
             for (int sl = 0; sl < nsl; ++sl) {
+                if (fail.load(std::memory_order_relaxed)) continue;
+                int bad = 0;
                 diagonals(sl, d, bad);
                 sp[sl + 1] = (int)d.size();
-                if ((int)d.size() > kDiaMaxDiags) bad = 1;
+                if (bad || (int)d.size() > kDiaMaxDiags) fail.store(1, std::memory_order_relaxed);
             }
-#pragma omp atomic
-            fail |= bad;
         }
-        return !fail;
+        return !fail.load();
     };
     // FP64 takes two rows a lane when its 32-row slices average more diagonals than one chunk
     // of the kernel holds (H at 128^3: 11 diagonals, 32.9 against 41.6 us a product; A and G,
