@@ -146,8 +146,10 @@ int oneshot(int variant, int issym, char mode, int nr, int n, const double *Av, 
     if (g_one.s && g_one.key == key && !issym) {
         g_one.stamps.clear();
         g_one.s->opt.verbose = verbose;
-        rc = g_one.s->reload(Ai, Aj, Av, Gi, Gj, Gv, IDv, Hi, Hj, Hv, Li, Lj, Lv, Ui, Uj, Uv);
+        rc = g_one.s->stage_inputs(b, x);   // ahead of the matrix copies
+        if (rc == FIIM_OK) rc = g_one.s->reload(Ai, Aj, Av, Gi, Gj, Gv, IDv, Hi, Hj, Hv, Li, Lj, Lv, Ui, Uj, Uv);
         if (rc == FIIM_OK) g_one.stamps = st;
+        else g_one.s->inputs_staged = false;
     } else {
         g_one.stamps.clear();
         if (g_one.s) {

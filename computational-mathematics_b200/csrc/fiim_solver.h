@@ -55,6 +55,14 @@ struct Solver : SolverBase {
     int solve_finish(double *x_io, fiim_result *res);
     int pending_launches = 0, host_loops = 0;
     Stager stager;               // host-to-device copies from pageable memory
+    // The reference-facing call's reload: b and x0 are copied ahead of the matrices
+    // (stage_inputs; the next solve_start then copies no inputs), and each sliced-diagonal
+    // copy is refreshed on the second stream `aux` while the later matrices' copies run.
+    bool inputs_staged = false;
+    int stage_inputs(const double *b, const double *x);
+    cudaStream_t aux = nullptr;
+    cudaEvent_t aux_ev[5] = {};
+    int *h_spec = nullptr;       // pinned: per matrix, the flag of its refresh on `aux`
     // Small systems: the whole solve as one cooperative launch (fiim_persist.cuh).
     bool persistent = false;
     int persist_grid = 0;

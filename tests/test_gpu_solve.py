@@ -211,6 +211,32 @@ def test_dropin_reload_replaces_diagonal_values():
         FB.dropin_cache(prev)
 
 
+def test_dropin_reload_takes_each_calls_b_and_x0():
+    """With the device-copy reuse off every drop-in call uploads the system again, with its
+    b and x0 copied ahead of the matrices. Calls with other right-hand sides and nonzero
+    initial guesses, over new values in the same structure and then the same values, each
+    equal a fresh solver's result bit for bit."""
+    A = FB.gen_convdiff3d(40, 0.5)
+    n = len(A[0]) - 1
+    F = FB.pdfiim_build(A, 0.05, 2, 2, 1, -1, "I", "B")
+    G, H = (F["Gi"], F["Gj"], F["Gv"]), (F["Hi"], F["Hj"], F["Hv"])
+    prev = FB.dropin_cache(False)
+    try:
+        for k, scale in enumerate((1.0, 1.0, 0.8, 0.8)):
+            AA = (A[0], A[1], A[2] * scale)
+            b = FB.rand_normal(n, 101 + k)
+            x0 = 0.01 * k * FB.rand_normal(n, 201 + k)
+            x = x0.copy()
+            r = FB.EPBiCGSTAB_pdfiim(AA, b, 1e-10, 500, G, F["IDv"], H, x)
+            S = FB.Solver(AA, F, variant="pdfiim")
+            y = x0.copy()
+            r1 = S.solve(b, y, tol=1e-10, nmax=500)
+            S.close()
+            assert r[2] == 0 and np.array_equal(x, y) and r[1] == r1["iter"], k
+    finally:
+        FB.dropin_cache(prev)
+
+
 @pytest.mark.parametrize("form", [None, "staged", "warp"])
 @pytest.mark.parametrize("long_len", [0, 2046, 2047, 2048, 2500])
 def test_solver_spmv_random_rows(monkeypatch, long_len, form):
