@@ -237,6 +237,39 @@ def test_dropin_reload_takes_each_calls_b_and_x0():
         FB.dropin_cache(prev)
 
 
+def test_dropin_reload_value_with_padding_pattern():
+    """A reload whose H holds the sliced-diagonal padding pattern as a value (a NaN) gives H's
+    copy up for the CSR streams, as a fresh solver does at set-up. The calls before and
+    after it, with ordinary values in the same structure, equal a fresh solver's results bit
+    for bit (the pattern's call NaN for NaN)."""
+    A = FB.gen_convdiff3d(40, 0.5)   # 64,000 rows: the graph path, whose products read the copies
+    n = len(A[0]) - 1
+    F = FB.pdfiim_build(A, 0.05, 2, 2, 1, -1, "I", "B")
+    G = (F["Gi"], F["Gj"], F["Gv"])
+    b = FB.rand_normal(n, 17)
+    pad = np.array([0xFFF7D1A6B00C5A1D], dtype=np.uint64).view(np.float64)[0]
+    prev = FB.dropin_cache(False)
+    try:
+        for k in range(3):
+            Hv = F["Hv"].copy()
+            if k == 1:
+                Hv[len(Hv) // 2] = pad
+            H = (F["Hi"], F["Hj"], Hv)
+            x = np.zeros(n)
+            r = FB.EPBiCGSTAB_pdfiim(A, b, 1e-10, 40, G, F["IDv"], H, x)
+            FF = dict(F, Hv=Hv)
+            S = FB.Solver(A, FF, variant="pdfiim")
+            form = S.spmv_shape(2)[1]
+            assert (form != 3) if k == 1 else (form == 3), k
+            y = np.zeros(n)
+            r1 = S.solve(b, y, tol=1e-10, nmax=40)
+            S.close()
+            assert np.array_equal(x, y, equal_nan=True) and r[1] == r1["iter"], k
+            assert np.isfinite(x).all() == (k != 1), k
+    finally:
+        FB.dropin_cache(prev)
+
+
 @pytest.mark.parametrize("form", [None, "staged", "warp"])
 @pytest.mark.parametrize("long_len", [0, 2046, 2047, 2048, 2500])
 def test_solver_spmv_random_rows(monkeypatch, long_len, form):
