@@ -1419,7 +1419,7 @@ int Solver::solve_finish(double *x_io, fiim_result *res) {
 
 // Enqueues the copies of b and x0 that the next solve_start would make. The reference-facing
 // call issues them before reload's matrix copies: a copy issued right after those copies and
-// the refresh ran at under half the link's rate on a B200 host (33.6 MB in 1.3-1.9 ms against
+// the refresh ran at under half the link's rate on B200 hosts (33.6 MB in 1.3-3.7 ms against
 // 0.63 ms).
 int Solver::stage_inputs(const double *b_in, const double *x_in) {
     FIIM_CUDA(cudaSetDevice(device));
